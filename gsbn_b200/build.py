@@ -1,0 +1,58 @@
+"""Builds libgsbn_b200.so (C ABI + sm_100a kernels + C++ engine) and the
+gsbn_sim command in place, with nvcc for sm_100a only.
+
+The plain FP32 path is compiled with -fmad=false so that no multiply-add is
+fused: the kernels then perform the same IEEE operations as the reference's
+CPU expressions.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INC = os.path.join(ROOT, "include")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC]
+PLAIN = ["-fmad=false"]
+
+
+def _sources(sub, ext):
+    d = os.path.join(CSRC, sub)
+    if not os.path.isdir(d):
+        return []
+    return sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith(ext))
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(verbose_ptxas=False):
+    nvcc = os.environ.get("NVCC", "nvcc")
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for src in sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+        _run([nvcc] + ARCH + COMMON + PLAIN + extra + ["-c", src, "-o", obj])
+        objs.append(obj)
+    for src in _sources("engine", ".cpp"):
+        obj = os.path.join(objdir, "engine_" + os.path.basename(src) + ".o")
+        _run([nvcc] + COMMON + ["-x", "c++", "-c", src, "-o", obj])
+        objs.append(obj)
+    lib = os.path.join(HERE, "libgsbn_b200.so")
+    _run([nvcc] + ARCH + ["-shared", "-o", lib] + objs + ["-cudart", "static"])
+    main = os.path.join(CSRC, "engine", "main", "gsbn_sim.cpp")
+    if os.path.exists(main):
+        exe = os.path.join(HERE, "gsbn_sim")
+        _run([nvcc] + COMMON + ["-x", "c++", main, "-o", exe, "-L" + HERE, "-lgsbn_b200",
+                                "-Xlinker", "-rpath=$ORIGIN"])
+    return lib
+
+
+if __name__ == "__main__":
+    build(verbose_ptxas="-v" in sys.argv)

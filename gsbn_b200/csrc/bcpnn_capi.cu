@@ -1,0 +1,863 @@
+/*
+ * bcpnn_capi.cu -- implementation of include/bcpnn.h for one network on one
+ * B200: device allocation with gsbn's initial values, per-run orchestration
+ * (decay tables, all-cells catch-up, one fused kernel per tick, captured once
+ * per run length into a CUDA graph and replayed), and state import/export in
+ * gsbn's Database layouts.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "bcpnn.h"
+#include "bcpnn_device.cuh"
+#include "bcpnn_numerics.h"
+
+using namespace bcpnn;
+
+namespace {
+
+struct TableSlot {
+  uint32_t kp_bits = 0;
+  int len = 0;   /* valid entries */
+  int cap = 0;   /* allocated entries */
+  float4* ptr = nullptr;
+  uint64_t stamp = 0;
+};
+
+struct PopHost {
+  bcpnn_pop_desc d;
+  int H, M, n, hcu_start, mcu_start, dim_proj = 0;
+  std::vector<int> in_proj, out_proj;
+  int log_words;
+  size_t log_offset;  /* words, within the common log buffer */
+  int* ext_off = nullptr;
+  int* ext_idx = nullptr;
+};
+
+struct ProjHost {
+  bcpnn_proj_desc d;
+  int H, M, C, Ns, proj_in_pop;
+  TableSlot slot[2];
+};
+
+}  // namespace
+
+struct bcpnn_net {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  std::vector<PopHost> pops;
+  std::vector<ProjHost> projs;
+  NetDev h;                 /* host image of the device descriptor */
+  NetDev* d_net = nullptr;
+  RunParams rp;             /* host image of the run parameters */
+  RunParams* d_rp = nullptr;
+  int total_hcu = 0, total_mcu = 0, max_m = 1;
+  int max_ticks = 0;
+  uint32_t* log_buf = nullptr;
+  size_t log_words_per_tick = 0;
+  int64_t k_total = 0;      /* ticks executed since creation */
+  int last_run_ticks = 0;
+  bool exchange = false;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  uint64_t launches = 0;
+  uint64_t all_cells = 0;   /* cells swept by all-cells catch-ups */
+  uint64_t stamp = 0;
+  float* scratch = nullptr; /* staging for strided cell fields */
+  size_t scratch_n = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(bcpnn_net* net, int code, const std::string& msg) {
+  if (net) net->err = msg;
+  return code;
+}
+
+#define CU(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(net, BCPNN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+template <typename T>
+int dalloc(bcpnn_net* net, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  CU(cudaMalloc((void**)p, count * sizeof(T)));
+  net->allocs.push_back((void*)*p);
+  return BCPNN_OK;
+}
+
+template <typename T>
+int dfill(bcpnn_net* net, T* p, size_t count, T value) {
+  std::vector<T> v(count, value);
+  CU(cudaMemcpyAsync(p, v.data(), count * sizeof(T), cudaMemcpyHostToDevice, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  return BCPNN_OK;
+}
+
+int grid_for(size_t n, int block) {
+  size_t g = (n + block - 1) / block;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+int check_device_error(bcpnn_net* net) {
+  int e = 0;
+  CU(cudaMemcpyAsync(&e, net->h.err, sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  if (e) {
+    CU(cudaMemsetAsync(net->h.err, 0, sizeof(int), net->stream));
+    return fail(net, BCPNN_ERR_DEVICE, "kernel reported error word " + std::to_string(e) +
+                                           " (a slot's source MCU index is outside the source population)");
+  }
+  return BCPNN_OK;
+}
+
+/* (re)build the decay table of slot s of projection p for kp = taupdt*prn
+   with at least `need` entries */
+int fill_slot(bcpnn_net* net, int p, int s, float prn, int need) {
+  ProjHost& J = net->projs[p];
+  const ProjDev& D = net->h.projs[p];
+  float kp = D.taupdt * prn;
+  TableSlot& T = J.slot[s];
+  if (T.ptr && T.kp_bits == bx_fbits(kp) && T.len >= need) return BCPNN_OK;
+  if (T.cap < need) {
+    int cap = 1024;
+    while (cap < need) cap *= 2;
+    if (T.ptr) CU(cudaFree(T.ptr));
+    T.ptr = nullptr;
+    CU(cudaMalloc((void**)&T.ptr, (size_t)cap * 4 * sizeof(float4)));
+    T.cap = cap;
+  }
+  build_table_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.cap, kp, D.ke, D.kzi, D.kzj);
+  CU(cudaGetLastError());
+  net->launches++;
+  T.kp_bits = bx_fbits(kp);
+  T.len = T.cap;
+  return BCPNN_OK;
+}
+
+/* Tables of projection p for this run: slot *s_cur for prn, and, when the
+   all-cells catch-up runs, slot *s_old for old_prn.  Two slots per projection
+   cover the usual alternation of training and recall segments. */
+int prepare_tables(bcpnn_net* net, int p, float prn, float old_prn, bool with_all, int need_cur, int need_old,
+                   int* s_cur, int* s_old) {
+  ProjHost& J = net->projs[p];
+  const ProjDev& D = net->h.projs[p];
+  uint32_t b_cur = bx_fbits(D.taupdt * prn), b_old = bx_fbits(D.taupdt * old_prn);
+  auto lookup = [&](uint32_t b) {
+    for (int s = 0; s < 2; ++s)
+      if (J.slot[s].ptr && J.slot[s].kp_bits == b) return s;
+    return -1;
+  };
+  int sc = lookup(b_cur);
+  int so = with_all ? lookup(b_old) : -1;
+  if (with_all && b_old == b_cur) so = sc;
+  if (sc < 0) {
+    if (so >= 0) sc = so ^ 1;
+    else sc = (J.slot[0].stamp <= J.slot[1].stamp) ? 0 : 1;
+  }
+  if (with_all && so < 0) so = (b_old == b_cur) ? sc : (sc ^ 1);
+  int rc = fill_slot(net, p, sc, prn, need_cur);
+  if (rc) return rc;
+  if (with_all && so != sc && (rc = fill_slot(net, p, so, old_prn, need_old))) return rc;
+  if (with_all && so == sc && b_old != b_cur) return fail(net, BCPNN_ERR_STATE, "decay table slot conflict");
+  J.slot[sc].stamp = ++net->stamp;
+  if (with_all) J.slot[so].stamp = ++net->stamp;
+  *s_cur = sc;
+  *s_old = so;
+  return BCPNN_OK;
+}
+
+int capture_graph(bcpnn_net* net, int n_ticks, bool with_all, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+  for (const PopHost& P : net->pops)
+    cudaMemsetAsync(net->log_buf + P.log_offset, 0, (size_t)n_ticks * P.log_words * sizeof(uint32_t), net->stream);
+  cudaMemsetAsync(net->h.ss_log, 0, (size_t)n_ticks * net->h.n_projs * sizeof(uint32_t), net->stream);
+  if (with_all) {
+    for (int p = 0; p < net->h.n_projs; ++p) {
+      const ProjHost& J = net->projs[p];
+      all_rows_kernel<<<grid_for((size_t)J.H * J.C, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
+      all_cells_kernel<<<grid_for((size_t)J.H * J.C * J.M, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
+    }
+  }
+  size_t smem = tick_smem_bytes(net->max_m);
+  for (int it = 0; it < n_ticks; ++it)
+    tick_kernel<<<net->total_hcu, kBlock, smem, net->stream>>>(net->d_net, net->d_rp, it, net->max_m);
+  cudaError_t le = cudaGetLastError();
+  cudaError_t ce = cudaStreamEndCapture(net->stream, &g);
+  if (le != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(net, BCPNN_ERR_CUDA, std::string("kernel launch during capture: ") + cudaGetErrorString(le));
+  }
+  CU(ce);
+  cudaError_t ie = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  CU(ie);
+  return BCPNN_OK;
+}
+
+/* name -> (kind, pointer, count, element type) resolution */
+enum Kind { K_PLAIN, K_PARITY, K_CELL, K_SIQ, K_SI };
+struct Resolved {
+  Kind kind;
+  int type;       /* BCPNN_F32 / I32 / I8 */
+  size_t count;
+  void* ptr;      /* K_PLAIN */
+  void* par[2];   /* K_PARITY, K_SI */
+  int field;      /* K_CELL */
+  float4* cell;
+  int proj;
+};
+
+bool resolve(const bcpnn_net* net, const char* cname, Resolved* r) {
+  if (!cname) return false;
+  std::string name(cname);
+  size_t us = name.rfind('_');
+  if (us == std::string::npos || us + 1 >= name.size()) return false;
+  std::string base = name.substr(0, us);
+  const char* num = name.c_str() + us + 1;
+  for (const char* c = num; *c; ++c)
+    if (*c < '0' || *c > '9') return false;
+  int id = std::atoi(num);
+  r->proj = id;
+  if (id < (int)net->pops.size()) {
+    const PopHost& P = net->pops[id];
+    const PopDev& D = net->h.pops[id];
+    size_t n = (size_t)P.n;
+    auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
+    auto parity = [&](float* a, float* b, size_t count) { r->kind = K_PARITY; r->par[0] = a; r->par[1] = b; r->type = BCPNN_F32; r->count = count; return true; };
+    if (base == "dsup") return parity(D.dsup[0], D.dsup[1], n);
+    if (base == "epsc") return parity(D.epsc[0], D.epsc[1], n * P.dim_proj);
+    if (base == "bj") return parity(D.bj[0], D.bj[1], n * P.dim_proj);
+    if (base == "act") return plain(D.act, BCPNN_F32, n);
+    if (base == "spike") return plain(D.spike, BCPNN_I8, n);
+    if (base == ".counter") return plain(D.counter, BCPNN_I32, n);
+  }
+  if (id < (int)net->projs.size()) {
+    const ProjHost& J = net->projs[id];
+    const ProjDev& D = net->h.projs[id];
+    size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
+    auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
+    auto cell = [&](int f) { r->kind = K_CELL; r->field = f; r->cell = D.cell; r->type = BCPNN_F32; r->count = cells; return true; };
+    if (base == "ii") return plain(D.ii, BCPNN_I32, R);
+    if (base == "di") return plain(D.di, BCPNN_I32, R);
+    if (base == "qi") return plain(D.qi, BCPNN_I32, R);
+    if (base == "pi") return plain(D.pi, BCPNN_F32, R);
+    if (base == "ei") return plain(D.ei, BCPNN_F32, R);
+    if (base == "zi") return plain(D.zi, BCPNN_F32, R);
+    if (base == "ti") return plain(D.ti, BCPNN_I32, R);
+    if (base == "pj") return plain(D.pj, BCPNN_F32, HM);
+    if (base == "ej") return plain(D.ej, BCPNN_F32, HM);
+    if (base == "zj") return plain(D.zj, BCPNN_F32, HM);
+    if (base == "tij") return plain(D.tij, BCPNN_I32, cells);
+    if (base == "wij") return plain(D.wij, BCPNN_F32, cells);
+    if (base == "pij") return cell(0);
+    if (base == "eij") return cell(1);
+    if (base == "zi2") return cell(2);
+    if (base == "zj2") return cell(3);
+    if (base == "si") { r->kind = K_SI; r->par[0] = D.si[0]; r->par[1] = D.si[1]; r->type = BCPNN_I8; r->count = (size_t)J.Ns; return true; }
+    if (base == ".siq") { r->kind = K_SIQ; r->type = BCPNN_I8; r->count = R; return true; }
+  }
+  return false;
+}
+
+size_t type_size(int t) { return t == BCPNN_I8 ? 1 : 4; }
+
+int ensure_scratch(bcpnn_net* net, size_t n) {
+  if (net->scratch_n >= n) return BCPNN_OK;
+  if (net->scratch) CU(cudaFree(net->scratch));
+  net->scratch = nullptr;
+  CU(cudaMalloc((void**)&net->scratch, n * sizeof(float)));
+  net->scratch_n = n;
+  return BCPNN_OK;
+}
+
+}  // namespace
+
+/* ======================================================================== */
+
+extern "C" {
+
+const char* bcpnn_status_string(int s) {
+  switch (s) {
+    case BCPNN_OK: return "ok";
+    case BCPNN_ERR_INVALID: return "invalid argument";
+    case BCPNN_ERR_CUDA: return "CUDA runtime error";
+    case BCPNN_ERR_NOT_FOUND: return "unknown state vector";
+    case BCPNN_ERR_SIZE: return "size mismatch";
+    case BCPNN_ERR_STATE: return "invalid state";
+    case BCPNN_ERR_DEVICE: return "device error word set";
+  }
+  return "unknown status";
+}
+
+const char* bcpnn_last_error(const bcpnn_net* net) { return net ? net->err.c_str() : "null handle"; }
+
+int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
+  if (!out) return BCPNN_ERR_INVALID;
+  *out = nullptr;
+  if (!desc || desc->n_pops <= 0 || desc->n_pops > 16 || desc->n_projs < 0 || desc->n_projs > kMaxProj ||
+      (desc->n_pops && !desc->pops) || (desc->n_projs && !desc->projs) || !(desc->dt > 0.0f) ||
+      desc->max_ticks_per_run <= 0)
+    return BCPNN_ERR_INVALID;
+  for (int p = 0; p < desc->n_pops; ++p)
+    if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 || desc->pops[p].mcu_num > 1024)
+      return BCPNN_ERR_INVALID;
+  for (int p = 0; p < desc->n_projs; ++p) {
+    const bcpnn_proj_desc& d = desc->projs[p];
+    if (d.src_pop < 0 || d.src_pop >= desc->n_pops || d.dest_pop < 0 || d.dest_pop >= desc->n_pops ||
+        (int)d.slot_num <= 0)
+      return BCPNN_ERR_INVALID;
+  }
+  bcpnn_net* net = new bcpnn_net();
+  net->device = desc->device;
+  net->max_ticks = desc->max_ticks_per_run;
+  net->exchange = desc->exchange_spikes != 0;
+  std::memset(&net->h, 0, sizeof(NetDev));
+  std::memset(&net->rp, 0, sizeof(RunParams));
+  int rc = BCPNN_OK;
+  auto bail = [&](int code) { *out = net; return code; };
+  if (cudaSetDevice(net->device) != cudaSuccess) { net->err = "cudaSetDevice failed"; return bail(BCPNN_ERR_CUDA); }
+  if (cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    net->err = "cudaStreamCreate failed";
+    return bail(BCPNN_ERR_CUDA);
+  }
+
+  /* populations: running HCU/MCU offsets (ProcUpdLazy.cpp:19-29) */
+  NetDev& H = net->h;
+  H.n_pops = desc->n_pops;
+  H.n_projs = desc->n_projs;
+  H.dt = desc->dt;
+  H.poisson_hz = desc->poisson_noise_hz;
+  H.seed = desc->seed;
+  for (int p = 0; p < desc->n_pops; ++p) {
+    PopHost P;
+    P.d = desc->pops[p];
+    P.H = P.d.hcu_num;
+    P.M = P.d.mcu_num;
+    P.n = P.H * P.M;
+    P.hcu_start = net->total_hcu;
+    P.mcu_start = net->total_mcu;
+    net->total_hcu += P.H;
+    net->total_mcu += P.n;
+    net->max_m = std::max(net->max_m, P.M);
+    net->pops.push_back(P);
+  }
+  /* projections: dim_conn, proj_in_pop, coefficients (Proj.cpp:16-52) */
+  for (int q = 0; q < desc->n_projs; ++q) {
+    ProjHost J;
+    J.d = desc->projs[q];
+    PopHost& src = net->pops[J.d.src_pop];
+    PopHost& dst = net->pops[J.d.dest_pop];
+    J.H = dst.H;
+    J.M = dst.M;
+    J.Ns = src.n;
+    J.C = src.n;
+    int slot = (int)J.d.slot_num;
+    if (J.C > slot) J.C = slot;
+    J.proj_in_pop = dst.dim_proj++;
+    dst.in_proj.push_back(q);
+    net->projs.push_back(J);
+  }
+  /* ProcExchangeSpike publishes the spikes of populations that are the
+     destination of a projection (ProcExchangeSpike.cpp:109-119) */
+  if (net->exchange) {
+    for (int q = 0; q < desc->n_projs; ++q) {
+      int s = net->projs[q].d.src_pop;
+      if (net->pops[s].in_proj.size() > 0) net->pops[s].out_proj.push_back(q);
+    }
+  }
+  /* spike log: per population a [max_ticks][words] region */
+  net->log_words_per_tick = 0;
+  for (auto& P : net->pops) {
+    P.log_words = (P.n + 31) / 32;
+    P.log_offset = net->log_words_per_tick * (size_t)desc->max_ticks_per_run;
+    net->log_words_per_tick += P.log_words;
+  }
+
+  float dt = desc->dt;
+  if ((rc = dalloc(net, &net->log_buf, (size_t)net->max_ticks * net->log_words_per_tick))) return bail(rc);
+  uint32_t* ss = nullptr;
+  if ((rc = dalloc(net, &ss, (size_t)net->max_ticks * std::max(1, desc->n_projs)))) return bail(rc);
+  H.ss_log = ss;
+  unsigned long long* cnt = nullptr;
+  if ((rc = dalloc(net, &cnt, 3))) return bail(rc);
+  H.counters = cnt;
+  int* errw = nullptr;
+  if ((rc = dalloc(net, &errw, 1))) return bail(rc);
+  H.err = errw;
+  if (cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), net->stream) != cudaSuccess ||
+      cudaMemsetAsync(errw, 0, sizeof(int), net->stream) != cudaSuccess) {
+    net->err = "memset failed";
+    return bail(BCPNN_ERR_CUDA);
+  }
+  float* lg = nullptr;
+  float* wm = nullptr;
+  if ((rc = dalloc(net, &lg, net->total_mcu))) return bail(rc);
+  if ((rc = dalloc(net, &wm, net->total_hcu))) return bail(rc);
+  if ((rc = dfill(net, lg, net->total_mcu, 0.0f))) return bail(rc);
+  if ((rc = dfill(net, wm, net->total_hcu, 0.0f))) return bail(rc);
+  H.lginp = lg;
+  H.wmask = wm;
+
+  std::vector<int> idx_lists;
+  for (int p = 0; p < desc->n_pops; ++p) {
+    PopHost& P = net->pops[p];
+    PopDev& D = H.pops[p];
+    D.H = P.H; D.M = P.M; D.n = P.n; D.hcu_start = P.hcu_start; D.mcu_start = P.mcu_start;
+    D.dim_proj = P.dim_proj; D.id = p;
+    D.taumdt = dt / P.d.taum;                  /* Pop.cpp:34 */
+    D.wtagain = P.d.wtagain;
+    D.maxfqdt = P.d.maxfq * dt;                /* Pop.cpp:36 */
+    D.igain = P.d.igain;
+    D.wgain = P.d.wgain;
+    D.lgbias = P.d.lgbias;
+    D.snoise = P.d.snoise;
+    size_t n = P.n, ne = n * std::max(1, P.dim_proj);
+    for (int b = 0; b < 2; ++b) {
+      if ((rc = dalloc(net, &D.dsup[b], n))) return bail(rc);
+      if ((rc = dalloc(net, &D.epsc[b], ne))) return bail(rc);
+      if ((rc = dalloc(net, &D.bj[b], ne))) return bail(rc);
+      /* dsup = log(1.0/M) in double, stored as float (Pop.cpp:59) */
+      if ((rc = dfill(net, D.dsup[b], n, (float)bx_log_d(1.0 / P.M)))) return bail(rc);
+      if ((rc = dfill(net, D.epsc[b], ne, 0.0f))) return bail(rc);
+      if ((rc = dfill(net, D.bj[b], ne, 0.0f))) return bail(rc);
+    }
+    if ((rc = dalloc(net, &D.act, n))) return bail(rc);
+    if ((rc = dfill(net, D.act, n, (float)(1.0 / P.M)))) return bail(rc);   /* Pop.cpp:60 */
+    if ((rc = dalloc(net, &D.spike, n))) return bail(rc);
+    if ((rc = dfill(net, D.spike, n, (int8_t)0))) return bail(rc);
+    if ((rc = dalloc(net, &D.counter, n))) return bail(rc);
+    if ((rc = dfill(net, D.counter, n, 0))) return bail(rc);
+    D.spk_log = net->log_buf + P.log_offset;
+    D.log_words = P.log_words;
+    D.n_in = (int)P.in_proj.size();
+    D.n_out = (int)P.out_proj.size();
+    D.ext = 0;
+  }
+  /* in/out projection index lists */
+  {
+    std::vector<int> all;
+    std::vector<std::pair<size_t, size_t>> off(desc->n_pops);
+    for (int p = 0; p < desc->n_pops; ++p) {
+      size_t a = all.size();
+      for (int q : net->pops[p].in_proj) all.push_back(q);
+      size_t b = all.size();
+      for (int q : net->pops[p].out_proj) all.push_back(q);
+      off[p] = {a, b};
+    }
+    int* dl = nullptr;
+    if ((rc = dalloc(net, &dl, std::max<size_t>(1, all.size())))) return bail(rc);
+    if (!all.empty() && cudaMemcpy(dl, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+      net->err = "copy of projection lists failed";
+      return bail(BCPNN_ERR_CUDA);
+    }
+    for (int p = 0; p < desc->n_pops; ++p) {
+      H.pops[p].in_proj = dl + off[p].first;
+      H.pops[p].out_proj = dl + off[p].second;
+    }
+  }
+  for (int q = 0; q < desc->n_projs; ++q) {
+    ProjHost& J = net->projs[q];
+    ProjDev& D = H.projs[q];
+    const bcpnn_proj_desc& d = J.d;
+    D.src = d.src_pop; D.dest = d.dest_pop; D.H = J.H; D.M = J.M; D.C = J.C; D.Ns = J.Ns;
+    D.proj_in_pop = J.proj_in_pop;
+    D.kzi = dt / d.tauzi;                       /* Proj.cpp:38-52 */
+    D.kzj = dt / d.tauzj;
+    D.ke = dt / d.taue;
+    D.taupdt = dt / d.taup;
+    D.eps = dt / d.taup;
+    D.eps2 = (dt / d.taup) * (dt / d.taup);
+    D.kfti = 1 / (d.maxfq * d.tauzi);
+    D.kftj = 1 / (d.maxfq * d.tauzj);
+    D.bgain = d.bgain;
+    D.wgain = d.wgain;
+    D.kepsc = d.tauepsc > 0.0f ? dt / d.tauepsc : D.kzi;
+    size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
+    if ((rc = dalloc(net, &D.ii, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.di, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.qi, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.pi, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.ei, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.zi, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.ti, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.pj, HM))) return bail(rc);
+    if ((rc = dalloc(net, &D.ej, HM))) return bail(rc);
+    if ((rc = dalloc(net, &D.zj, HM))) return bail(rc);
+    if ((rc = dalloc(net, &D.cell, cells))) return bail(rc);
+    if ((rc = dalloc(net, &D.tij, cells))) return bail(rc);
+    if ((rc = dalloc(net, &D.wij, cells))) return bail(rc);
+    if ((rc = dalloc(net, &D.si[0], J.Ns))) return bail(rc);
+    if ((rc = dalloc(net, &D.si[1], J.Ns))) return bail(rc);
+    if ((rc = dalloc(net, &D.list, R))) return bail(rc);
+    if ((rc = dalloc(net, &D.list_cnt, J.H))) return bail(rc);
+    if ((rc = dfill(net, D.ii, R, -1))) return bail(rc);                          /* Proj.cpp:88 */
+    if ((rc = dfill(net, D.di, R, 0))) return bail(rc);
+    if ((rc = dfill(net, D.qi, R, 0))) return bail(rc);
+    if ((rc = dfill(net, D.pi, R, (float)(1.0 / J.C)))) return bail(rc);          /* Proj.cpp:91 */
+    if ((rc = dfill(net, D.ei, R, 0.0f))) return bail(rc);
+    if ((rc = dfill(net, D.zi, R, 0.0f))) return bail(rc);
+    if ((rc = dfill(net, D.ti, R, 0))) return bail(rc);
+    if ((rc = dfill(net, D.pj, HM, (float)(1.0 / J.M)))) return bail(rc);         /* Proj.cpp:96 */
+    if ((rc = dfill(net, D.ej, HM, 0.0f))) return bail(rc);
+    if ((rc = dfill(net, D.zj, HM, 0.0f))) return bail(rc);
+    float pij0 = (float)(1.0 / J.C / J.M);                                         /* Proj.cpp:99 */
+    if ((rc = dfill(net, D.cell, cells, make_float4(pij0, 0.0f, 0.0f, 0.0f)))) return bail(rc);
+    if ((rc = dfill(net, D.tij, cells, 0))) return bail(rc);
+    if ((rc = dfill(net, D.wij, cells, 0.0f))) return bail(rc);
+    if ((rc = dfill(net, D.si[0], (size_t)J.Ns, (int8_t)0))) return bail(rc);
+    if ((rc = dfill(net, D.si[1], (size_t)J.Ns, (int8_t)0))) return bail(rc);
+    if ((rc = dfill(net, D.list_cnt, (size_t)J.H, 0))) return bail(rc);
+  }
+  /* CTA -> (population, HCU) */
+  {
+    std::vector<int> cp, ch;
+    for (int p = 0; p < desc->n_pops; ++p)
+      for (int hh = 0; hh < net->pops[p].H; ++hh) { cp.push_back(p); ch.push_back(hh); }
+    int* dp = nullptr;
+    int* dh = nullptr;
+    if ((rc = dalloc(net, &dp, cp.size()))) return bail(rc);
+    if ((rc = dalloc(net, &dh, ch.size()))) return bail(rc);
+    if (cudaMemcpy(dp, cp.data(), cp.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dh, ch.data(), ch.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+      net->err = "copy of CTA map failed";
+      return bail(BCPNN_ERR_CUDA);
+    }
+    H.cta_pop = dp;
+    H.cta_hcu = dh;
+  }
+  if ((rc = dalloc(net, &net->d_net, 1))) return bail(rc);
+  if ((rc = dalloc(net, &net->d_rp, 1))) return bail(rc);
+  if (cudaMemcpy(net->d_net, &net->h, sizeof(NetDev), cudaMemcpyHostToDevice) != cudaSuccess) {
+    net->err = "copy of network descriptor failed";
+    return bail(BCPNN_ERR_CUDA);
+  }
+  size_t smem = tick_smem_bytes(net->max_m);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    net->err = "cannot raise the shared memory limit of tick_kernel";
+    return bail(BCPNN_ERR_CUDA);
+  }
+  if (cudaStreamSynchronize(net->stream) != cudaSuccess) {
+    net->err = "initialisation failed";
+    return bail(BCPNN_ERR_CUDA);
+  }
+  *out = net;
+  return BCPNN_OK;
+}
+
+int bcpnn_net_destroy(bcpnn_net* net) {
+  if (!net) return BCPNN_ERR_INVALID;
+  cudaSetDevice(net->device);
+  if (net->stream) cudaStreamSynchronize(net->stream);
+  for (auto& kv : net->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& J : net->projs)
+    for (auto& s : J.slot)
+      if (s.ptr) cudaFree(s.ptr);
+  for (void* p : net->allocs) cudaFree(p);
+  if (net->scratch) cudaFree(net->scratch);
+  if (net->stream) cudaStreamDestroy(net->stream);
+  delete net;
+  return BCPNN_OK;
+}
+
+int bcpnn_set_conn(bcpnn_net* net, int32_t proj, const int32_t* ii, const int32_t* di, size_t n_slots) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (proj < 0 || proj >= (int)net->projs.size() || !ii || !di)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_conn: bad projection or null table");
+  const ProjHost& J = net->projs[proj];
+  if (n_slots != (size_t)J.H * J.C) return fail(net, BCPNN_ERR_SIZE, "bcpnn_set_conn: slot count != H*C");
+  for (size_t s = 0; s < n_slots; ++s) {
+    if (ii[s] >= J.Ns || ii[s] < -1) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_conn: ii outside [-1, Hs*Ms)");
+    if (ii[s] >= 0 && (di[s] < 1 || di[s] > 31))
+      return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_conn: delay outside [1, 31] ticks");
+  }
+  CU(cudaSetDevice(net->device));
+  const ProjDev& D = net->h.projs[proj];
+  CU(cudaMemcpyAsync(D.ii, ii, n_slots * sizeof(int), cudaMemcpyHostToDevice, net->stream));
+  CU(cudaMemcpyAsync(D.di, di, n_slots * sizeof(int), cudaMemcpyHostToDevice, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  return BCPNN_OK;
+}
+
+int bcpnn_set_stimulus(bcpnn_net* net, const float* lginp, size_t n_mcu, const float* wmask_row, size_t n_hcu) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (!lginp || !wmask_row) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_stimulus: null buffer");
+  if (n_mcu != (size_t)net->total_mcu || n_hcu != (size_t)net->total_hcu)
+    return fail(net, BCPNN_ERR_SIZE, "bcpnn_set_stimulus: sizes must be total MCUs and total HCUs");
+  CU(cudaSetDevice(net->device));
+  CU(cudaMemcpyAsync((void*)net->h.lginp, lginp, n_mcu * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  CU(cudaMemcpyAsync((void*)net->h.wmask, wmask_row, n_hcu * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  return BCPNN_OK;
+}
+
+int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* ticks, const int32_t* offsets,
+                         const int32_t* idx) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (pop < 0 || pop >= (int)net->pops.size() || n < 0 || (n > 0 && (!ticks || !offsets || !idx)))
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_ext_spikes: bad arguments");
+  PopHost& P = net->pops[pop];
+  /* later entries for the same tick replace earlier ones (std::map assignment,
+     Pop.cpp:97) */
+  std::map<int, std::pair<int, int>> by_tick;
+  int t0 = 0, t1 = 0;
+  for (int k = 0; k < n; ++k) {
+    if (ticks[k] < 0) continue;
+    if (offsets[k + 1] < offsets[k]) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_ext_spikes: bad offsets");
+    for (int e = offsets[k]; e < offsets[k + 1]; ++e)
+      if (idx[e] < 0 || idx[e] >= P.n)
+        return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_ext_spikes: MCU index outside the population");
+    by_tick[ticks[k]] = {offsets[k], offsets[k + 1]};
+  }
+  std::vector<int> off, flat;
+  if (!by_tick.empty()) {
+    t0 = by_tick.begin()->first;
+    t1 = by_tick.rbegin()->first + 1;
+    off.assign((size_t)(t1 - t0) + 1, 0);
+    for (int t = t0; t < t1; ++t) {
+      off[t - t0] = (int)flat.size();
+      auto it = by_tick.find(t);
+      if (it != by_tick.end())
+        for (int e = it->second.first; e < it->second.second; ++e) flat.push_back(idx[e]);
+    }
+    off[t1 - t0] = (int)flat.size();
+  } else {
+    off.assign(1, 0);
+  }
+  CU(cudaSetDevice(net->device));
+  CU(cudaStreamSynchronize(net->stream));
+  if (P.ext_off) { CU(cudaFree(P.ext_off)); P.ext_off = nullptr; }
+  if (P.ext_idx) { CU(cudaFree(P.ext_idx)); P.ext_idx = nullptr; }
+  CU(cudaMalloc((void**)&P.ext_off, off.size() * sizeof(int)));
+  CU(cudaMalloc((void**)&P.ext_idx, std::max<size_t>(1, flat.size()) * sizeof(int)));
+  CU(cudaMemcpy(P.ext_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!flat.empty()) CU(cudaMemcpy(P.ext_idx, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
+  net->allocs.push_back(P.ext_off);
+  net->allocs.push_back(P.ext_idx);
+  PopDev& D = net->h.pops[pop];
+  D.ext = 1;
+  D.ext_off = P.ext_off;
+  D.ext_idx = P.ext_idx;
+  D.ext_t0 = t0;
+  D.ext_t1 = t1;
+  CU(cudaMemcpy(net->d_net, &net->h, sizeof(NetDev), cudaMemcpyHostToDevice));
+  return BCPNN_OK;
+}
+
+int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn, float old_prn) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (n_ticks <= 0 || n_ticks > net->max_ticks)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_run: n_ticks outside [1, max_ticks_per_run]");
+  if (first_simstep < 1 || (int64_t)first_simstep + n_ticks > (1 << 24))
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_run: simstep outside [1, 2^24)");
+  CU(cudaSetDevice(net->device));
+  bool with_all = (old_prn != prn);
+  int need = first_simstep + n_ticks + 1;
+  for (int p = 0; p < (int)net->projs.size(); ++p) {
+    int s = 0, so = -1, rc;
+    if ((rc = prepare_tables(net, p, prn, old_prn, with_all, need, first_simstep + 1, &s, &so))) return rc;
+    const ProjHost& J = net->projs[p];
+    net->rp.tab[p] = J.slot[s].ptr;
+    net->rp.tab_len[p] = J.slot[s].len;
+    if (with_all) {
+      net->rp.tab_old[p] = J.slot[so].ptr;
+      net->rp.tab_old_len[p] = J.slot[so].len;
+    } else {
+      net->rp.tab_old[p] = nullptr;
+      net->rp.tab_old_len[p] = 0;
+    }
+  }
+  net->rp.simstep0 = first_simstep;
+  net->rp.k0 = (int)(net->k_total & 0x7fffffff);
+  net->rp.n_ticks = n_ticks;
+  net->rp.prn = prn;
+  net->rp.old_prn = old_prn;
+  CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));
+  auto key = std::make_pair(n_ticks, with_all ? 1 : 0);
+  auto it = net->graphs.find(key);
+  cudaGraphExec_t ge = nullptr;
+  if (it == net->graphs.end()) {
+    int rc = capture_graph(net, n_ticks, with_all, &ge);
+    if (rc) return rc;
+    net->graphs[key] = ge;
+  } else {
+    ge = it->second;
+  }
+  CU(cudaGraphLaunch(ge, net->stream));
+  net->launches += (uint64_t)n_ticks + (with_all ? 2u * net->projs.size() : 0u);
+  if (with_all)
+    for (const ProjHost& J : net->projs) net->all_cells += (uint64_t)J.H * J.C * J.M;
+  net->k_total += n_ticks;
+  net->last_run_ticks = n_ticks;
+  return BCPNN_OK;
+}
+
+int bcpnn_sync(bcpnn_net* net) {
+  if (!net) return BCPNN_ERR_INVALID;
+  CU(cudaSetDevice(net->device));
+  CU(cudaStreamSynchronize(net->stream));
+  return check_device_error(net);
+}
+
+int bcpnn_spike_log_words(const bcpnn_net* net, int32_t pop, int32_t* words) {
+  if (!net || !words || pop < 0 || pop >= (int)net->pops.size()) return BCPNN_ERR_INVALID;
+  *words = net->pops[pop].log_words;
+  return BCPNN_OK;
+}
+
+int bcpnn_get_spike_log(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (pop < 0 || pop >= (int)net->pops.size() || !out) return fail(net, BCPNN_ERR_INVALID, "bcpnn_get_spike_log: bad arguments");
+  const PopHost& P = net->pops[pop];
+  size_t need = (size_t)net->last_run_ticks * P.log_words;
+  if (n_words != need) return fail(net, BCPNN_ERR_SIZE, "bcpnn_get_spike_log: n_words != last run ticks * words");
+  CU(cudaSetDevice(net->device));
+  if (need) CU(cudaMemcpyAsync(out, net->log_buf + P.log_offset, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  return check_device_error(net);
+}
+
+int bcpnn_get_ss_flags(bcpnn_net* net, uint8_t* out, size_t n_bytes) {
+  if (!net) return BCPNN_ERR_INVALID;
+  size_t need = (size_t)net->last_run_ticks * net->projs.size();
+  if (!out || n_bytes != need) return fail(net, BCPNN_ERR_SIZE, "bcpnn_get_ss_flags: n_bytes != ticks * projections");
+  CU(cudaSetDevice(net->device));
+  std::vector<uint32_t> w(need);
+  if (need) CU(cudaMemcpyAsync(w.data(), net->h.ss_log, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  for (size_t i = 0; i < need; ++i) out[i] = (uint8_t)w[i];
+  return BCPNN_OK;
+}
+
+int bcpnn_state_info(const bcpnn_net* net, const char* name, int32_t* type, size_t* count) {
+  if (!net || !type || !count) return BCPNN_ERR_INVALID;
+  Resolved r;
+  if (!resolve(net, name, &r)) return BCPNN_ERR_NOT_FOUND;
+  *type = r.type;
+  *count = r.count;
+  return BCPNN_OK;
+}
+
+int bcpnn_read_state(bcpnn_net* net, const char* name, void* host, size_t bytes) {
+  if (!net) return BCPNN_ERR_INVALID;
+  Resolved r;
+  if (!resolve(net, name, &r)) return fail(net, BCPNN_ERR_NOT_FOUND, std::string("unknown state vector ") + (name ? name : "(null)"));
+  if (!host || bytes != r.count * type_size(r.type)) return fail(net, BCPNN_ERR_SIZE, "bcpnn_read_state: size mismatch");
+  CU(cudaSetDevice(net->device));
+  int last = (int)((net->k_total - 1) & 1);  /* buffer written by the last tick (1 before any tick) */
+  switch (r.kind) {
+    case K_PLAIN:
+      CU(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    case K_PARITY:
+    case K_SI:
+      CU(cudaMemcpyAsync(host, r.par[last], bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    case K_CELL: {
+      int rc = ensure_scratch(net, r.count);
+      if (rc) return rc;
+      cell_gather_kernel<<<grid_for(r.count, 256), 256, 0, net->stream>>>(r.cell, r.count, r.field, net->scratch);
+      CU(cudaGetLastError());
+      net->launches++;
+      CU(cudaMemcpyAsync(host, net->scratch, bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    }
+    case K_SIQ: {
+      const ProjHost& J = net->projs[r.proj];
+      const ProjDev& D = net->h.projs[r.proj];
+      std::vector<int> cnt(J.H), list((size_t)J.H * J.C);
+      CU(cudaMemcpyAsync(cnt.data(), D.list_cnt, J.H * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+      CU(cudaMemcpyAsync(list.data(), D.list, list.size() * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+      CU(cudaStreamSynchronize(net->stream));
+      int8_t* o = (int8_t*)host;
+      std::memset(o, 0, bytes);
+      for (int hh = 0; hh < J.H; ++hh)
+        for (int e = 0; e < cnt[hh] && e < J.C; ++e) {
+          int row = list[(size_t)hh * J.C + e];
+          if (row >= 0 && (size_t)row < r.count) o[row] = 1;
+        }
+      break;
+    }
+  }
+  CU(cudaStreamSynchronize(net->stream));
+  return BCPNN_OK;
+}
+
+int bcpnn_write_state(bcpnn_net* net, const char* name, const void* host, size_t bytes) {
+  if (!net) return BCPNN_ERR_INVALID;
+  Resolved r;
+  if (!resolve(net, name, &r)) return fail(net, BCPNN_ERR_NOT_FOUND, std::string("unknown state vector ") + (name ? name : "(null)"));
+  if (!host || bytes != r.count * type_size(r.type)) return fail(net, BCPNN_ERR_SIZE, "bcpnn_write_state: size mismatch");
+  CU(cudaSetDevice(net->device));
+  int last = (int)((net->k_total - 1) & 1);
+  switch (r.kind) {
+    case K_PLAIN:
+      CU(cudaMemcpyAsync(r.ptr, host, bytes, cudaMemcpyHostToDevice, net->stream));
+      break;
+    case K_PARITY:
+    case K_SI:
+      CU(cudaMemcpyAsync(r.par[last], host, bytes, cudaMemcpyHostToDevice, net->stream));
+      break;
+    case K_CELL: {
+      int rc = ensure_scratch(net, r.count);
+      if (rc) return rc;
+      CU(cudaMemcpyAsync(net->scratch, host, bytes, cudaMemcpyHostToDevice, net->stream));
+      cell_scatter_kernel<<<grid_for(r.count, 256), 256, 0, net->stream>>>(r.cell, r.count, r.field, net->scratch);
+      CU(cudaGetLastError());
+      net->launches++;
+      break;
+    }
+    case K_SIQ: {
+      const ProjHost& J = net->projs[r.proj];
+      const ProjDev& D = net->h.projs[r.proj];
+      const int8_t* in = (const int8_t*)host;
+      std::vector<int> cnt(J.H, 0), list((size_t)J.H * J.C, 0);
+      for (int hh = 0; hh < J.H; ++hh)
+        for (int s = 0; s < J.C; ++s)
+          if (in[(size_t)hh * J.C + s] > 0) list[(size_t)hh * J.C + cnt[hh]++] = hh * J.C + s;
+      CU(cudaMemcpyAsync(D.list_cnt, cnt.data(), J.H * sizeof(int), cudaMemcpyHostToDevice, net->stream));
+      CU(cudaMemcpyAsync(D.list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, net->stream));
+      break;
+    }
+  }
+  CU(cudaStreamSynchronize(net->stream));
+  return BCPNN_OK;
+}
+
+int bcpnn_counters(bcpnn_net* net, uint64_t out[3]) {
+  if (!net || !out) return BCPNN_ERR_INVALID;
+  CU(cudaSetDevice(net->device));
+  unsigned long long c[3];
+  CU(cudaMemcpyAsync(c, net->h.counters, sizeof(c), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  /* the all-cells sweep is counted on the host: every cell of every
+     projection per sweep (Proj.cpp:558-586 loops over all of them) */
+  out[0] = c[0];
+  out[1] = c[1];
+  out[2] = net->all_cells;
+  return BCPNN_OK;
+}
+
+int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out) {
+  if (!net || !out) return BCPNN_ERR_INVALID;
+  *out = net->launches;
+  return BCPNN_OK;
+}
+
+}  // extern "C"

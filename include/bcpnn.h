@@ -1,0 +1,174 @@
+/*
+ * bcpnn.h -- C ABI of the B200 BCPNN simulation core (libgsbn_b200.so).
+ *
+ * This is the layer under the drop-in procedures ProcUpdLazy, ProcExchangeSpike
+ * and ProcSpkRec of the C++ engine.  It replaces, for one network held on one
+ * GPU, what gsbn does per tick through Pop/Proj objects, SyncVector mirrors and
+ * per-object CUDA streams (src/gsbn/procedures/ProcUpdLazy.cpp,
+ * ProcUpdLazy/Pop.cpp, ProcUpdLazy/Proj.cpp).  Conventions:
+ *
+ *   - plain C types, caller-owned host buffers, library-owned device buffers;
+ *   - every call returns an int status (BCPNN_OK == 0); no exception crosses
+ *     the boundary; bcpnn_last_error() gives the message of the last failure;
+ *   - one CUDA stream per network handle; a handle is not thread-safe;
+ *   - the simulation state keeps the names and the row-major layouts of gsbn's
+ *     Database vectors (dsup_<pop>, pij_<proj>, ... ; row = dest_hcu*C + slot,
+ *     cell = row*M + mcu) at the read/write boundary, whatever the device
+ *     layout is.
+ *
+ * Numerics: plain FP32 with the same expression trees as gsbn's CPU path;
+ * exp/log and the random streams follow include/bcpnn_numerics.h, so a CPU
+ * replay with the same definitions is bit-identical.
+ */
+#ifndef BCPNN_H
+#define BCPNN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define BCPNN_OK 0
+#define BCPNN_ERR_INVALID (-1)   /* bad argument (null pointer, size, index) */
+#define BCPNN_ERR_CUDA (-2)      /* a CUDA runtime call failed               */
+#define BCPNN_ERR_NOT_FOUND (-3) /* unknown state vector name                */
+#define BCPNN_ERR_SIZE (-4)      /* buffer size does not match the vector    */
+#define BCPNN_ERR_STATE (-5)     /* call not valid in the current state      */
+#define BCPNN_ERR_DEVICE (-6)    /* a kernel reported an error word          */
+
+/* element types reported by bcpnn_state_info */
+#define BCPNN_F32 0
+#define BCPNN_I32 1
+#define BCPNN_I8 2
+
+typedef struct bcpnn_net bcpnn_net;
+
+/* One population: gsbn PopParam (src/gsbn/proto/gsbn.proto:38-59) fields used
+   by ProcUpdLazy/Pop.cpp:17-40. */
+typedef struct bcpnn_pop_desc {
+  int32_t hcu_num;
+  int32_t mcu_num;   /* 1 .. 1024 */
+  float taum;
+  float wtagain;
+  float maxfq;
+  float igain;
+  float wgain;
+  float lgbias;
+  float snoise;
+} bcpnn_pop_desc;
+
+/* One projection: gsbn ProjParam (gsbn.proto:61-74) fields used by
+   ProcUpdLazy/Proj.cpp:16-52. */
+typedef struct bcpnn_proj_desc {
+  int32_t src_pop;
+  int32_t dest_pop;
+  float tauzi;
+  float tauzj;
+  float taue;
+  float taup;
+  float maxfq;
+  float bgain;
+  float wgain;
+  float tauepsc;   /* <= 0 means "not set": tauepsc defaults to tauzi       */
+  float slot_num;  /* float in the schema; dim_conn = min(Hs*Ms, (int)slot) */
+} bcpnn_proj_desc;
+
+typedef struct bcpnn_net_desc {
+  int32_t n_pops;
+  const bcpnn_pop_desc* pops;
+  int32_t n_projs;
+  const bcpnn_proj_desc* projs;
+  float dt;                  /* GenParam.dt                                   */
+  uint32_t seed;             /* Philox key word 0 (ProcUpdLazy argi "seed")   */
+  float poisson_noise_hz;    /* ProcUpdLazy argf "poisson-noise-hz" (0: off)  */
+  int32_t exchange_spikes;   /* 1: ProcExchangeSpike runs every tick          */
+  int32_t device;            /* CUDA device ordinal                           */
+  int32_t max_ticks_per_run; /* capacity of the per-run spike log             */
+} bcpnn_net_desc;
+
+/* Build a network on the device with gsbn's initial values.
+   Replaces ProcUpdLazy::init_new (ProcUpdLazy.cpp:8-46), Pop::init_new
+   (ProcUpdLazy/Pop.cpp:8-65) and Proj::init_new (ProcUpdLazy/Proj.cpp:6-107). */
+int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out);
+
+/* Release every device buffer and the stream of the network. */
+int bcpnn_net_destroy(bcpnn_net* net);
+
+/* Connection table of one projection: ii (source MCU or -1) and di (delay in
+   ticks, 1..31) for all dest_hcu*C slots.  Replaces ProcInitConn::add_row
+   (ProcInitConn.cpp:92-103) writing ii_<proj>/di_<proj>. */
+int bcpnn_set_conn(bcpnn_net* net, int32_t proj, const int32_t* ii, const int32_t* di, size_t n_slots);
+
+/* Stimulus for the following ticks: lginp for every MCU of the network (row
+   lginp-idx of .lginp) and wmask for every HCU (row wmask-idx of .wmask), as
+   ProcExtGen publishes them (ProcExtGen.cpp:126-144) and Pop::update_sup_cpu
+   reads them (ProcUpdLazy/Pop.cpp:327-332). */
+int bcpnn_set_stimulus(bcpnn_net* net, const float* lginp, size_t n_mcu, const float* wmask_row, size_t n_hcu);
+
+/* External spike replay of one population (ProcUpdLazy args "external spike",
+   ProcUpdLazy/Pop.cpp:67-110 and fill_spike :389-409): n entries, entry k
+   overrides the spikes of tick ticks[k] with idx[offsets[k] .. offsets[k+1]).
+   Once set, every tick is overridden (ticks not listed give no spikes). */
+int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* ticks, const int32_t* offsets,
+                         const int32_t* idx);
+
+/* Advance n_ticks ticks with simstep first_simstep, first_simstep+1, ... .
+   prn is the plasticity of every tick of the run; old_prn is the value of
+   GlobalVar "old-prn" at the first tick (an all-cells catch-up runs first when
+   it differs from prn).  Asynchronous on the network's stream.  Replaces
+   ProcUpdLazy::update_gpu (ProcUpdLazy.cpp:128-180) called once per tick,
+   plus the ProcExchangeSpike copy (ProcExchangeSpike.cpp:94-139) when
+   desc->exchange_spikes is set. */
+int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn, float old_prn);
+
+/* Wait for all work queued on the network's stream. */
+int bcpnn_sync(bcpnn_net* net);
+
+/* Number of 32-bit words of one tick of population `pop` in the spike log. */
+int bcpnn_spike_log_words(const bcpnn_net* net, int32_t pop, int32_t* words);
+
+/* Copy the spike log of the last run for population `pop`: n_ticks rows of
+   bcpnn_spike_log_words() words; bit (i & 31) of word (i >> 5) is MCU i of the
+   population (index h*M + m, as ProcSpkRec writes it, ProcSpkRec/Pop.cpp:30-52).
+   Synchronises the stream. */
+int bcpnn_get_spike_log(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words);
+
+/* Per tick of the last run, one byte per projection: bit 0 set if row 9 was in
+   .ssi_<proj>, bit 1 if MCU 9 was in .ssj_<proj> (the debug flags ProcSpkRec
+   writes to ssi_pop_/ssj_pop_<proj>.csv, ProcSpkRec/Prj.cpp:95-138).  out has
+   n_ticks * n_projs bytes, tick-major. */
+int bcpnn_get_ss_flags(bcpnn_net* net, uint8_t* out, size_t n_bytes);
+
+/* Size and element type of a named state vector (gsbn Database names, e.g.
+   "pij_0", "dsup_1", "spike_0", ".counter_0"). */
+int bcpnn_state_info(const bcpnn_net* net, const char* name, int32_t* type, size_t* count);
+
+/* Copy a named state vector to / from host memory in gsbn's layout.  Replaces
+   Database::sync_vector_* + SyncVector::cpu_data/mutable_cpu_data
+   (include/gsbn/Database.hpp, src/gsbn/SyncVector.cu:277-322).
+   Synchronises the stream. */
+int bcpnn_read_state(bcpnn_net* net, const char* name, void* host, size_t bytes);
+int bcpnn_write_state(bcpnn_net* net, const char* name, const void* host, size_t bytes);
+
+/* Cumulative cell updates since creation: out[0] row cells, out[1] column
+   cells (active post MCUs x dim_conn, as gsbn's column loop counts them),
+   out[2] all-cells catch-up cells.  Synchronises the stream. */
+int bcpnn_counters(bcpnn_net* net, uint64_t out[3]);
+
+/* Number of kernels this library launched for the network since creation. */
+int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out);
+
+/* Message of the last failing call on this handle ("" if none). */
+const char* bcpnn_last_error(const bcpnn_net* net);
+
+/* Static description of a status code. */
+const char* bcpnn_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BCPNN_H */
