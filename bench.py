@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Throughput of the ProcUpdLazy hot path (+ spike recording) on B200.
+
+Workload: the 100x100 HCU/MCU network with a recurrent projection at HCU
+density 0.1 (C = 1000 slots per destination HCU, 1e7 synaptic cells), 100
+seeded one-MCU-per-HCU patterns trained 100 ticks each (1e4 ticks, prn 1)
+followed by 100 recalls of 100 ticks with 30% of the HCUs cued (1e4 ticks,
+prn 0): 2e4 ticks, 200 stimulus segments.  Synthetic inputs follow the
+reference's generator conventions (gsbn_b200/workloads.py); no dataset.
+
+A step is one full pass of that schedule from the network's initial state:
+bcpnn_reset, then one bcpnn_run per segment.  `value` is synaptic updates/s
+(row + column + all-cells cell updates, counted by the kernels) over K steps,
+timed with CUDA events on the library's stream, stimulus rows already
+resident in HBM.  `e2e` is the same metric through the C ABI with host
+buffers: per segment the stimulus is copied from pinned host memory and the
+segment's spike log is read back, and ProcCheck's recall evaluation runs on
+the host.  The network state (~0.5 GB) is larger than L2, so no flush is
+needed between steps.
+
+--impl reference times the CPU oracle (a restatement of gsbn's
+single-threaded ProcUpdLazy CPU path; the reference itself cannot be built
+here) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM traffic of tick_kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "tick_kernel_100x100.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, device):
+        self.samples = []
+        self.proc = None
+        self.device = device
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and s[3 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_schedule(work_dir):
+    """Workload files, network description, connectivity and the segment
+    schedule (identical for every step), with product-side helpers only: the
+    prototxt is parsed by the protobuf runtime, the ProcInitConn map by
+    gsbn_b200.workloads, the schedule by gsbn_b200.extgen."""
+    from gsbn_b200 import extgen, schema, workloads
+    w = workloads.config1()
+    sp, path = w.solver_param(work_dir)
+    pops, projs = workloads.net_from_solver_param(sp)
+    stim = schema.read_stim(sp.gen_param.stim_file)
+    conn = workloads.read_conn_map(w.conn, pops, projs)
+    runs = extgen.segments(sp)
+    return w, sp, pops, projs, stim, conn, runs
+
+
+def algorithmic_bytes(pops, projs, row_cells, col_cells, ticks):
+    """Bytes the reference algorithm must move per tick, summed: 44 B per row
+    cell, 40 B per column cell, 16 B per slot of the delay queue, 24 B per
+    j-trace MCU per projection and 8*dim_proj + 25 B per MCU of the
+    population update."""
+    n_mcu = sum(p["hcu_num"] * p["mcu_num"] for p in pops)
+    slots = sum(pops[q["dest_pop"]]["hcu_num"] * min(pops[q["src_pop"]]["hcu_num"] * pops[q["src_pop"]]["mcu_num"],
+                                                    int(q["slot_num"])) for q in projs)
+    per_tick = n_mcu * (8 * len(projs) + 25) + 24 * n_mcu * len(projs) + 16 * slots
+    return 44 * row_cells + 40 * col_cells + per_tick * ticks
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from gsbn_b200 import capi
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    work = tempfile.mkdtemp(prefix=f"gsbn_bench_{rank}_")
+    from gsbn_b200 import extgen
+    w, sp, pops, projs, stim, conn, runs = build_schedule(work)
+    seed = w.meta["seed"]
+    eps = float(np.float32(sp.gen_param.eps))
+    net = capi.Net(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed, device=dev, max_ticks=128)
+    for k, (ii, di) in enumerate(conn):
+        net.set_conn(k, ii, di)
+    # device-resident stimulus: every lgidx row -> lginp row, every wmask row
+    lgidx, wmask = extgen.stim_tables(stim)
+    net.upload_stimuli_idx(lgidx, eps, wmask)
+    stream = torch.cuda.ExternalStream(net.stream(), device=dev)
+    n_ticks = sum(r.n for r in runs)
+
+    def step(events=None):
+        net.reset()
+        for i, r in enumerate(runs):
+            net.use_stimulus(r.lgidx, r.wmask)
+            if events is not None:
+                events[i][0].record(stream)
+            net.run(r.first, r.n, r.prn, r.old_prn)
+            if events is not None:
+                events[i][1].record(stream)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    net.sync()
+    c0 = sum(net.counters())
+    l0 = net.kernel_launches()
+    per_run = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in runs]
+               for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(dev) as clk:
+        start.record(stream)
+        for s in range(args.steps):
+            step(per_run[s])
+        stop.record(stream)
+        net.sync()
+        torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(stop)
+    cells = sum(net.counters()) - c0
+    launches = net.kernel_launches() - l0
+    row, col, allc = net.counters()
+    # tick-kernel time: runs without an all-cells sweep contain only tick kernels
+    tk_ms, tk_ticks = 0.0, 0
+    for s in range(args.steps):
+        for i, r in enumerate(runs):
+            if r.prn == r.old_prn:
+                tk_ms += per_run[s][i][0].elapsed_time(per_run[s][i][1])
+                tk_ticks += r.n
+    tick_us = tk_ms * 1e3 / max(1, tk_ticks)
+    if world > 1:
+        t = torch.tensor([ms, float(cells)], dtype=torch.float64, device=f"cuda:{dev}")
+        mx = t.clone()
+        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
+        ms, cells = float(mx[0]), float(t[1])
+
+    # e2e: host buffers through the C ABI, spike logs read back, recall on host
+    pin_lg = [torch.empty(lgidx.shape[1], dtype=torch.int32, pin_memory=True).numpy() for r in runs]
+    pin_wm = [torch.empty(wmask.shape[1], dtype=torch.float32, pin_memory=True).numpy() for r in runs]
+    for i, r in enumerate(runs):
+        pin_lg[i][:] = lgidx[r.lgidx]
+        pin_wm[i][:] = wmask[r.wmask]
+    words = (pops[0]["hcu_num"] * pops[0]["mcu_num"] + 31) // 32
+    pin_log = [torch.empty((r.n, words), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32) for r in runs]
+    h2d = sum(a.nbytes + b.nbytes for a, b in zip(pin_lg, pin_wm))
+    d2h = sum(a.nbytes for a in pin_log)
+    lib = capi.load()
+
+    def e2e_step():
+        net.reset()
+        for i, r in enumerate(runs):
+            net._check(lib.bcpnn_set_stimulus_idx(net._h, capi._ptr(pin_lg[i]), pin_lg[i].size, eps,
+                                                  capi._ptr(pin_wm[i]), pin_wm[i].size))
+            net.run(r.first, r.n, r.prn, r.old_prn)
+            net._check(lib.bcpnn_get_spike_log(net._h, 0, capi._ptr(pin_log[i]), pin_log[i].size))
+        return extgen.recall(sp, lgidx, [(p["hcu_num"], p["mcu_num"]) for p in pops], runs,
+                             [[lg] for lg in pin_log])
+
+    recall = e2e_step()
+    net.sync()
+    e0 = sum(net.counters())
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        recall = e2e_step()
+    net.sync()
+    e_s = time.perf_counter() - t0
+    e_cells = sum(net.counters()) - e0
+    if world > 1:
+        t = torch.tensor([e_s, float(e_cells)], dtype=torch.float64, device=f"cuda:{dev}")
+        mx = t.clone()
+        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
+        e_s, e_cells = float(mx[0]), float(t[1])
+
+    out = None
+    if rank == 0:
+        pk, pk_kind = peaks()
+        row_step = row / (args.warmup + args.steps + 0.0)
+        # per tick-kernel launch (steady state): bytes of one average tick
+        per_step_row = row_step
+        per_step_col = col / (args.warmup + args.steps + 0.0)
+        bytes_per_tick = algorithmic_bytes(pops, projs, per_step_row, per_step_col, n_ticks) / n_ticks
+        achieved = bytes_per_tick / (tick_us * 1e-6) / 1e9
+        value = cells / (ms / 1e3)
+        out = {
+            "metric": "synaptic updates/s", "value": value, "unit": "cell updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded patterns and connectivity, gen_rnd.py conventions)",
+            "config": {"workload": "100x100 HCU/MCU, recurrent HCU density 0.1 (C=1000, 1e7 cells), 100 patterns: "
+                                   "1e4 training + 1e4 recall ticks per step",
+                       "ticks_per_step": n_ticks, "segments_per_step": len(runs),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "state 0.5 GB > 126 MB L2, no flush"},
+            "ticks_per_s": n_ticks * args.steps * world / (ms / 1e3),
+            "recall": f"{recall[0]}/{recall[1]}",
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "tick_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_kind": pk_kind,
+                         "traffic": profile_traffic(), "us_per_launch": tick_us,
+                         "algorithmic_bytes_per_launch": bytes_per_tick},
+            "e2e": {"value": e_cells / e_s, "unit": "cell updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e_s * 1e3 / args.steps},
+            "clocks": clk.summary(),
+        }
+    net.close()
+    return out
+
+
+def cpu_sample(sample_ticks=600):
+    """The oracle on a bounded sample of the workload: the first
+    `sample_ticks` training ticks (with the start-of-run all-cells pass), then
+    the training->recall all-cells catch-up and `sample_ticks // 2` recall
+    ticks.  Returns cells/s scaled to the full step by the phase rates."""
+    from gsbn_b200 import workloads
+    from oracle import sim
+    from tests.harness import load_workload, schedule
+    work = tempfile.mkdtemp(prefix="gsbn_cpu_")
+    sp, pops, projs, stim, conn, seed, phz = load_workload(workloads.config1(), work)
+    orc = sim.OracleNet(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed)
+    for k, (ii, di) in enumerate(conn):
+        orc.set_conn(k, ii, di)
+    runs = schedule(sp, stim, pops, orc.logf)
+    train = [r for r in runs if r.prn != 0.0]
+    recall = [r for r in runs if r.prn == 0.0]
+
+    def timed(rs, limit):
+        c0, t0, done = sum(orc.counters()), time.perf_counter(), 0
+        for r in rs:
+            n = min(r.n, limit - done)
+            if n <= 0:
+                break
+            orc.set_stimulus(r.lginp, r.wmask)
+            orc.run(r.first, n, r.prn, r.old_prn, spikes=False)
+            done += n
+        return time.perf_counter() - t0, sum(orc.counters()) - c0, done
+
+    def phase(rs, limit):
+        # the first tick carries the phase's all-cells catch-up: timed alone
+        head = [type(rs[0])(rs[0].first, 1, rs[0].prn, rs[0].old_prn, rs[0].lginp, rs[0].wmask, None)]
+        tail = [type(rs[0])(rs[0].first + 1, rs[0].n - 1, rs[0].prn, rs[0].prn, rs[0].lginp, rs[0].wmask, None)]
+        t1, c1, _ = timed(head, 1)
+        t2, c2, n2 = timed(tail + rs[1:], limit - 1)
+        total = sum(r.n for r in rs)
+        return t1 + t2 / n2 * (total - 1), c1 + c2 / n2 * (total - 1), t1 + t2, 1 + n2
+
+    t_tr, c_tr, s_tr, n_tr = phase(train, sample_ticks)
+    t_rc, c_rc, s_rc, n_rc = phase(recall, sample_ticks // 2)
+    sample = (f"{n_tr} training ticks + {n_rc} recall ticks of the 100x100 workload, including both all-cells "
+              f"catch-ups, {s_tr + s_rc:.1f} s of CPU; per-tick rates scaled to the 2e4-tick step")
+    return (c_tr + c_rc) / (t_tr + t_rc), sample, s_tr + s_rc
+
+
+def run_reference(args):
+    """The reference arm: the single-threaded CPU path (oracle restatement)."""
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(args.ref_ticks)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, sample, _ = cpu_sample(args.ref_ticks)
+        vals.append(v)
+    elapsed = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    return {
+        "metric": "synaptic updates/s", "value": value, "unit": "cell updates/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded patterns and connectivity, gen_rnd.py conventions)", "impl": "reference",
+        "config": {"workload": "100x100 HCU/MCU, recurrent HCU density 0.1 (C=1000, 1e7 cells), 100 patterns: "
+                               "1e4 training + 1e4 recall ticks per step"},
+        "cpu_baseline": {"value": value, "unit": "cell updates/s", "cores": 1, "kind": "port", "sample": sample,
+                         "cpu": cpu_model()},
+        "e2e": {"value": value, "unit": "cell updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-ticks", type=int, default=400)
+    ap.add_argument("--cpu-ticks", type=int, default=1200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            v, sample, secs = cpu_sample(args.cpu_ticks)
+            out["cpu_baseline"] = {"value": v, "unit": "cell updates/s", "cores": 1, "kind": "port",
+                                   "sample": sample, "cpu": cpu_model()}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -17,7 +17,8 @@ _NP = {F32: np.float32, I32: np.int32, I8: np.int8}
 
 # every entry point declared in include/bcpnn.h
 EXPORTS = (
-    "bcpnn_net_create", "bcpnn_net_destroy", "bcpnn_set_conn", "bcpnn_set_stimulus", "bcpnn_set_ext_spikes",
+    "bcpnn_net_create", "bcpnn_net_destroy", "bcpnn_set_conn", "bcpnn_set_stimulus", "bcpnn_upload_stimuli",
+    "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
     "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_ss_flags",
     "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_counters", "bcpnn_kernel_launches",
     "bcpnn_last_error", "bcpnn_status_string",
@@ -68,7 +69,13 @@ def load():
         "bcpnn_net_destroy": (ctypes.c_int, [vp]),
         "bcpnn_set_conn": (ctypes.c_int, [vp, i32, vp, vp, sz]),
         "bcpnn_set_stimulus": (ctypes.c_int, [vp, vp, sz, vp, sz]),
+        "bcpnn_upload_stimuli": (ctypes.c_int, [vp, i32, vp, i32, vp]),
+        "bcpnn_use_stimulus": (ctypes.c_int, [vp, i32, i32]),
+        "bcpnn_set_stimulus_idx": (ctypes.c_int, [vp, vp, sz, ctypes.c_float, vp, sz]),
+        "bcpnn_upload_stimuli_idx": (ctypes.c_int, [vp, i32, vp, ctypes.c_float, i32, vp]),
         "bcpnn_set_ext_spikes": (ctypes.c_int, [vp, i32, i32, vp, vp, vp]),
+        "bcpnn_reset": (ctypes.c_int, [vp]),
+        "bcpnn_get_stream": (ctypes.c_int, [vp, P(vp)]),
         "bcpnn_run": (ctypes.c_int, [vp, i32, i32, ctypes.c_float, ctypes.c_float]),
         "bcpnn_sync": (ctypes.c_int, [vp]),
         "bcpnn_spike_log_words": (ctypes.c_int, [vp, i32, P(i32)]),
@@ -138,6 +145,32 @@ class Net:
         lg = np.ascontiguousarray(lginp, dtype=np.float32)
         wm = np.ascontiguousarray(wmask_row, dtype=np.float32)
         self._check(self._lib.bcpnn_set_stimulus(self._h, _ptr(lg), lg.size, _ptr(wm), wm.size))
+
+    def upload_stimuli(self, lginp_rows, wmask_rows):
+        lg = np.ascontiguousarray(lginp_rows, dtype=np.float32)
+        wm = np.ascontiguousarray(wmask_rows, dtype=np.float32)
+        self._check(self._lib.bcpnn_upload_stimuli(self._h, lg.shape[0], _ptr(lg), wm.shape[0], _ptr(wm)))
+
+    def set_stimulus_idx(self, lgidx_row, eps, wmask_row):
+        lg = np.ascontiguousarray(lgidx_row, dtype=np.int32)
+        wm = np.ascontiguousarray(wmask_row, dtype=np.float32)
+        self._check(self._lib.bcpnn_set_stimulus_idx(self._h, _ptr(lg), lg.size, eps, _ptr(wm), wm.size))
+
+    def upload_stimuli_idx(self, lgidx_rows, eps, wmask_rows):
+        lg = np.ascontiguousarray(lgidx_rows, dtype=np.int32)
+        wm = np.ascontiguousarray(wmask_rows, dtype=np.float32)
+        self._check(self._lib.bcpnn_upload_stimuli_idx(self._h, lg.shape[0], _ptr(lg), eps, wm.shape[0], _ptr(wm)))
+
+    def use_stimulus(self, lginp_row, wmask_row):
+        self._check(self._lib.bcpnn_use_stimulus(self._h, lginp_row, wmask_row))
+
+    def reset(self):
+        self._check(self._lib.bcpnn_reset(self._h))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self._lib.bcpnn_get_stream(self._h, ctypes.byref(s)))
+        return s.value
 
     def set_ext_spikes(self, pop, table):
         """table: dict tick -> list of MCU indices."""

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -67,10 +68,16 @@ struct bcpnn_net {
   int64_t k_total = 0;      /* ticks executed since creation */
   int last_run_ticks = 0;
   bool exchange = false;
+  bool direct = false;      /* GSBN_DIRECT_LAUNCH=1: launch kernels one by one (profilers) */
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   uint64_t launches = 0;
   uint64_t all_cells = 0;   /* cells swept by all-cells catch-ups */
   uint64_t stamp = 0;
+  float* stim_lg = nullptr; /* device stimulus tables (bcpnn_upload_stimuli) */
+  float* stim_wm = nullptr;
+  int stim_lg_rows = 0, stim_wm_rows = 0;
+  const float* cur_lg = nullptr; /* stimulus of the next run */
+  const float* cur_wm = nullptr;
   float* scratch = nullptr; /* staging for strided cell fields */
   size_t scratch_n = 0;
   std::string err;
@@ -96,14 +103,6 @@ int dalloc(bcpnn_net* net, T** p, size_t count) {
   if (count == 0) count = 1;
   CU(cudaMalloc((void**)p, count * sizeof(T)));
   net->allocs.push_back((void*)*p);
-  return BCPNN_OK;
-}
-
-template <typename T>
-int dfill(bcpnn_net* net, T* p, size_t count, T value) {
-  std::vector<T> v(count, value);
-  CU(cudaMemcpyAsync(p, v.data(), count * sizeof(T), cudaMemcpyHostToDevice, net->stream));
-  CU(cudaStreamSynchronize(net->stream));
   return BCPNN_OK;
 }
 
@@ -182,9 +181,64 @@ int prepare_tables(bcpnn_net* net, int p, float prn, float old_prn, bool with_al
   return BCPNN_OK;
 }
 
-int capture_graph(bcpnn_net* net, int n_ticks, bool with_all, cudaGraphExec_t* out) {
-  cudaGraph_t g = nullptr;
-  CU(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+template <typename T>
+int dset(bcpnn_net* net, T* p, size_t n, T v) {
+  if (n == 0) return BCPNN_OK;
+  fill_kernel<T><<<grid_for(n, 256), 256, 0, net->stream>>>(p, n, v);
+  CU(cudaGetLastError());
+  net->launches++;
+  return BCPNN_OK;
+}
+
+int dzero(bcpnn_net* net, void* p, size_t bytes) {
+  if (bytes) CU(cudaMemsetAsync(p, 0, bytes, net->stream));
+  return BCPNN_OK;
+}
+
+/* gsbn's initial values (Pop.cpp:59-65, Proj.cpp:88-105) for every state
+   vector; connectivity (ii, di), stimulus and replay tables are kept. */
+int reset_state(bcpnn_net* net) {
+  int rc;
+  NetDev& H = net->h;
+  for (size_t p = 0; p < net->pops.size(); ++p) {
+    const PopHost& P = net->pops[p];
+    PopDev& D = H.pops[p];
+    size_t n = P.n, ne = n * std::max(1, P.dim_proj);
+    for (int b = 0; b < 2; ++b) {
+      if ((rc = dset(net, D.dsup[b], n, (float)bx_log_d(1.0 / P.M)))) return rc;   /* log(1.0/M), Pop.cpp:59 */
+      if ((rc = dzero(net, D.epsc[b], ne * sizeof(float)))) return rc;
+      if ((rc = dzero(net, D.bj[b], ne * sizeof(float)))) return rc;
+    }
+    if ((rc = dset(net, D.act, n, (float)(1.0 / P.M)))) return rc;                 /* Pop.cpp:60 */
+    if ((rc = dzero(net, D.spike, n))) return rc;
+    if ((rc = dzero(net, D.counter, n * sizeof(int)))) return rc;
+  }
+  for (size_t q = 0; q < net->projs.size(); ++q) {
+    const ProjHost& J = net->projs[q];
+    ProjDev& D = H.projs[q];
+    size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
+    if ((rc = dzero(net, D.qi, R * sizeof(int)))) return rc;
+    if ((rc = dset(net, D.pi, R, (float)(1.0 / J.C)))) return rc;                  /* Proj.cpp:91 */
+    if ((rc = dzero(net, D.ei, R * sizeof(float)))) return rc;
+    if ((rc = dzero(net, D.zi, R * sizeof(float)))) return rc;
+    if ((rc = dzero(net, D.ti, R * sizeof(int)))) return rc;
+    if ((rc = dset(net, D.pj, HM, (float)(1.0 / J.M)))) return rc;                 /* Proj.cpp:96 */
+    if ((rc = dzero(net, D.ej, HM * sizeof(float)))) return rc;
+    if ((rc = dzero(net, D.zj, HM * sizeof(float)))) return rc;
+    float pij0 = (float)(1.0 / J.C / J.M);                                         /* Proj.cpp:99 */
+    if ((rc = dset(net, D.cell, cells, make_float4(pij0, 0.0f, 0.0f, 0.0f)))) return rc;
+    if ((rc = dzero(net, D.tij, cells * sizeof(int)))) return rc;
+    if ((rc = dzero(net, D.wij, cells * sizeof(float)))) return rc;
+    if ((rc = dzero(net, D.si[0], (size_t)J.Ns))) return rc;
+    if ((rc = dzero(net, D.si[1], (size_t)J.Ns))) return rc;
+    if ((rc = dzero(net, D.list_cnt, (size_t)J.H * sizeof(int)))) return rc;
+  }
+  net->k_total = 0;
+  return BCPNN_OK;
+}
+
+/* the work of one run, queued on the network's stream */
+void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
   for (const PopHost& P : net->pops)
     cudaMemsetAsync(net->log_buf + P.log_offset, 0, (size_t)n_ticks * P.log_words * sizeof(uint32_t), net->stream);
   cudaMemsetAsync(net->h.ss_log, 0, (size_t)n_ticks * net->h.n_projs * sizeof(uint32_t), net->stream);
@@ -198,6 +252,12 @@ int capture_graph(bcpnn_net* net, int n_ticks, bool with_all, cudaGraphExec_t* o
   size_t smem = tick_smem_bytes(net->max_m);
   for (int it = 0; it < n_ticks; ++it)
     tick_kernel<<<net->total_hcu, kBlock, smem, net->stream>>>(net->d_net, net->d_rp, it, net->max_m);
+}
+
+int capture_graph(bcpnn_net* net, int n_ticks, bool with_all, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_run(net, n_ticks, with_all);
   cudaError_t le = cudaGetLastError();
   cudaError_t ce = cudaStreamEndCapture(net->stream, &g);
   if (le != cudaSuccess) {
@@ -328,6 +388,10 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   net->device = desc->device;
   net->max_ticks = desc->max_ticks_per_run;
   net->exchange = desc->exchange_spikes != 0;
+  {
+    const char* e = std::getenv("GSBN_DIRECT_LAUNCH");
+    net->direct = e && e[0] == '1';
+  }
   std::memset(&net->h, 0, sizeof(NetDev));
   std::memset(&net->rp, 0, sizeof(RunParams));
   int rc = BCPNN_OK;
@@ -410,8 +474,6 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   float* wm = nullptr;
   if ((rc = dalloc(net, &lg, net->total_mcu))) return bail(rc);
   if ((rc = dalloc(net, &wm, net->total_hcu))) return bail(rc);
-  if ((rc = dfill(net, lg, net->total_mcu, 0.0f))) return bail(rc);
-  if ((rc = dfill(net, wm, net->total_hcu, 0.0f))) return bail(rc);
   H.lginp = lg;
   H.wmask = wm;
 
@@ -434,16 +496,10 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
       if ((rc = dalloc(net, &D.epsc[b], ne))) return bail(rc);
       if ((rc = dalloc(net, &D.bj[b], ne))) return bail(rc);
       /* dsup = log(1.0/M) in double, stored as float (Pop.cpp:59) */
-      if ((rc = dfill(net, D.dsup[b], n, (float)bx_log_d(1.0 / P.M)))) return bail(rc);
-      if ((rc = dfill(net, D.epsc[b], ne, 0.0f))) return bail(rc);
-      if ((rc = dfill(net, D.bj[b], ne, 0.0f))) return bail(rc);
     }
     if ((rc = dalloc(net, &D.act, n))) return bail(rc);
-    if ((rc = dfill(net, D.act, n, (float)(1.0 / P.M)))) return bail(rc);   /* Pop.cpp:60 */
     if ((rc = dalloc(net, &D.spike, n))) return bail(rc);
-    if ((rc = dfill(net, D.spike, n, (int8_t)0))) return bail(rc);
     if ((rc = dalloc(net, &D.counter, n))) return bail(rc);
-    if ((rc = dfill(net, D.counter, n, 0))) return bail(rc);
     D.spk_log = net->log_buf + P.log_offset;
     D.log_words = P.log_words;
     D.n_in = (int)P.in_proj.size();
@@ -507,24 +563,19 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     if ((rc = dalloc(net, &D.si[1], J.Ns))) return bail(rc);
     if ((rc = dalloc(net, &D.list, R))) return bail(rc);
     if ((rc = dalloc(net, &D.list_cnt, J.H))) return bail(rc);
-    if ((rc = dfill(net, D.ii, R, -1))) return bail(rc);                          /* Proj.cpp:88 */
-    if ((rc = dfill(net, D.di, R, 0))) return bail(rc);
-    if ((rc = dfill(net, D.qi, R, 0))) return bail(rc);
-    if ((rc = dfill(net, D.pi, R, (float)(1.0 / J.C)))) return bail(rc);          /* Proj.cpp:91 */
-    if ((rc = dfill(net, D.ei, R, 0.0f))) return bail(rc);
-    if ((rc = dfill(net, D.zi, R, 0.0f))) return bail(rc);
-    if ((rc = dfill(net, D.ti, R, 0))) return bail(rc);
-    if ((rc = dfill(net, D.pj, HM, (float)(1.0 / J.M)))) return bail(rc);         /* Proj.cpp:96 */
-    if ((rc = dfill(net, D.ej, HM, 0.0f))) return bail(rc);
-    if ((rc = dfill(net, D.zj, HM, 0.0f))) return bail(rc);
     float pij0 = (float)(1.0 / J.C / J.M);                                         /* Proj.cpp:99 */
-    if ((rc = dfill(net, D.cell, cells, make_float4(pij0, 0.0f, 0.0f, 0.0f)))) return bail(rc);
-    if ((rc = dfill(net, D.tij, cells, 0))) return bail(rc);
-    if ((rc = dfill(net, D.wij, cells, 0.0f))) return bail(rc);
-    if ((rc = dfill(net, D.si[0], (size_t)J.Ns, (int8_t)0))) return bail(rc);
-    if ((rc = dfill(net, D.si[1], (size_t)J.Ns, (int8_t)0))) return bail(rc);
-    if ((rc = dfill(net, D.list_cnt, (size_t)J.H, 0))) return bail(rc);
   }
+  for (int q = 0; q < desc->n_projs; ++q) {
+    const ProjHost& J = net->projs[q];
+    size_t R = (size_t)J.H * J.C;
+    if ((rc = dset(net, H.projs[q].ii, R, -1))) return bail(rc);                   /* Proj.cpp:88 */
+    if ((rc = dzero(net, H.projs[q].di, R * sizeof(int)))) return bail(rc);
+  }
+  if ((rc = dzero(net, lg, (size_t)net->total_mcu * sizeof(float)))) return bail(rc);
+  if ((rc = dzero(net, wm, (size_t)net->total_hcu * sizeof(float)))) return bail(rc);
+  net->cur_lg = lg;
+  net->cur_wm = wm;
+  if ((rc = reset_state(net))) return bail(rc);
   /* CTA -> (population, HCU) */
   {
     std::vector<int> cp, ch;
@@ -572,6 +623,8 @@ int bcpnn_net_destroy(bcpnn_net* net) {
       if (s.ptr) cudaFree(s.ptr);
   for (void* p : net->allocs) cudaFree(p);
   if (net->scratch) cudaFree(net->scratch);
+  if (net->stim_lg) cudaFree(net->stim_lg);
+  if (net->stim_wm) cudaFree(net->stim_wm);
   if (net->stream) cudaStreamDestroy(net->stream);
   delete net;
   return BCPNN_OK;
@@ -602,8 +655,88 @@ int bcpnn_set_stimulus(bcpnn_net* net, const float* lginp, size_t n_mcu, const f
   if (n_mcu != (size_t)net->total_mcu || n_hcu != (size_t)net->total_hcu)
     return fail(net, BCPNN_ERR_SIZE, "bcpnn_set_stimulus: sizes must be total MCUs and total HCUs");
   CU(cudaSetDevice(net->device));
-  CU(cudaMemcpyAsync((void*)net->h.lginp, lginp, n_mcu * sizeof(float), cudaMemcpyHostToDevice, net->stream));
-  CU(cudaMemcpyAsync((void*)net->h.wmask, wmask_row, n_hcu * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  CU(cudaMemcpyAsync(net->h.lginp, lginp, n_mcu * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  CU(cudaMemcpyAsync(net->h.wmask, wmask_row, n_hcu * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  net->cur_lg = net->h.lginp;
+  net->cur_wm = net->h.wmask;
+  return BCPNN_OK;
+}
+
+int bcpnn_upload_stimuli(bcpnn_net* net, int32_t n_lginp_rows, const float* lginp_rows, int32_t n_wmask_rows,
+                         const float* wmask_rows) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (n_lginp_rows <= 0 || n_wmask_rows <= 0 || !lginp_rows || !wmask_rows)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_upload_stimuli: empty tables");
+  CU(cudaSetDevice(net->device));
+  CU(cudaStreamSynchronize(net->stream));
+  if (net->stim_lg) { CU(cudaFree(net->stim_lg)); net->stim_lg = nullptr; }
+  if (net->stim_wm) { CU(cudaFree(net->stim_wm)); net->stim_wm = nullptr; }
+  size_t nl = (size_t)n_lginp_rows * net->total_mcu, nw = (size_t)n_wmask_rows * net->total_hcu;
+  CU(cudaMalloc((void**)&net->stim_lg, nl * sizeof(float)));
+  CU(cudaMalloc((void**)&net->stim_wm, nw * sizeof(float)));
+  CU(cudaMemcpy(net->stim_lg, lginp_rows, nl * sizeof(float), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(net->stim_wm, wmask_rows, nw * sizeof(float), cudaMemcpyHostToDevice));
+  net->stim_lg_rows = n_lginp_rows;
+  net->stim_wm_rows = n_wmask_rows;
+  net->cur_lg = net->h.lginp;
+  net->cur_wm = net->h.wmask;
+  return BCPNN_OK;
+}
+
+int bcpnn_use_stimulus(bcpnn_net* net, int32_t lginp_row, int32_t wmask_row) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (lginp_row < 0 || lginp_row >= net->stim_lg_rows || wmask_row < 0 || wmask_row >= net->stim_wm_rows)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_use_stimulus: row outside the uploaded tables");
+  net->cur_lg = net->stim_lg + (size_t)lginp_row * net->total_mcu;
+  net->cur_wm = net->stim_wm + (size_t)wmask_row * net->total_hcu;
+  return BCPNN_OK;
+}
+
+/* lginp of every MCU from one row of pattern indices (one MCU index per HCU,
+   anything else = no input), ProcExtGen.cpp:130-144: log(1+eps) on the
+   indexed MCU, log(0+eps) elsewhere, float logs as the reference computes
+   them. */
+static void lginp_from_idx(const bcpnn_net* net, const int32_t* lgidx_row, float eps, float* out) {
+  float hit = bx_logf(1 + eps), miss = bx_logf(0 + eps);
+  size_t k = 0;
+  int h = 0;
+  for (const PopHost& P : net->pops)
+    for (int i = 0; i < P.H; ++i, ++h)
+      for (int j = 0; j < P.M; ++j) out[k++] = (lgidx_row[h] == j) ? hit : miss;
+}
+
+int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hcu, float eps, const float* wmask_row,
+                           size_t n_wmask) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (!lgidx_row || !wmask_row) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_stimulus_idx: null buffer");
+  if (n_hcu != (size_t)net->total_hcu || n_wmask != (size_t)net->total_hcu)
+    return fail(net, BCPNN_ERR_SIZE, "bcpnn_set_stimulus_idx: sizes must be total HCUs");
+  std::vector<float> lg(net->total_mcu);
+  lginp_from_idx(net, lgidx_row, eps, lg.data());
+  return bcpnn_set_stimulus(net, lg.data(), lg.size(), wmask_row, n_wmask);
+}
+
+int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
+                             int32_t n_wmask_rows, const float* wmask_rows) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (n_lgidx_rows <= 0 || !lgidx_rows) return fail(net, BCPNN_ERR_INVALID, "bcpnn_upload_stimuli_idx: empty table");
+  std::vector<float> lg((size_t)n_lgidx_rows * net->total_mcu);
+  for (int r = 0; r < n_lgidx_rows; ++r)
+    lginp_from_idx(net, lgidx_rows + (size_t)r * net->total_hcu, eps, lg.data() + (size_t)r * net->total_mcu);
+  return bcpnn_upload_stimuli(net, n_lgidx_rows, lg.data(), n_wmask_rows, wmask_rows);
+}
+
+int bcpnn_reset(bcpnn_net* net) {
+  if (!net) return BCPNN_ERR_INVALID;
+  CU(cudaSetDevice(net->device));
+  int rc = reset_state(net);
+  if (rc) return rc;
+  return BCPNN_OK;
+}
+
+int bcpnn_get_stream(const bcpnn_net* net, void** stream) {
+  if (!net || !stream) return BCPNN_ERR_INVALID;
+  *stream = (void*)net->stream;
   return BCPNN_OK;
 }
 
@@ -688,18 +821,25 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   net->rp.n_ticks = n_ticks;
   net->rp.prn = prn;
   net->rp.old_prn = old_prn;
+  net->rp.lginp = net->cur_lg;
+  net->rp.wmask = net->cur_wm;
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));
-  auto key = std::make_pair(n_ticks, with_all ? 1 : 0);
-  auto it = net->graphs.find(key);
-  cudaGraphExec_t ge = nullptr;
-  if (it == net->graphs.end()) {
-    int rc = capture_graph(net, n_ticks, with_all, &ge);
-    if (rc) return rc;
-    net->graphs[key] = ge;
+  if (net->direct) {
+    enqueue_run(net, n_ticks, with_all);
+    CU(cudaGetLastError());
   } else {
-    ge = it->second;
+    auto key = std::make_pair(n_ticks, with_all ? 1 : 0);
+    auto it = net->graphs.find(key);
+    cudaGraphExec_t ge = nullptr;
+    if (it == net->graphs.end()) {
+      int rc = capture_graph(net, n_ticks, with_all, &ge);
+      if (rc) return rc;
+      net->graphs[key] = ge;
+    } else {
+      ge = it->second;
+    }
+    CU(cudaGraphLaunch(ge, net->stream));
   }
-  CU(cudaGraphLaunch(ge, net->stream));
   net->launches += (uint64_t)n_ticks + (with_all ? 2u * net->projs.size() : 0u);
   if (with_all)
     for (const ProjHost& J : net->projs) net->all_cells += (uint64_t)J.H * J.C * J.M;

@@ -91,8 +91,8 @@ struct NetDev {
   ProjDev projs[kMaxProj];
   const int* cta_pop;   /* CTA -> population */
   const int* cta_hcu;   /* CTA -> HCU        */
-  const float* lginp;   /* [total MCUs] */
-  const float* wmask;   /* [total HCUs] */
+  float* lginp;         /* [total MCUs] host-set stimulus */
+  float* wmask;         /* [total HCUs] */
   uint32_t* ss_log;     /* [max_ticks][n_projs] debug flags of ProcSpkRec */
   unsigned long long* counters; /* row cells, col cells, all cells */
   int* err;
@@ -112,6 +112,8 @@ struct RunParams {
   int k0;         /* ticks executed before the run (parity base) */
   int n_ticks;
   float prn, old_prn;
+  const float* lginp;   /* stimulus of the run: [total MCUs] */
+  const float* wmask;   /* [total HCUs] */
   const float4* tab[kMaxProj];      /* kp = taupdt*prn     */
   const float4* tab_old[kMaxProj];  /* kp = taupdt*old_prn */
   int tab_len[kMaxProj];
@@ -361,8 +363,8 @@ __global__ void __launch_bounds__(kBlock) tick_kernel(const NetDev* __restrict__
   int8_t* s_skip = s_spk + max_m;
 
   /* ---- population update, Pop.cpp:229-323 -------------------------------- */
-  const float* lginp = net->lginp + pop.mcu_start;
-  const float* wmask = net->wmask + pop.hcu_start;
+  const float* lginp = rp->lginp + pop.mcu_start;
+  const float* wmask = rp->wmask + pop.hcu_start;
   const float* epsc_prev = pop.epsc[prev];
   const float* bj_prev = pop.bj[prev];
   const float* dsup_prev = pop.dsup[prev];
@@ -622,6 +624,12 @@ __global__ void __launch_bounds__(kBlock) tick_kernel(const NetDev* __restrict__
     }
     __syncthreads();
   }
+}
+
+/* fill kernels used to (re)initialise the state on the device */
+template <typename T>
+__global__ void fill_kernel(T* p, size_t n, T v) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
 
 /* gather / scatter of one float of the (pij, eij, zi2, zj2) cells */

@@ -244,3 +244,49 @@ def config2(seed=0, record=True, check=True, n_patterns=50, train_ticks=80, reca
         'rec_param { directory: "@REC@" }', procs("@CONN@", seed, poisson_hz, record=record, check=check)]) + "\n"
     meta = dict(patterns=n_patterns, ticks=t, n_cued=n_cued, seed=seed, cells=10 * 25 * 10 + 10 * 10 * 10)
     return Workload("5x10 + 10x10 two projections", text, stim, conn, meta)
+
+
+def net_from_solver_param(sp):
+    """Populations (pop_num copies of each PopParam, ProcUpdLazy.cpp:19-29) and
+    the projections whose source and destination exist (ProcUpdLazy.cpp:35-45),
+    as the dicts gsbn_b200.capi.Net takes."""
+    pops = []
+    for pp in sp.net_param.pop_param:
+        for _ in range(pp.pop_num):
+            pops.append(dict(hcu_num=pp.hcu_num, mcu_num=pp.mcu_num, taum=pp.taum, wtagain=pp.wtagain,
+                             maxfq=pp.maxfq, igain=pp.igain, wgain=pp.wgain, lgbias=pp.lgbias, snoise=pp.snoise))
+    projs = []
+    for q in sp.net_param.proj_param:
+        if q.src_pop < len(pops) and q.dest_pop < len(pops):
+            projs.append(dict(src_pop=q.src_pop, dest_pop=q.dest_pop, tauzi=q.tauzi, tauzj=q.tauzj, taue=q.taue,
+                              taup=q.taup, maxfq=q.maxfq, bgain=q.bgain, wgain=q.wgain,
+                              tauepsc=q.tauepsc if q.HasField("tauepsc") else 0.0, slot_num=q.slot_num))
+    return pops, projs
+
+
+def read_conn_map(text, pops, projs):
+    """(ii, di) slot tables per projection from a ProcInitConn map: every
+    (src_mcu, delay) pair of line `proj,dest_hcu,...` goes to the first empty
+    slot of that HCU, or is dropped when the HCU is full (ProcInitConn.cpp:48-103)."""
+    tables = []
+    for q in projs:
+        s = pops[q["src_pop"]]
+        C = min(s["hcu_num"] * s["mcu_num"], int(q["slot_num"]))
+        H = pops[q["dest_pop"]]["hcu_num"]
+        tables.append([np.full(H * C, -1, np.int32), np.zeros(H * C, np.int32), C, np.zeros(H, np.int64)])
+    for line in text.splitlines():
+        v = line.split(",")
+        if len(v) <= 2:
+            continue
+        ii, di, C, nxt = tables[int(v[0])]
+        h = int(v[1])
+        for i in range(2, len(v) - 1, 2):
+            src = int(v[i])
+            k = nxt[h]
+            while k < C and ii[h * C + k] >= 0:
+                k += 1
+            if k < C:
+                ii[h * C + k] = src
+                di[h * C + k] = int(v[i + 1])
+                nxt[h] = k
+    return [(t[0], t[1]) for t in tables]

@@ -108,6 +108,24 @@ int bcpnn_set_conn(bcpnn_net* net, int32_t proj, const int32_t* ii, const int32_
    reads them (ProcUpdLazy/Pop.cpp:327-332). */
 int bcpnn_set_stimulus(bcpnn_net* net, const float* lginp, size_t n_mcu, const float* wmask_row, size_t n_hcu);
 
+/* Device-resident stimulus tables, uploaded once: n_lginp_rows rows of
+   total-MCU lginp values and n_wmask_rows rows of total-HCU wmask values, the
+   device copy of what ProcExtGen keeps in .lginp/.wmask (ProcExtGen.cpp:57-103).
+   bcpnn_use_stimulus selects the rows used by the following runs without any
+   host->device copy; bcpnn_set_stimulus switches back to host-set values. */
+int bcpnn_upload_stimuli(bcpnn_net* net, int32_t n_lginp_rows, const float* lginp_rows, int32_t n_wmask_rows,
+                         const float* wmask_rows);
+int bcpnn_use_stimulus(bcpnn_net* net, int32_t lginp_row, int32_t wmask_row);
+
+/* The same from ProcExtGen's pattern-index rows (.lgidx, one MCU index per
+   HCU; any other value means no input to that HCU): the library computes
+   lginp = log(1+eps) on the indexed MCU and log(0+eps) elsewhere
+   (ProcExtGen.cpp:130-144) with its own float log. */
+int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hcu, float eps, const float* wmask_row,
+                           size_t n_wmask);
+int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
+                             int32_t n_wmask_rows, const float* wmask_rows);
+
 /* External spike replay of one population (ProcUpdLazy args "external spike",
    ProcUpdLazy/Pop.cpp:67-110 and fill_spike :389-409): n entries, entry k
    overrides the spikes of tick ticks[k] with idx[offsets[k] .. offsets[k+1]).
@@ -123,6 +141,15 @@ int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* 
    plus the ProcExchangeSpike copy (ProcExchangeSpike.cpp:94-139) when
    desc->exchange_spikes is set. */
 int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn, float old_prn);
+
+/* Restore gsbn's initial values in every state vector (Pop.cpp:59-65,
+   Proj.cpp:88-105) and restart the tick count; connectivity, stimulus and
+   replay tables are kept.  Asynchronous, on the device. */
+int bcpnn_reset(bcpnn_net* net);
+
+/* The cudaStream_t (as void*) the network's work is queued on, for callers
+   that time or order their own work against it. */
+int bcpnn_get_stream(const bcpnn_net* net, void** stream);
 
 /* Wait for all work queued on the network's stream. */
 int bcpnn_sync(bcpnn_net* net);

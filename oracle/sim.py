@@ -209,12 +209,14 @@ def proc_args(sp, name):
 def parse_conn_map(text, pops, projs):
     """Slot tables (ii, di) per projection from a connection map: lines
     `proj,dest_hcu,src_mcu,delay,src_mcu,delay,...`; each pair fills the first
-    empty slot of the destination HCU and is dropped when none is left."""
-    tables = []
+    empty slot of the destination HCU and is dropped when none is left.  Slots
+    only ever fill in order here, so the first empty slot is a running count."""
+    tables, fill = [], []
     for q in projs:
         C = dim_conn(pops, q)
         H = pops[q["dest_pop"]]["hcu_num"]
         tables.append((np.full(H * C, -1, np.int32), np.zeros(H * C, np.int32), C))
+        fill.append(np.zeros(H, np.int64))
     for line in text.splitlines():
         v = line.split(",")
         if len(v) > 2:
@@ -222,13 +224,12 @@ def parse_conn_map(text, pops, projs):
             hcu = int(v[1])
             ii, di, C = tables[prj]
             for i in range(2, len(v) - 1, 2):
-                src, dl = int(v[i]), int(v[i + 1])
-                base = hcu * C
-                for s in range(C):
-                    if ii[base + s] < 0:
-                        ii[base + s] = src
-                        di[base + s] = dl
-                        break
+                s = fill[prj][hcu]
+                if s < C:
+                    ii[hcu * C + s] = int(v[i])
+                    di[hcu * C + s] = int(v[i + 1])
+                    if int(v[i]) >= 0:  # a negative source leaves the slot empty
+                        fill[prj][hcu] = s + 1
     return [(t[0], t[1]) for t in tables]
 
 
