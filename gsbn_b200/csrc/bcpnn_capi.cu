@@ -19,6 +19,7 @@
 
 #include "bcpnn.h"
 #include "bcpnn_device.cuh"
+#include "bcpnn_tick.cuh"
 #include "bcpnn_numerics.h"
 
 using namespace bcpnn;
@@ -69,6 +70,9 @@ struct bcpnn_net {
   int last_run_ticks = 0;
   bool exchange = false;
   bool direct = false;      /* GSBN_DIRECT_LAUNCH=1: launch kernels one by one (profilers) */
+  bool persistent = false;  /* one cooperative launch per run (else one launch per tick) */
+  size_t tick_smem = 0;     /* dynamic shared memory of tick_kernel */
+  unsigned int* bar = nullptr; /* grid barrier arrival counter of the persistent kernel */
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   uint64_t launches = 0;
   uint64_t all_cells = 0;   /* cells swept by all-cells catch-ups */
@@ -119,8 +123,10 @@ int check_device_error(bcpnn_net* net) {
   CU(cudaStreamSynchronize(net->stream));
   if (e) {
     CU(cudaMemsetAsync(net->h.err, 0, sizeof(int), net->stream));
-    return fail(net, BCPNN_ERR_DEVICE, "kernel reported error word " + std::to_string(e) +
-                                           " (a slot's source MCU index is outside the source population)");
+    std::string why;
+    if (e & kErrIndex) why += " a slot's source MCU index is outside the source population;";
+    if (e & kErrBarrier) why += " a grid barrier of the persistent tick kernel timed out;";
+    return fail(net, BCPNN_ERR_DEVICE, "kernel reported error word " + std::to_string(e) + ":" + why);
   }
   return BCPNN_OK;
 }
@@ -249,9 +255,17 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
       all_cells_kernel<<<grid_for((size_t)J.H * J.C * J.M, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
     }
   }
-  size_t smem = tick_smem_bytes(net->max_m);
-  for (int it = 0; it < n_ticks; ++it)
-    tick_kernel<<<net->total_hcu, kBlock, smem, net->stream>>>(net->d_net, net->d_rp, it, net->max_m);
+  size_t smem = net->tick_smem;
+  if (net->persistent) {
+    cudaMemsetAsync(net->bar, 0, sizeof(unsigned int), net->stream);
+    int it0 = 0, n = n_ticks;
+    void* args[] = {(void*)&net->d_net, (void*)&net->d_rp, (void*)&it0, (void*)&n, (void*)&net->bar};
+    cudaLaunchCooperativeKernel((const void*)tick_kernel, dim3(net->total_hcu), dim3(kBlock), args, smem,
+                                net->stream);
+  } else {
+    for (int it = 0; it < n_ticks; ++it)
+      tick_kernel<<<net->total_hcu, kBlock, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+  }
 }
 
 int capture_graph(bcpnn_net* net, int n_ticks, bool with_all, cudaGraphExec_t* out) {
@@ -376,8 +390,15 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
       desc->max_ticks_per_run <= 0)
     return BCPNN_ERR_INVALID;
   for (int p = 0; p < desc->n_pops; ++p)
-    if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 || desc->pops[p].mcu_num > 1024)
+    if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 || desc->pops[p].mcu_num > kBlock)
       return BCPNN_ERR_INVALID;
+  {
+    std::vector<int> n_in(desc->n_pops, 0);
+    for (int p = 0; p < desc->n_projs; ++p)
+      if (desc->projs[p].dest_pop >= 0 && desc->projs[p].dest_pop < desc->n_pops) n_in[desc->projs[p].dest_pop]++;
+    for (int c : n_in)
+      if (c > kMaxIn) return BCPNN_ERR_INVALID;
+  }
   for (int p = 0; p < desc->n_projs; ++p) {
     const bcpnn_proj_desc& d = desc->projs[p];
     if (d.src_pop < 0 || d.src_pop >= desc->n_pops || d.dest_pop < 0 || d.dest_pop >= desc->n_pops ||
@@ -599,11 +620,35 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     net->err = "copy of network descriptor failed";
     return bail(BCPNN_ERR_CUDA);
   }
-  size_t smem = tick_smem_bytes(net->max_m);
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+  /* shared memory of the resident tick kernel: the largest population */
+  size_t smem = 0;
+  for (const PopHost& P : net->pops) {
+    int C[kMaxIn] = {0};
+    for (size_t q = 0; q < P.in_proj.size(); ++q) C[q] = net->projs[P.in_proj[q]].C;
+    smem = std::max(smem, tick_smem_bytes_for(P.M, (int)P.in_proj.size(), C));
+  }
+  int smem_max = 0;
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, net->device);
+  if (smem + 1024 > (size_t)smem_max) {
+    net->err = "network too large for the resident tick kernel: " + std::to_string(smem) +
+               " bytes of shared memory per HCU";
+    return bail(BCPNN_ERR_INVALID);
+  }
+  net->tick_smem = smem;
+  if (cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
     net->err = "cannot raise the shared memory limit of tick_kernel";
     return bail(BCPNN_ERR_CUDA);
+  }
+  /* persistent path: every CTA of the grid must be resident at once */
+  {
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, net->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tick_kernel, kBlock, smem);
+    const char* e = std::getenv("GSBN_PER_TICK");
+    bool forced = e && e[0] == '1';
+    net->persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu;
+    if ((rc = dalloc(net, &net->bar, 1))) return bail(rc);
   }
   if (cudaStreamSynchronize(net->stream) != cudaSuccess) {
     net->err = "initialisation failed";
@@ -824,7 +869,7 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   net->rp.lginp = net->cur_lg;
   net->rp.wmask = net->cur_wm;
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));
-  if (net->direct) {
+  if (net->direct || net->persistent) {
     enqueue_run(net, n_ticks, with_all);
     CU(cudaGetLastError());
   } else {
@@ -840,7 +885,7 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     }
     CU(cudaGraphLaunch(ge, net->stream));
   }
-  net->launches += (uint64_t)n_ticks + (with_all ? 2u * net->projs.size() : 0u);
+  net->launches += (uint64_t)(net->persistent ? 1 : n_ticks) + (with_all ? 2u * net->projs.size() : 0u);
   if (with_all)
     for (const ProjHost& J : net->projs) net->all_cells += (uint64_t)J.H * J.C * J.M;
   net->k_total += n_ticks;

@@ -40,12 +40,16 @@
 
 namespace bcpnn {
 
-constexpr int kBlock = 256;         /* threads of tick_kernel                  */
+constexpr int kBlock = 512;         /* threads of tick_kernel                  */
+constexpr int kWarps = kBlock / 32;
 constexpr int kMaxProj = 64;        /* projections per network                 */
-constexpr int kRowChunkCells = 4096;/* row-phase cells staged in shared memory */
+constexpr int kRowChunkCells = kBlock; /* row cells staged per chunk (one per thread) */
+constexpr int kColU = 2;            /* column cells per thread per batch         */
+constexpr int kMaxIn = 8;           /* incoming projections per population       */
 
 /* error bits of NetDev::err */
 constexpr int kErrIndex = 1;        /* ii out of the source population range   */
+constexpr int kErrBarrier = 2;      /* a grid barrier wait ran out of time      */
 
 struct PopDev {
   int H, M, n, hcu_start, mcu_start, dim_proj, id;
@@ -137,13 +141,46 @@ __device__ __forceinline__ Coef make_coef(float kp, float ke, float kzi, float k
   return k;
 }
 
+/* The transcendental functions are real calls in device code: several call
+   sites share one copy of their instructions, which keeps the tick kernel's
+   instruction footprint small (its rarely taken paths are otherwise fetched
+   from L2 every tick). */
+__device__ __noinline__ float dev_expf(float x) { return bx_expf(x); }
+__device__ __noinline__ float dev_logf(float x) { return bx_logf(x); }
+__device__ __noinline__ float dev_normal01(uint32_t seed, uint32_t pop, uint32_t tick, uint32_t mcu) {
+  return bx_normal01(seed, pop, tick, mcu);
+}
+
 /* table entry computed inline (used to build tables and for an elapsed time
    beyond the table) */
-__device__ __forceinline__ void table_entry(float kp, float ke, float kzi, float kzj, int d, float4 out[4]) {
+__device__ __forceinline__ void table_entry(float kp, float ke, float kzi, float kzj, int d, float4& o0, float4& o1,
+                                            float4& o2, float4& o3) {
   float fd = (float)d;
   float a = kp * fd, b = ke * fd, c = kzi * fd, e = kzj * fd;
   float D3 = (kzi - ke) + kzj;
   float Dezi = ke - kzi;
+  float Ep = dev_expf(a);
+  float Epe = dev_expf(a - b);
+  float Epzz = dev_expf((a - c) - e);
+  float Ee = dev_expf(b);
+  float Ezi = dev_expf(c);
+  float Ezj = dev_expf(e);
+  float Emzi = dev_expf(-kzi * fd);
+  float Emzj = dev_expf(-kzj * fd);
+  float Epzi = dev_expf(a - c);
+  float Eezi = dev_expf(b - c);
+  o0 = make_float4(Ep, Epe, Epzz, Ep * D3);
+  o1 = make_float4(Ee, (Ezi * Ezj) * D3, Emzi, Emzj);
+  o2 = make_float4(Ep, Epe, Epzi, Ep * Dezi);
+  o3 = make_float4(Ee, Eezi, Ee * Dezi, Emzi);
+}
+
+/* the cell part (entry[0], entry[1]) of the decay factors for d elapsed
+   ticks, computed with the same float expressions as table_entry */
+__device__ __forceinline__ void cell_factors(float kp, float ke, float kzi, float kzj, int d, float4& A, float4& B) {
+  float fd = (float)d;
+  float a = kp * fd, b = ke * fd, c = kzi * fd, e = kzj * fd;
+  float D3 = (kzi - ke) + kzj;
   float Ep = bx_expf(a);
   float Epe = bx_expf(a - b);
   float Epzz = bx_expf((a - c) - e);
@@ -152,12 +189,35 @@ __device__ __forceinline__ void table_entry(float kp, float ke, float kzi, float
   float Ezj = bx_expf(e);
   float Emzi = bx_expf(-kzi * fd);
   float Emzj = bx_expf(-kzj * fd);
-  float Epzi = bx_expf(a - c);
-  float Eezi = bx_expf(b - c);
-  out[0] = make_float4(Ep, Epe, Epzz, Ep * D3);
-  out[1] = make_float4(Ee, (Ezi * Ezj) * D3, Emzi, Emzj);
-  out[2] = make_float4(Ep, Epe, Epzi, Ep * Dezi);
-  out[3] = make_float4(Ee, Eezi, Ee * Dezi, Emzi);
+  A = make_float4(Ep, Epe, Epzz, Ep * D3);
+  B = make_float4(Ee, (Ezi * Ezj) * D3, Emzi, Emzj);
+}
+
+/* the two float4 of part `part` (0: cell, 2: row) of an entry beyond the
+   table, computed; one out-of-line copy */
+struct F4x2 {
+  float4 a, b;
+};
+
+__device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float kzj, int d, int part) {
+  float4 t0, t1, t2, t3;
+  table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+  F4x2 r;
+  if (part == 0) {
+    r.a = t0;
+    r.b = t1;
+  } else {
+    r.a = t2;
+    r.b = t3;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void table_pair(float kp, float ke, float kzi, float kzj, int d, int part, float4& A,
+                                           float4& B) {
+  F4x2 r = table_pair_nl(kp, ke, kzi, kzj, d, part);
+  A = r.a;
+  B = r.b;
 }
 
 __device__ __forceinline__ void load_entry(const float4* tab, int len, const Coef& k, int d, int part,
@@ -166,10 +226,7 @@ __device__ __forceinline__ void load_entry(const float4* tab, int len, const Coe
     A = tab[(size_t)d * 4 + part];
     B = tab[(size_t)d * 4 + part + 1];
   } else {
-    float4 t[4];
-    table_entry(k.kp, k.ke, k.kzi, k.kzj, d, t);
-    A = t[part];
-    B = t[part + 1];
+    table_pair(k.kp, k.ke, k.kzi, k.kzj, d, part, A, B);
   }
 }
 
@@ -205,12 +262,12 @@ __device__ __forceinline__ void row_decay(float& pi, float& ei, float& zi, const
 
 __global__ void build_table_kernel(float4* tab, int len, float kp, float ke, float kzi, float kzj) {
   for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < len; d += gridDim.x * blockDim.x) {
-    float4 t[4];
-    table_entry(kp, ke, kzi, kzj, d, t);
-    tab[(size_t)d * 4 + 0] = t[0];
-    tab[(size_t)d * 4 + 1] = t[1];
-    tab[(size_t)d * 4 + 2] = t[2];
-    tab[(size_t)d * 4 + 3] = t[3];
+    float4 t0, t1, t2, t3;
+    table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+    tab[(size_t)d * 4 + 0] = t0;
+    tab[(size_t)d * 4 + 1] = t1;
+    tab[(size_t)d * 4 + 2] = t2;
+    tab[(size_t)d * 4 + 3] = t3;
   }
 }
 
@@ -266,7 +323,7 @@ __global__ void all_cells_kernel(const NetDev* __restrict__ net, const RunParams
         int h = r / J.C;
         float pi = J.pi[r];
         float pj = J.pj[h * J.M + j];
-        J.wij[c] = J.wgain * bx_logf((q.x + J.eps2) / ((pi + J.eps) * (pj + J.eps)));
+        J.wij[c] = J.wgain * dev_logf((q.x + J.eps2) / ((pi + J.eps) * (pj + J.eps)));
       }
     }
   }
@@ -276,30 +333,36 @@ __global__ void all_cells_kernel(const NetDev* __restrict__ net, const RunParams
 /* block helpers                                                              */
 /* ------------------------------------------------------------------------ */
 
-/* Ordered compaction of one flag per thread over a block of kBlock threads:
-   returns the position of this thread's item among the set flags and writes
-   the total to *total (shared). */
-__device__ __forceinline__ int block_prefix(bool flag, int* s_warp, int* total) {
+/* Ordered compaction over the kBlock threads: position of this thread's item
+   among the set flags (in thread order) and, through *total, their number.
+   Contains two __syncthreads; every thread of the block must call it. */
+__device__ __forceinline__ int block_prefix(bool flag, int* s_warp, int* s_total, int* total) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned m = __ballot_sync(0xffffffffu, flag);
   int before = __popc(m & ((1u << lane) - 1u));
   if (lane == 0) s_warp[warp] = __popc(m);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int w = 0; w < kBlock / 32; ++w) {
-      int c = s_warp[w];
-      s_warp[w] = acc;
-      acc += c;
+  if (warp == 0) {
+    int c = lane < kWarps ? s_warp[lane] : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    *total = acc;
+    if (lane < kWarps) s_warp[lane] = incl - c;
+    if (lane == 31) *s_total = incl;
   }
   __syncthreads();
-  int pos = s_warp[warp] + before;
-  return pos;
+  int base = s_warp[warp];
+  *total = *s_total;
+  __syncwarp();
+  return base + before;
 }
 
+/* maximum over the block (exact, order independent); one __syncthreads */
 __device__ __forceinline__ float block_max(float v, float* s_red) {
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     float w = __shfl_xor_sync(0xffffffffu, v, o);
     v = (w > v) ? w : v;
@@ -307,323 +370,13 @@ __device__ __forceinline__ float block_max(float v, float* s_red) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) s_red[warp] = v;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    float m = s_red[0];
-    for (int w = 1; w < kBlock / 32; ++w) m = (s_red[w] > m) ? s_red[w] : m;
-    s_red[0] = m;
+  float r = s_red[lane % kWarps];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    float w = __shfl_xor_sync(0xffffffffu, r, o);
+    r = (w > r) ? w : r;
   }
-  __syncthreads();
-  float r = s_red[0];
-  __syncthreads();
   return r;
-}
-
-/* ------------------------------------------------------------------------ */
-/* one tick for one (population, destination HCU)                             */
-/* ------------------------------------------------------------------------ */
-
-/* dynamic shared memory layout (floats unless noted):
-   s_dsup[M] s_act[M] s_epsc[M] s_pj[M] s_w[kRowChunkCells] s_pi[kRowChunkCells]
-   s_spkl[M] (int) s_spk[M] (int8) s_skip[kRowChunkCells] (int8)            */
-__host__ __device__ inline size_t tick_smem_bytes(int max_m) {
-  return (size_t)4 * max_m * 4 + (size_t)kRowChunkCells * 8 + (size_t)max_m * 4 + (size_t)max_m +
-         (size_t)kRowChunkCells + 64;
-}
-
-__global__ void __launch_bounds__(kBlock) tick_kernel(const NetDev* __restrict__ net,
-                                                      const RunParams* __restrict__ rp, int it, int max_m) {
-  extern __shared__ float smem[];
-  __shared__ int s_warp[kBlock / 32];
-  __shared__ float s_red[kBlock / 32];
-  __shared__ int s_total;
-  __shared__ float s_dsup0;
-  __shared__ float s_vsum;
-  __shared__ int s_nspk;
-  __shared__ int s_cnt;
-  __shared__ int s_flag9;
-
-  const int P = net->cta_pop[blockIdx.x];
-  const int h = net->cta_hcu[blockIdx.x];
-  const PopDev& pop = net->pops[P];
-  const int M = pop.M, n = pop.n;
-  const int simstep = rp->simstep0 + it;
-  const int kk = rp->k0 + it;
-  const int cur = kk & 1, prev = cur ^ 1;
-  const float prn = rp->prn;
-  const int tid = threadIdx.x;
-
-  float* s_dsup = smem;
-  float* s_act = s_dsup + max_m;
-  float* s_epsc = s_act + max_m;
-  float* s_pj = s_epsc + max_m;
-  float* s_w = s_pj + max_m;
-  float* s_pi = s_w + kRowChunkCells;
-  int* s_spkl = (int*)(s_pi + kRowChunkCells);
-  int8_t* s_spk = (int8_t*)(s_spkl + max_m);
-  int8_t* s_skip = s_spk + max_m;
-
-  /* ---- population update, Pop.cpp:229-323 -------------------------------- */
-  const float* lginp = rp->lginp + pop.mcu_start;
-  const float* wmask = rp->wmask + pop.hcu_start;
-  const float* epsc_prev = pop.epsc[prev];
-  const float* bj_prev = pop.bj[prev];
-  const float* dsup_prev = pop.dsup[prev];
-
-  /* support of MCU `idx` of HCU `hh` (update_sup_kernel_1_cpu) */
-  auto support = [&](int hh, int idx) -> float {
-    float wsup = 0.0f;
-    int offset = 0;
-    for (int m = 0; m < pop.dim_proj; m++) {
-      wsup += bj_prev[offset + idx] + epsc_prev[offset + idx];
-      offset += n;
-    }
-    float noise = 0.0f;
-    if (pop.snoise != 0.0f) noise = pop.snoise * bx_normal01(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
-    float sup = pop.lgbias + pop.igain * lginp[idx] + noise;
-    sup += (pop.wgain * wmask[hh]) * wsup;
-    float d = dsup_prev[idx];
-    return d + (sup - d) * pop.taumdt;
-  };
-
-  for (int j = tid; j < M; j += kBlock) s_dsup[j] = support(h, h * M + j);
-  if (tid == 0) s_dsup0 = (h == 0) ? -1.0f : support(0, 0);
-  __syncthreads();
-  if (h == 0 && tid == 0) s_dsup0 = s_dsup[0];
-  __syncthreads();
-  /* max seeded with the population's first MCU (Pop.cpp:270) */
-  float tmax = s_dsup0;
-  for (int j = tid; j < M; j += kBlock) tmax = (s_dsup[j] > tmax) ? s_dsup[j] : tmax;
-  const float maxdsup = block_max(tmax, s_red);
-  const float maxact = bx_expf(pop.wtagain * maxdsup);
-  for (int j = tid; j < M; j += kBlock) {
-    float a = bx_expf(pop.wtagain * (s_dsup[j] - maxdsup));
-    if (maxact < 1.0f) a *= maxact;
-    s_act[j] = a;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    float vsum = 0.0f;
-    for (int m = 0; m < M; m++) vsum += s_act[m];  /* serial, in MCU order */
-    s_vsum = vsum;
-  }
-  __syncthreads();
-  const float vsum = s_vsum;
-  const float pr = net->poisson_hz * net->dt;
-  for (int j = tid; j < M; j += kBlock) {
-    int idx = h * M + j;
-    float a = s_act[j];
-    if (vsum > 1.0f) a /= vsum;
-    pop.act[idx] = a;
-    pop.dsup[cur][idx] = s_dsup[j];
-    float u = bx_uniform01(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
-    int8_t spk = (int8_t)(u < a * pop.maxfqdt);
-    if (net->poisson_hz > 0.0f) {
-      float up = bx_uniform01_poisson(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
-      if (up < pr) spk = 1;
-    }
-    pop.counter[idx] += spk;
-    s_spk[j] = spk;
-  }
-  /* external spike replay overrides the sampled spikes (Pop.cpp:389-409) */
-  if (pop.ext) {
-    __syncthreads();
-    for (int j = tid; j < M; j += kBlock) s_spk[j] = 0;
-    __syncthreads();
-    if (simstep >= pop.ext_t0 && simstep < pop.ext_t1) {
-      int b0 = pop.ext_off[simstep - pop.ext_t0], b1 = pop.ext_off[simstep - pop.ext_t0 + 1];
-      for (int e = b0 + tid; e < b1; e += kBlock) {
-        int v = pop.ext_idx[e];
-        if (v >= h * M && v < h * M + M) s_spk[v - h * M] = 1;
-      }
-    }
-  }
-  __syncthreads();
-  /* publish spikes; ordered list of this HCU's spiking MCUs */
-  if (tid == 0) s_nspk = 0;
-  for (int base = 0; base < M; base += kBlock) {
-    int j = base + tid;
-    bool f = (j < M) && s_spk[j] > 0;
-    int pos = block_prefix(f, s_warp, &s_total);
-    if (f) s_spkl[s_nspk + pos] = j;
-    __syncthreads();
-    if (tid == 0) s_nspk += s_total;
-    __syncthreads();
-  }
-  uint32_t* log = pop.spk_log + (size_t)it * pop.log_words;
-  for (int j = tid; j < M; j += kBlock) {
-    int idx = h * M + j;
-    int8_t s = s_spk[j];
-    pop.spike[idx] = s;
-    if (s) atomicOr(&log[idx >> 5], 1u << (idx & 31));
-    for (int q = 0; q < pop.n_out; ++q) net->projs[pop.out_proj[q]].si[cur][idx] = s;
-  }
-  const int nspk = s_nspk;
-
-  /* ---- incoming projections ------------------------------------------------ */
-  for (int q = 0; q < pop.n_in; ++q) {
-    const int p = pop.in_proj[q];
-    const ProjDev& J = net->projs[p];
-    const int C = J.C;
-    const float kp = J.taupdt * prn;
-    const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-    const float4* tab = rp->tab[p];
-    const int tlen = rp->tab_len[p];
-    const size_t eoff = (size_t)J.proj_in_pop * n;
-
-    /* j-traces and bias, Proj.cpp:310-363 */
-    for (int j = tid; j < M; j += kBlock) {
-      int idx = h * M + j;
-      float pj = J.pj[idx], ej = J.ej[idx], zj = J.zj[idx];
-      float e = pop.epsc[prev][eoff + idx];
-      e *= (1 - J.kepsc);
-      pj += (ej - pj) * kp;
-      ej += (zj - ej) * k.ke;
-      zj *= (1 - J.kzj);
-      if (s_spk[j] > 0) zj += J.kftj;
-      float b = pop.bj[prev][eoff + idx];
-      if (kp != 0.0f) b = J.bgain * bx_logf(pj + J.eps);
-      pop.bj[cur][eoff + idx] = b;
-      J.pj[idx] = pj;
-      J.ej[idx] = ej;
-      J.zj[idx] = zj;
-      s_epsc[j] = e;
-      s_pj[j] = pj;
-    }
-    if (tid == 0) s_flag9 = 0;
-    __syncthreads();
-
-    /* row updates of this HCU's active rows, ascending, Proj.cpp:365-479 */
-    const int nrow = J.list_cnt[h];
-    const int* rows = J.list + (size_t)h * C;
-    const int rch = (kRowChunkCells / M) > 0 ? (kRowChunkCells / M) : 1;
-    for (int base = 0; base < nrow; base += rch) {
-      const int nr = (nrow - base) < rch ? (nrow - base) : rch;
-      for (int t = tid; t < nr; t += kBlock) {
-        int r = rows[base + t];
-        if (r == 9) s_flag9 = 1;
-        int pdt = simstep - J.ti[r];
-        if (pdt <= 0) {
-          J.zi[r] += J.kfti;
-          J.ti[r] = simstep;
-          s_pi[t] = J.pi[r];
-        } else {
-          float pi = J.pi[r], ei = J.ei[r], zi = J.zi[r];
-          float4 A, B;
-          load_entry(tab, tlen, k, pdt, 2, A, B);
-          row_decay(pi, ei, zi, k, A, B);
-          zi = zi + J.kfti;
-          J.pi[r] = pi;
-          J.ei[r] = ei;
-          J.zi[r] = zi;
-          J.ti[r] = simstep;
-          s_pi[t] = pi;
-        }
-      }
-      __syncthreads();
-      for (int c = tid; c < nr * M; c += kBlock) {
-        int rr = c / M;
-        int j = c - rr * M;
-        int r = rows[base + rr];
-        size_t index = (size_t)r * M + j;
-        int pdt = simstep - J.tij[index];
-        float4 cv = J.cell[index];
-        if (pdt <= 0) {
-          cv.z += J.kfti;
-          J.cell[index] = cv;
-          J.tij[index] = simstep;
-          s_skip[c] = 1;
-        } else {
-          float4 A, B;
-          load_entry(tab, tlen, k, pdt, 0, A, B);
-          cell_decay(cv.x, cv.y, cv.z, cv.w, k, A, B);
-          cv.z = cv.z + J.kfti;
-          J.cell[index] = cv;
-          J.tij[index] = simstep;
-          float w;
-          if (kp != 0.0f) {
-            w = J.wgain * bx_logf((cv.x + J.eps2) / ((s_pi[rr] + J.eps) * (s_pj[j] + J.eps)));
-            J.wij[index] = w;
-          } else {
-            w = J.wij[index];
-          }
-          s_w[c] = w;
-          s_skip[c] = 0;
-        }
-      }
-      __syncthreads();
-      for (int j = tid; j < M; j += kBlock) {
-        float e = s_epsc[j];
-        for (int rr = 0; rr < nr; ++rr)
-          if (!s_skip[rr * M + j]) e += s_w[rr * M + j];
-        s_epsc[j] = e;
-      }
-      __syncthreads();
-    }
-    for (int j = tid; j < M; j += kBlock) pop.epsc[cur][eoff + h * M + j] = s_epsc[j];
-
-    /* column updates of this HCU's spiking MCUs, Proj.cpp:481-536 */
-    for (int c = tid; c < nspk * C; c += kBlock) {
-      int qq = c / C;
-      int s = c - qq * C;
-      int j = s_spkl[qq];
-      int r = h * C + s;
-      if (J.ii[r] < 0) continue;
-      size_t index = (size_t)r * M + j;
-      int pdt = simstep - J.tij[index];
-      float4 cv = J.cell[index];
-      if (pdt <= 0) {
-        cv.w += J.kftj;
-      } else {
-        float4 A, B;
-        load_entry(tab, tlen, k, pdt, 0, A, B);
-        cell_decay(cv.x, cv.y, cv.z, cv.w, k, A, B);
-        cv.w = cv.w + J.kftj;
-      }
-      J.cell[index] = cv;
-      J.tij[index] = simstep;
-    }
-
-    /* delay queue of this HCU's slots and ordered compaction of the next
-       tick's active rows, Proj.cpp:621-630, 645-664 */
-    if (tid == 0) s_cnt = 0;
-    __syncthreads();
-    const int8_t* si = J.si[prev];
-    for (int base = 0; base < C; base += kBlock) {
-      int s = base + tid;
-      bool act = false;
-      int r = h * C + s;
-      if (s < C) {
-        int src = J.ii[r];
-        if (src >= 0) {
-          if (src >= J.Ns) {
-            atomicOr(net->err, kErrIndex);
-          } else {
-            int qv = J.qi[r];
-            act = (qv & 0x01) != 0;
-            qv >>= 1;
-            if (si[src] > 0) qv |= (0x01 << (J.di[r] - 1));
-            J.qi[r] = qv;
-          }
-        }
-      }
-      int pos = block_prefix(act, s_warp, &s_total);
-      if (act) J.list[(size_t)h * C + s_cnt + pos] = r;
-      __syncthreads();
-      if (tid == 0) s_cnt += s_total;
-      __syncthreads();
-    }
-    if (tid == 0) {
-      J.list_cnt[h] = s_cnt;
-      /* debug flags of ProcSpkRec (ssi/ssj contain index 9) */
-      uint8_t f = 0;
-      if (s_flag9) f |= 1;
-      if (h == 9 / M && 9 < n && s_spk[9 - h * M] > 0) f |= 2;
-      if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + p], (uint32_t)f);
-      atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
-      atomicAdd(&net->counters[1], (unsigned long long)nspk * C);
-    }
-    __syncthreads();
-  }
 }
 
 /* fill kernels used to (re)initialise the state on the device */

@@ -1,0 +1,797 @@
+/*
+ * bcpnn_tick.cuh -- the tick of the plain FP32 path: one CTA per (population,
+ * destination HCU), all state that only this HCU uses kept in shared memory
+ * for the whole launch.
+ *
+ * What one tick of gsbn does for destination HCU h (ProcUpdLazy.cpp:88-124):
+ *   population update      Pop.cpp:229-323   support, softmax/WTA, spikes
+ *   external spike replay  Pop.cpp:389-409
+ *   per incoming projection:
+ *     j-traces and bias    Proj.cpp:310-363
+ *     active rows          Proj.cpp:365-479, 667-720 (ordered epsc sum)
+ *     active columns       Proj.cpp:481-536, 722-760
+ *     delay queue          Proj.cpp:621-630, 645-664 (next tick's rows)
+ * reads, from other HCUs, only (a) the previous tick's presynaptic spikes and
+ * (b) the population's MCU-0 support terms, which seed every HCU's softmax
+ * maximum (Pop.cpp:270).  So the per-MCU traces, the delay queue and the
+ * active-row list of h live in shared memory; only spikes, the MCU-0 seed
+ * values, cells, row traces and logs go through global memory per tick, and
+ * everything is written back to the gsbn-layout arrays at the end of the
+ * launch.
+ *
+ * Launch forms (same code):
+ *   - persistent: one cooperative launch per run, a bounded grid barrier
+ *     between ticks (tick t+1 reads what other CTAs published in tick t);
+ *   - one launch per tick when the grid cannot be co-resident.
+ * The next tick's first row chunk (its traces, cells and decay-table entries)
+ * is staged into shared memory before the barrier, so its loads overlap the
+ * wait.
+ */
+#ifndef BCPNN_TICK_CUH
+#define BCPNN_TICK_CUH
+
+#include "bcpnn_device.cuh"
+
+namespace bcpnn {
+
+/* The CTA is split in two warp groups that run concurrently inside a tick:
+   group A (warps 0-7): support, softmax, spikes, j-traces, active rows;
+   group B (warps 8-15): delay queue (next tick's rows), then, once A has
+   published the spike list, the column updates.  A column cell whose row is
+   also active this tick must see the row update first: B leaves those cells,
+   and all threads do them after the groups join. */
+constexpr int kGroup = kBlock / 2;
+constexpr int kGroupWarps = kGroup / 32;
+constexpr int kBarA = 1, kBarB = 2, kBarSpikes = 3, kBarRows = 4;
+
+__device__ __forceinline__ void group_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kGroup) : "memory");
+}
+
+/* ordered compaction within a warp group (see block_prefix) */
+__device__ __forceinline__ int group_prefix(bool flag, int gtid, int bar_id, int* s_warp, int* s_total, int* total) {
+  int lane = gtid & 31, warp = gtid >> 5;
+  unsigned m = __ballot_sync(0xffffffffu, flag);
+  int before = __popc(m & ((1u << lane) - 1u));
+  if (lane == 0) s_warp[warp] = __popc(m);
+  group_sync(bar_id);
+  if (warp == 0) {
+    int c = lane < kGroupWarps ? s_warp[lane] : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane < kGroupWarps) s_warp[lane] = incl - c;
+    if (lane == 31) *s_total = incl;
+  }
+  group_sync(bar_id);
+  int base = s_warp[warp];
+  *total = *s_total;
+  __syncwarp();
+  return base + before;
+}
+
+__device__ __forceinline__ float group_max(float v, int gtid, int bar_id, float* s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    float w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = (w > v) ? w : v;
+  }
+  int lane = gtid & 31, warp = gtid >> 5;
+  if (lane == 0) s_red[warp] = v;
+  group_sync(bar_id);
+  float r = s_red[lane % kGroupWarps];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    float w = __shfl_xor_sync(0xffffffffu, r, o);
+    r = (w > r) ? w : r;
+  }
+  return r;
+}
+
+/* shared-memory layout of a CTA, in 32-bit words from the dynamic base;
+   float4 arrays first (16-byte alignment) */
+struct TickLayout {
+  int stg_rtr, stg_rA, stg_rB;   /* [kBlock] float4: row traces (pi,ei,zi), table parts 2,3 */
+  int stg_cv, stg_cA, stg_cB;    /* [kRowChunkCells] float4: cell, table parts 0,1          */
+  int stg_row, stg_ti;           /* [kBlock] int                                           */
+  int stg_tv, stg_wv;            /* [kRowChunkCells] int / float                           */
+  int w_dsup, w_act, w_spkl, w_pi, w_w;
+  int w_spk, w_skip;             /* bytes                                                  */
+  int st_dsup, st_act, st_cnt;
+  int st_q[kMaxIn];              /* per incoming projection (QView) */
+  int total;
+};
+
+/* words of one projection's resident block: pj ej zj epsc bj [M]; ii di qi
+   [C]; list [2][C]; bits [2][ceil(C/32)]; nlist [2] */
+__host__ __device__ inline int qblock_words(int M, int C) { return 5 * M + 5 * C + 2 * ((C + 31) / 32) + 2; }
+
+__host__ __device__ inline void tick_layout(int M, int n_in, const int* C, TickLayout& L) {
+  int o = 0;
+  L.stg_rtr = o; o += 4 * kBlock;
+  L.stg_rA = o; o += 4 * kBlock;
+  L.stg_rB = o; o += 4 * kBlock;
+  L.stg_cv = o; o += 4 * kRowChunkCells;
+  L.stg_cA = o; o += 4 * kRowChunkCells;
+  L.stg_cB = o; o += 4 * kRowChunkCells;
+  L.stg_row = o; o += kBlock;
+  L.stg_ti = o; o += kBlock;
+  L.stg_tv = o; o += kRowChunkCells;
+  L.stg_wv = o; o += kRowChunkCells;
+  L.w_dsup = o; o += M;
+  L.w_act = o; o += M;
+  L.w_spkl = o; o += M;
+  L.w_pi = o; o += kBlock;
+  L.w_w = o; o += kRowChunkCells;
+  L.w_spk = o; o += (M + 3) / 4;
+  L.w_skip = o; o += (kRowChunkCells + 3) / 4;
+  L.st_dsup = o; o += M;
+  L.st_act = o; o += M;
+  L.st_cnt = o; o += M;
+  for (int q = 0; q < kMaxIn; ++q) {
+    L.st_q[q] = o;
+    if (q < n_in) o += qblock_words(M, C[q]);
+  }
+  L.total = o;
+}
+
+/* views of projection q's resident block; list/bits/nlist by tick parity */
+struct QView {
+  float *pj, *ej, *zj, *epsc, *bj;
+  int *ii, *di, *qi;
+  int* list;      /* [2][C] */
+  uint32_t* bits; /* [2][W] */
+  int* nlist;     /* [2] */
+  int W;
+};
+
+__device__ __forceinline__ QView qview(float* sm, const TickLayout& L, int q, int M, int C) {
+  QView v;
+  float* b = sm + L.st_q[q];
+  v.pj = b;
+  v.ej = b + M;
+  v.zj = b + 2 * M;
+  v.epsc = b + 3 * M;
+  v.bj = b + 4 * M;
+  int* ib = (int*)(b + 5 * M);
+  v.ii = ib;
+  v.di = ib + C;
+  v.qi = ib + 2 * C;
+  v.list = ib + 3 * C;
+  v.W = (C + 31) / 32;
+  v.bits = (uint32_t*)(ib + 5 * C);
+  v.nlist = ib + 5 * C + 2 * v.W;
+  return v;
+}
+
+__device__ __forceinline__ int row_chunk_rows(int M) {
+  int r = kRowChunkCells / M;
+  if (r < 1) r = 1;
+  return r;
+}
+
+/* Stage rows [base, base+nr) of `list` of projection J for a tick at
+   `simstep`: row traces, cells of the chunk, and the decay-table entries for
+   their elapsed ticks.  Threads gtid, gtid+gsize, ... of a group of gsize. */
+__device__ __forceinline__ void stage_rows(const ProjDev& J, const int* list, int base, int nr, int M, int simstep,
+                                           const float4* tab, int tlen, float* sm, const TickLayout& L, int gtid,
+                                           int gsize) {
+  float4* rtr = (float4*)(sm + L.stg_rtr);
+  float4* rA = (float4*)(sm + L.stg_rA);
+  float4* rB = (float4*)(sm + L.stg_rB);
+  float4* cv = (float4*)(sm + L.stg_cv);
+  float4* cA = (float4*)(sm + L.stg_cA);
+  float4* cB = (float4*)(sm + L.stg_cB);
+  int* srow = (int*)(sm + L.stg_row);
+  int* sti = (int*)(sm + L.stg_ti);
+  int* stv = (int*)(sm + L.stg_tv);
+  float* swv = sm + L.stg_wv;
+  for (int t = gtid; t < nr; t += gsize) {
+    int r = list[base + t];
+    int ti = J.ti[r];
+    float pi = J.pi[r], ei = J.ei[r], zi = J.zi[r];
+    int pdt = simstep - ti;
+    float4 A = make_float4(0, 0, 0, 0), B = A;
+    if (pdt > 0 && pdt < tlen) {
+      A = tab[(size_t)pdt * 4 + 2];
+      B = tab[(size_t)pdt * 4 + 3];
+    }
+    srow[t] = r;
+    sti[t] = ti;
+    rtr[t] = make_float4(pi, ei, zi, 0.0f);
+    rA[t] = A;
+    rB[t] = B;
+  }
+  for (int c = gtid; c < nr * M; c += gsize) {
+    int rr = c / M;
+    int j = c - rr * M;
+    size_t index = (size_t)list[base + rr] * M + j;
+    int tv = J.tij[index];
+    float4 c4 = J.cell[index];
+    float wv = J.wij[index];
+    int pdt = simstep - tv;
+    float4 A = make_float4(0, 0, 0, 0), B = A;
+    if (pdt > 0 && pdt < tlen) {
+      A = tab[(size_t)pdt * 4 + 0];
+      B = tab[(size_t)pdt * 4 + 1];
+    }
+    stv[c] = tv;
+    cv[c] = c4;
+    swv[c] = wv;
+    cA[c] = A;
+    cB[c] = B;
+  }
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void atomic_add_release(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+/* Grid-wide barrier of a cooperative launch: arrival counter `bar` (zero at
+   launch) must reach `target`.  The wait is bounded: after kBarrierNs, or as
+   soon as another CTA has set an error word, it gives up, sets kErrBarrier
+   and returns false, and every CTA leaves its tick loop. */
+constexpr unsigned long long kBarrierNs = 2000000000ull;
+
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int target, int* err, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomic_add_release(bar, 1u);
+    unsigned long long t0 = globaltimer_ns();
+    int ok = 1;
+    while (load_acquire(bar) < target) {
+      if (*(volatile int*)err) {
+        ok = 0;
+        break;
+      }
+      if (globaltimer_ns() - t0 > kBarrierNs) {
+        atomicOr(err, kErrBarrier);
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+/* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */
+__global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restrict__ net,
+                                                         const RunParams* __restrict__ rp, int it0, int n_ticks,
+                                                         unsigned int* bar) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ int s_warpA[kGroupWarps], s_warpB[kGroupWarps];
+  __shared__ float s_red[kGroupWarps];
+  __shared__ int s_totalA, s_totalB;
+  __shared__ float s_dsup0;
+  __shared__ float s_vsum;
+  __shared__ int s_flag9;
+  __shared__ int s_nspk;
+  __shared__ int s_ok;
+
+  const int P = net->cta_pop[blockIdx.x];
+  const int h = net->cta_hcu[blockIdx.x];
+  const PopDev& pop = net->pops[P];
+  const int M = pop.M, n = pop.n;
+  const int n_in = pop.n_in;
+  const int tid = threadIdx.x;
+  const bool groupA = tid < kGroup;
+  const int gtid = groupA ? tid : tid - kGroup;
+  const float prn = rp->prn;
+
+  int Cq[kMaxIn];
+#pragma unroll
+  for (int q = 0; q < kMaxIn; ++q) Cq[q] = q < n_in ? net->projs[pop.in_proj[q]].C : 0;
+  TickLayout L;
+  tick_layout(M, n_in, Cq, L);
+
+  float* w_dsup = sm + L.w_dsup;
+  float* w_act = sm + L.w_act;
+  int* w_spkl = (int*)(sm + L.w_spkl);
+  float* w_pi = sm + L.w_pi;
+  float* w_w = sm + L.w_w;
+  int8_t* w_spk = (int8_t*)(sm + L.w_spk);
+  int8_t* w_skip = (int8_t*)(sm + L.w_skip);
+  float* st_dsup = sm + L.st_dsup;
+  float* st_act = sm + L.st_act;
+  int* st_cnt = (int*)(sm + L.st_cnt);
+
+  /* ---- load the resident state (buffers written by the previous tick) ---- */
+  const int cur0 = (rp->k0 + it0) & 1;
+  {
+    const int prev0 = cur0 ^ 1;
+    for (int j = tid; j < M; j += kBlock) {
+      int idx = h * M + j;
+      st_dsup[j] = pop.dsup[prev0][idx];
+      st_act[j] = pop.act[idx];
+      st_cnt[j] = pop.counter[idx];
+      w_spk[j] = pop.spike[idx];
+    }
+    for (int q = 0; q < n_in; ++q) {
+      const ProjDev& J = net->projs[pop.in_proj[q]];
+      QView V = qview(sm, L, q, M, J.C);
+      const size_t eoff = (size_t)J.proj_in_pop * n;
+      for (int j = tid; j < M; j += kBlock) {
+        int idx = h * M + j;
+        V.pj[j] = J.pj[idx];
+        V.ej[j] = J.ej[idx];
+        V.zj[j] = J.zj[idx];
+        V.epsc[j] = pop.epsc[prev0][eoff + idx];
+        V.bj[j] = pop.bj[prev0][eoff + idx];
+      }
+      for (int s = tid; s < J.C; s += kBlock) {
+        int r = h * J.C + s;
+        V.ii[s] = J.ii[r];
+        V.di[s] = J.di[r];
+        V.qi[s] = J.qi[r];
+        V.list[cur0 * J.C + s] = J.list[r];
+      }
+      for (int w = tid; w < V.W; w += kBlock) V.bits[cur0 * V.W + w] = 0u;
+      if (tid == 0) V.nlist[cur0] = J.list_cnt[h];
+    }
+  }
+  __syncthreads();
+  for (int q = 0; q < n_in; ++q) {
+    const ProjDev& J = net->projs[pop.in_proj[q]];
+    QView V = qview(sm, L, q, M, J.C);
+    for (int e = tid; e < V.nlist[cur0]; e += kBlock) {
+      int s = V.list[cur0 * J.C + e] - h * J.C;
+      atomicOr(&V.bits[cur0 * V.W + (s >> 5)], 1u << (s & 31));
+    }
+  }
+  if (n_in > 0) {
+    const ProjDev& J = net->projs[pop.in_proj[0]];
+    QView V = qview(sm, L, 0, M, J.C);
+    int nr = V.nlist[cur0] < row_chunk_rows(M) ? V.nlist[cur0] : row_chunk_rows(M);
+    const int p0 = pop.in_proj[0];
+    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, rp->tab[p0], rp->tab_len[p0], sm, L, tid,
+               kBlock);
+  }
+
+  for (int it = it0; it < it0 + n_ticks; ++it) {
+    if (it > it0) {
+      if (!grid_sync(bar, (unsigned int)(it - it0) * gridDim.x, net->err, &s_ok)) return;
+    } else {
+      __syncthreads();
+    }
+    const int simstep = rp->simstep0 + it;
+    const int kk = rp->k0 + it;
+    const int cur = kk & 1, prev = cur ^ 1, nxt = cur ^ 1;
+
+    if (groupA) {
+      /* ================= group A: population, j-traces, rows ============= */
+      /* population update, Pop.cpp:229-323 */
+      const float* lginp = rp->lginp + pop.mcu_start;
+      const float* wmask = rp->wmask + pop.hcu_start;
+      for (int j = gtid; j < M; j += kGroup) {
+        float wsup = 0.0f;
+        for (int m = 0; m < pop.dim_proj; m++) {
+          const float* b = sm + L.st_q[m];
+          wsup += b[4 * M + j] + b[3 * M + j];   /* bj + epsc */
+        }
+        int idx = h * M + j;
+        float noise = 0.0f;
+        if (pop.snoise != 0.0f)
+          noise = pop.snoise * dev_normal01(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
+        float sup = pop.lgbias + pop.igain * lginp[idx] + noise;
+        sup += (pop.wgain * wmask[h]) * wsup;
+        float d = st_dsup[j];
+        w_dsup[j] = d + (sup - d) * pop.taumdt;
+      }
+      /* the softmax max of every HCU is seeded with the population's first
+         MCU (Pop.cpp:270), published by HCU 0's CTA in the previous tick */
+      const int tseed = (M < kGroup) ? kGroup - 1 : 0;
+      if (gtid == tseed && h != 0) {
+        float wsup = 0.0f;
+        int offset = 0;
+        for (int m = 0; m < pop.dim_proj; m++) {
+          wsup += __ldcg(pop.bj[prev] + offset) + __ldcg(pop.epsc[prev] + offset);
+          offset += n;
+        }
+        float noise = 0.0f;
+        if (pop.snoise != 0.0f) noise = pop.snoise * dev_normal01(net->seed, (uint32_t)P, (uint32_t)simstep, 0u);
+        float sup = pop.lgbias + pop.igain * lginp[0] + noise;
+        sup += (pop.wgain * wmask[0]) * wsup;
+        float d = __ldcg(pop.dsup[prev]);
+        s_dsup0 = d + (sup - d) * pop.taumdt;
+      }
+      group_sync(kBarA);
+      const float seed0 = (h == 0) ? w_dsup[0] : s_dsup0;
+      float tmax = seed0;
+      for (int j = gtid; j < M; j += kGroup) tmax = (w_dsup[j] > tmax) ? w_dsup[j] : tmax;
+      const float maxdsup = group_max(tmax, gtid, kBarA, s_red);
+      const float maxact = bx_expf(pop.wtagain * maxdsup);
+      for (int j = gtid; j < M; j += kGroup) {
+        float a = bx_expf(pop.wtagain * (w_dsup[j] - maxdsup));
+        if (maxact < 1.0f) a *= maxact;
+        w_act[j] = a;
+      }
+      group_sync(kBarA);
+      if (gtid == 0) {
+        /* serial, in MCU order (Pop.cpp:281-293) */
+        float vsum = 0.0f;
+        int m = 0;
+        for (; m + 4 <= M; m += 4) {
+          float a0 = w_act[m], a1 = w_act[m + 1], a2 = w_act[m + 2], a3 = w_act[m + 3];
+          vsum += a0;
+          vsum += a1;
+          vsum += a2;
+          vsum += a3;
+        }
+        for (; m < M; m++) vsum += w_act[m];
+        s_vsum = vsum;
+      }
+      group_sync(kBarA);
+      const float vsum = s_vsum;
+      const float pr = net->poisson_hz * net->dt;
+      for (int j = gtid; j < M; j += kGroup) {
+        int idx = h * M + j;
+        float a = w_act[j];
+        if (vsum > 1.0f) a /= vsum;
+        st_act[j] = a;
+        st_dsup[j] = w_dsup[j];
+        float u = bx_uniform01(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
+        int8_t spk = (int8_t)(u < a * pop.maxfqdt);
+        if (net->poisson_hz > 0.0f) {
+          float up = bx_uniform01_poisson(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
+          if (up < pr) spk = 1;
+        }
+        st_cnt[j] += spk;
+        w_spk[j] = spk;
+      }
+      if (h == 0 && gtid == 0) pop.dsup[cur][0] = w_dsup[0];
+      /* external spike replay overrides the sampled spikes (Pop.cpp:389-409) */
+      if (pop.ext) {
+        group_sync(kBarA);
+        for (int j = gtid; j < M; j += kGroup) w_spk[j] = 0;
+        group_sync(kBarA);
+        if (simstep >= pop.ext_t0 && simstep < pop.ext_t1) {
+          int b0 = pop.ext_off[simstep - pop.ext_t0], b1 = pop.ext_off[simstep - pop.ext_t0 + 1];
+          for (int e = b0 + gtid; e < b1; e += kGroup) {
+            int v = pop.ext_idx[e];
+            if (v >= h * M && v < h * M + M) w_spk[v - h * M] = 1;
+          }
+        }
+      }
+      group_sync(kBarA);
+      /* ordered list of this HCU's spiking MCUs; publish */
+      int nspk = 0;
+      for (int base = 0; base < M; base += kGroup) {
+        int j = base + gtid;
+        bool f = (j < M) && w_spk[j] > 0;
+        int tot;
+        int pos = group_prefix(f, gtid, kBarA, s_warpA, &s_totalA, &tot);
+        if (f) w_spkl[nspk + pos] = j;
+        nspk += tot;
+      }
+      if (gtid == 0) s_nspk = nspk;
+      {
+        uint32_t* log = pop.spk_log + (size_t)it * pop.log_words;
+        for (int j = gtid; j < M; j += kGroup) {
+          int idx = h * M + j;
+          int8_t sv = w_spk[j];
+          if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
+          for (int q = 0; q < pop.n_out; ++q) net->projs[pop.out_proj[q]].si[cur][idx] = sv;
+        }
+      }
+      /* hand the spike list to group B */
+      asm volatile("bar.arrive %0, %1;" ::"r"(kBarSpikes), "r"(kBlock) : "memory");
+
+      for (int q = 0; q < n_in; ++q) {
+        const int p = pop.in_proj[q];
+        const ProjDev& J = net->projs[p];
+        const int C = J.C;
+        QView V = qview(sm, L, q, M, C);
+        const float kp = J.taupdt * prn;
+        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+        const float4* tab = rp->tab[p];
+        const int tlen = rp->tab_len[p];
+        const size_t eoff = (size_t)J.proj_in_pop * n;
+
+        /* j-traces and bias, Proj.cpp:310-363 */
+        for (int j = gtid; j < M; j += kGroup) {
+          float pj = V.pj[j], ej = V.ej[j], zj = V.zj[j];
+          float e = V.epsc[j];
+          e *= (1 - J.kepsc);
+          pj += (ej - pj) * kp;
+          ej += (zj - ej) * k.ke;
+          zj *= (1 - J.kzj);
+          if (w_spk[j] > 0) zj += J.kftj;
+          if (kp != 0.0f) V.bj[j] = J.bgain * bx_logf(pj + J.eps);
+          V.pj[j] = pj;
+          V.ej[j] = ej;
+          V.zj[j] = zj;
+          V.epsc[j] = e;
+        }
+        if (gtid == 0) {
+          s_flag9 = 0;
+          if (h == 0) pop.bj[cur][eoff] = V.bj[0];
+        }
+        group_sync(kBarA);
+
+        /* row updates of this HCU's active rows, ascending, Proj.cpp:365-479 */
+        const int nrow = V.nlist[cur];
+        const int* list = V.list + cur * C;
+        const int rch = row_chunk_rows(M);
+        const float4* stg_rtr = (const float4*)(sm + L.stg_rtr);
+        const float4* stg_rA = (const float4*)(sm + L.stg_rA);
+        const float4* stg_rB = (const float4*)(sm + L.stg_rB);
+        const float4* stg_cv = (const float4*)(sm + L.stg_cv);
+        const float4* stg_cA = (const float4*)(sm + L.stg_cA);
+        const float4* stg_cB = (const float4*)(sm + L.stg_cB);
+        const int* stg_row = (const int*)(sm + L.stg_row);
+        const int* stg_ti = (const int*)(sm + L.stg_ti);
+        const int* stg_tv = (const int*)(sm + L.stg_tv);
+        const float* stg_wv = sm + L.stg_wv;
+        for (int base = 0; base < nrow; base += rch) {
+          const int nr = (nrow - base) < rch ? (nrow - base) : rch;
+          if (!(q == 0 && base == 0)) {
+            stage_rows(J, list, base, nr, M, simstep, tab, tlen, sm, L, gtid, kGroup);
+            group_sync(kBarA);
+          }
+          for (int t = gtid; t < nr; t += kGroup) {
+            int r = stg_row[t];
+            if (r == 9) s_flag9 = 1;
+            float4 tr = stg_rtr[t];
+            int pdt = simstep - stg_ti[t];
+            if (pdt <= 0) {
+              J.zi[r] = tr.z + J.kfti;
+              J.ti[r] = simstep;
+              w_pi[t] = tr.x;
+            } else {
+              float pi = tr.x, ei = tr.y, zi = tr.z;
+              float4 A = stg_rA[t], B = stg_rB[t];
+              if (pdt >= tlen) load_entry(tab, tlen, k, pdt, 2, A, B);
+              row_decay(pi, ei, zi, k, A, B);
+              zi = zi + J.kfti;
+              J.pi[r] = pi;
+              J.ei[r] = ei;
+              J.zi[r] = zi;
+              J.ti[r] = simstep;
+              w_pi[t] = pi;
+            }
+          }
+          group_sync(kBarA);
+          for (int c = gtid; c < nr * M; c += kGroup) {
+            int rr = c / M;
+            int j = c - rr * M;
+            size_t index = (size_t)stg_row[rr] * M + j;
+            int pdt = simstep - stg_tv[c];
+            float4 cv = stg_cv[c];
+            if (pdt <= 0) {
+              cv.z += J.kfti;
+              J.cell[index] = cv;
+              J.tij[index] = simstep;
+              w_skip[c] = 1;
+            } else {
+              float4 A = stg_cA[c], B = stg_cB[c];
+              if (pdt >= tlen) load_entry(tab, tlen, k, pdt, 0, A, B);
+              cell_decay(cv.x, cv.y, cv.z, cv.w, k, A, B);
+              cv.z = cv.z + J.kfti;
+              J.cell[index] = cv;
+              J.tij[index] = simstep;
+              float w;
+              if (kp != 0.0f) {
+                w = J.wgain * bx_logf((cv.x + J.eps2) / ((w_pi[rr] + J.eps) * (V.pj[j] + J.eps)));
+                J.wij[index] = w;
+              } else {
+                w = stg_wv[c];
+              }
+              w_w[c] = w;
+              w_skip[c] = 0;
+            }
+          }
+          group_sync(kBarA);
+          for (int j = gtid; j < M; j += kGroup) {
+            float e = V.epsc[j];
+            for (int rr = 0; rr < nr; ++rr)
+              if (!w_skip[rr * M + j]) e += w_w[rr * M + j];
+            V.epsc[j] = e;
+          }
+          group_sync(kBarA);
+        }
+        if (gtid == 0) {
+          if (h == 0) pop.epsc[cur][eoff] = V.epsc[0];
+          /* debug flags of ProcSpkRec (ssi/ssj contain index 9) */
+          uint32_t f = 0;
+          if (s_flag9) f |= 1;
+          if (h == 9 / M && 9 < n && w_spk[9 - h * M] > 0) f |= 2;
+          if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + p], f);
+          atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
+        }
+      }
+      /* rows done: group B may now update column cells of active rows */
+      asm volatile("bar.arrive %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
+    } else {
+      /* ================= group B: delay queue, columns =================== */
+      for (int q = 0; q < n_in; ++q) {
+        const ProjDev& J = net->projs[pop.in_proj[q]];
+        const int C = J.C;
+        QView V = qview(sm, L, q, M, C);
+        /* delay queue of this HCU's slots and ordered compaction of the next
+           tick's active rows, Proj.cpp:621-630, 645-664 */
+        const int8_t* si = J.si[prev];
+        int* nlist = V.list + nxt * C;
+        uint32_t* nbits = V.bits + nxt * V.W;
+        int cnt = 0;
+        for (int s0 = 0; s0 < C; s0 += kGroup) {
+          int s = s0 + gtid;
+          bool act = false;
+          if (s < C) {
+            int src = V.ii[s];
+            if (src >= 0) {
+              if (src >= J.Ns) {
+                atomicOr(net->err, kErrIndex);
+              } else {
+                int qv = V.qi[s];
+                act = (qv & 0x01) != 0;
+                qv >>= 1;
+                if (__ldcg(si + src) > 0) qv |= (0x01 << (V.di[s] - 1));
+                V.qi[s] = qv;
+              }
+            }
+          }
+          unsigned m = __ballot_sync(0xffffffffu, act);
+          if ((gtid & 31) == 0 && s < C) nbits[s >> 5] = m;
+          int tot;
+          int pos = group_prefix(act, gtid, kBarB, s_warpB, &s_totalB, &tot);
+          if (act) nlist[cnt + pos] = h * C + s;
+          cnt += tot;
+        }
+        if (gtid == 0) V.nlist[nxt] = cnt;
+      }
+      /* wait for group A's spike list */
+      asm volatile("bar.sync %0, %1;" ::"r"(kBarSpikes), "r"(kBlock) : "memory");
+      const int nspk = s_nspk;
+      /* column updates of this HCU's spiking MCUs, Proj.cpp:481-536.  Pass
+         0: slots whose row is not active this tick; pass 1, after group A's
+         row updates: the cells of active rows.  One code site for both, loads
+         of a batch issued before its compute. */
+      for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) asm volatile("bar.sync %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
+        if (nspk == 0) continue;
+        for (int q = 0; q < n_in; ++q) {
+          const int p = pop.in_proj[q];
+          const ProjDev& J = net->projs[p];
+          const int C = J.C;
+          QView V = qview(sm, L, q, M, C);
+          const float kp = J.taupdt * prn;
+          const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+          const float4* tab = rp->tab[p];
+          const int tlen = rp->tab_len[p];
+          const uint32_t* cbits = V.bits + cur * V.W;
+          const int* clist = V.list + cur * C;
+          const int ncol = (pass == 0) ? nspk * C : V.nlist[cur] * nspk;
+          for (int b0 = 0; b0 < ncol; b0 += kColU * kGroup) {
+            size_t index[kColU];
+            int tv[kColU];
+            float4 cv[kColU];
+            bool ok[kColU];
+#pragma unroll
+            for (int u = 0; u < kColU; ++u) {
+              int c = b0 + u * kGroup + gtid;
+              ok[u] = false;
+              if (c < ncol) {
+                int s, j;
+                if (pass == 0) {
+                  int qq = c / C;
+                  s = c - qq * C;
+                  j = w_spkl[qq];
+                  ok[u] = V.ii[s] >= 0 && !((cbits[s >> 5] >> (s & 31)) & 1u);
+                } else {
+                  int rr = c / nspk;
+                  s = clist[rr] - h * C;
+                  j = w_spkl[c - rr * nspk];
+                  ok[u] = V.ii[s] >= 0;
+                }
+                index[u] = (size_t)(h * C + s) * M + j;
+              }
+              if (ok[u]) {
+                tv[u] = J.tij[index[u]];
+                cv[u] = J.cell[index[u]];
+              }
+            }
+            /* decay-table entries of the whole batch, then the compute */
+            float4 tA[kColU], tB[kColU];
+#pragma unroll
+            for (int u = 0; u < kColU; ++u) {
+              int pdt = simstep - tv[u];
+              if (ok[u] && pdt > 0 && pdt < tlen) {
+                tA[u] = tab[(size_t)pdt * 4 + 0];
+                tB[u] = tab[(size_t)pdt * 4 + 1];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < kColU; ++u) {
+              if (!ok[u]) continue;
+              int pdt = simstep - tv[u];
+              float4 c4 = cv[u];
+              if (pdt <= 0) {
+                c4.w += J.kftj;
+              } else {
+                float4 A = tA[u], B = tB[u];
+                if (pdt >= tlen) cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+                cell_decay(c4.x, c4.y, c4.z, c4.w, k, A, B);
+                c4.w = c4.w + J.kftj;
+              }
+              J.cell[index[u]] = c4;
+              J.tij[index[u]] = simstep;
+            }
+          }
+          if (pass == 0 && gtid == 0) atomicAdd(&net->counters[1], (unsigned long long)nspk * C);
+        }
+      }
+    }
+    __syncthreads();
+
+    /* stage the next tick's first row chunk before the barrier */
+    if (it + 1 < it0 + n_ticks && n_in > 0) {
+      const int p0 = pop.in_proj[0];
+      const ProjDev& J = net->projs[p0];
+      QView V = qview(sm, L, 0, M, J.C);
+      int nr = V.nlist[nxt] < row_chunk_rows(M) ? V.nlist[nxt] : row_chunk_rows(M);
+      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, rp->tab[p0], rp->tab_len[p0], sm, L, tid, kBlock);
+    }
+  }
+
+  /* ---- write the resident state back (buffers of the last tick) --------- */
+  __syncthreads();
+  {
+    const int last = (rp->k0 + it0 + n_ticks - 1) & 1;
+    const int next = last ^ 1;
+    for (int j = tid; j < M; j += kBlock) {
+      int idx = h * M + j;
+      pop.dsup[last][idx] = st_dsup[j];
+      pop.act[idx] = st_act[j];
+      pop.counter[idx] = st_cnt[j];
+      pop.spike[idx] = w_spk[j];
+    }
+    for (int q = 0; q < n_in; ++q) {
+      const ProjDev& J = net->projs[pop.in_proj[q]];
+      QView V = qview(sm, L, q, M, J.C);
+      const size_t eoff = (size_t)J.proj_in_pop * n;
+      for (int j = tid; j < M; j += kBlock) {
+        int idx = h * M + j;
+        J.pj[idx] = V.pj[j];
+        J.ej[idx] = V.ej[j];
+        J.zj[idx] = V.zj[j];
+        pop.epsc[last][eoff + idx] = V.epsc[j];
+        pop.bj[last][eoff + idx] = V.bj[j];
+      }
+      for (int s = tid; s < J.C; s += kBlock) {
+        int r = h * J.C + s;
+        J.qi[r] = V.qi[s];
+        J.list[r] = V.list[next * J.C + s];
+      }
+      if (tid == 0) J.list_cnt[h] = V.nlist[next];
+    }
+  }
+}
+
+/* dynamic shared memory of tick_kernel for the largest population */
+inline size_t tick_smem_bytes_for(int M, int n_in, const int* C) {
+  TickLayout L;
+  tick_layout(M, n_in, C, L);
+  return (size_t)L.total * 4;
+}
+
+}  // namespace bcpnn
+
+#endif /* BCPNN_TICK_CUH */

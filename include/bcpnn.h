@@ -50,7 +50,7 @@ typedef struct bcpnn_net bcpnn_net;
    by ProcUpdLazy/Pop.cpp:17-40. */
 typedef struct bcpnn_pop_desc {
   int32_t hcu_num;
-  int32_t mcu_num;   /* 1 .. 1024 */
+  int32_t mcu_num;   /* 1 .. 512 */
   float taum;
   float wtagain;
   float maxfq;
@@ -89,7 +89,9 @@ typedef struct bcpnn_net_desc {
   int32_t max_ticks_per_run; /* capacity of the per-run spike log             */
 } bcpnn_net_desc;
 
-/* Build a network on the device with gsbn's initial values.
+/* Build a network on the device with gsbn's initial values.  Limits: at most
+   16 populations, 64 projections, 8 projections into one population, 512
+   MCUs per HCU, and one HCU's resident state must fit in shared memory.
    Replaces ProcUpdLazy::init_new (ProcUpdLazy.cpp:8-46), Pop::init_new
    (ProcUpdLazy/Pop.cpp:8-65) and Proj::init_new (ProcUpdLazy/Proj.cpp:6-107). */
 int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out);

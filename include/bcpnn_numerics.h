@@ -12,30 +12,31 @@
  *     replayable).
  *
  *  2. bx_expf / bx_logf: float exp and log written with IEEE-754 basic
- *     operations only (+, -, *, /, sqrt, exact conversions and bit moves).
- *     Every such operation is correctly rounded on x86-64 SSE and on the GPU,
- *     so a host and a device evaluation of the same expression give the same
- *     bits, provided no fused multiply-add is formed (compile host code with
+ *     operations only (+, -, *, /, exact conversions and bit moves).  Every
+ *     such operation is correctly rounded on x86-64 SSE and on the GPU, so a
+ *     host and a device evaluation of the same expression give the same bits,
+ *     provided no fused multiply-add is formed (compile host code with
  *     -ffp-contract=off and device code with -fmad=false).  gsbn evaluates
  *     std::exp(float)/std::log(float) (glibc expf/logf) on the CPU and CUDA
  *     expf/logf on the GPU; those two differ in the last bit and make CPU and
- *     GPU spike trains diverge.  Here the float argument is widened to double,
- *     the function is evaluated to about 1e-15 relative error and rounded once
- *     to float, so the result is the correctly rounded value except when the
- *     exact value lies within ~1e-15 (relative) of a float rounding boundary.
+ *     GPU spike trains diverge.  These are evaluated in float (they sit on
+ *     the per-cell path of the kernels) and stay within 2 ulp of the
+ *     correctly rounded result (tests/test_numerics.py measures it).
+ *     Double-precision versions (bx_exp_d, bx_log_d) serve host-side
+ *     initial values and the Box-Muller transform.
  *
  *     Methods (textbook, no vendor code):
  *       exp: Cody & Waite additive range reduction x = k ln2 + r with a
- *            two-part ln2, |r| <= ln2/2, degree-14 Taylor polynomial of e^r in
- *            Horner form, exact scaling by 2^k (W. J. Cody, W. Waite,
+ *            two-part ln2, |r| <= ln2/2, Taylor polynomial of e^r in Horner
+ *            form, exact scaling by 2^k in two steps (W. J. Cody, W. Waite,
  *            "Software Manual for the Elementary Functions", 1980, ch. 6).
  *       log: x = 2^e m with m in [sqrt(2)/2, sqrt(2)), log m = 2 atanh(s),
- *            s = (m-1)/(m+1), odd power series of atanh to s^27
- *            (Abramowitz & Stegun 4.1.27 / 4.6.22).
+ *            s = (m-1)/(m+1), odd power series of atanh (Abramowitz &
+ *            Stegun 4.1.27 / 4.6.22), e ln2 added with a two-part ln2.
  *       cos(2 pi u): reduction to [-pi/2, pi/2] by symmetry and an even
  *            Taylor series to x^26.
- *     All coefficients are exact values of 1/n! and 1/(2n+1) rounded to
- *     double, written as hexadecimal literals.
+ *     All coefficients are exact values of 1/n!, 2/(2n+1) and 1/(2n+1)
+ *     rounded to the working precision, written as hexadecimal literals.
  */
 #ifndef BCPNN_NUMERICS_H
 #define BCPNN_NUMERICS_H
@@ -132,12 +133,37 @@ BX_HD double bx_exp_d(double x) {
   return (p * s1) * s2;
 }
 
-/* float exp with one final rounding (see header comment). */
-BX_HD float bx_expf(float xf) {
-  if (xf != xf) return xf;                          /* NaN */
-  if (xf > 89.0f) return bx_bitsf(0x7f800000u);     /* +inf */
-  if (xf < -104.0f) return 0.0f;                    /* below half the least subnormal */
-  return (float)bx_exp_d((double)xf);
+/* float exp (see header comment): e^x = 2^k e^r, k = rint(x log2 e).
+   Branch-free: out-of-range inputs are clamped for the computation and the
+   special results selected at the end, so independent calls can overlap. */
+BX_HD float bx_expf(float x) {
+  const float LOG2E = 0x1.715476p+0f;
+  const float LN2_HI = 0x1.62e4p-1f;                 /* 16 significant bits: k*LN2_HI exact for |k| <= 256 */
+  const float LN2_LO = 0x1.7f7d1cp-20f;
+  const float SHIFT = 0x1.8p23f;                     /* adding and removing it rounds to an integer */
+  float xc = x < -104.0f ? -104.0f : x;
+  xc = xc > 89.0f ? 89.0f : xc;
+  xc = (x != x) ? 0.0f : xc;
+  float t = xc * LOG2E + SHIFT;
+  float kf = t - SHIFT;
+  float r = (xc - kf * LN2_HI) - kf * LN2_LO;        /* |r| <= ln2/2 + 2^-20 */
+  float p = 0x1.a01a02p-16f;                         /* 1/8! */
+  p = p * r + 0x1.a01a02p-13f;                       /* 1/7! */
+  p = p * r + 0x1.6c16c2p-10f;                       /* 1/6! */
+  p = p * r + 0x1.111112p-7f;                        /* 1/5! */
+  p = p * r + 0x1.555556p-5f;                        /* 1/4! */
+  p = p * r + 0x1.555556p-3f;                        /* 1/3! */
+  p = p * r + 0.5f;
+  p = p * r + 1.0f;
+  p = p * r + 1.0f;
+  int k = (int)(bx_fbits(t) - 0x4B400000u);          /* kf as an integer, in [-151, 129] */
+  int k1 = k >> 1, k2 = k - k1;                      /* both in [-76, 65]: normal powers of two */
+  float s1 = bx_bitsf((uint32_t)(k1 + 127) << 23);
+  float s2 = bx_bitsf((uint32_t)(k2 + 127) << 23);
+  float res = (p * s1) * s2;                         /* exact, then one rounding (subnormal or overflow) */
+  res = x > 89.0f ? bx_bitsf(0x7f800000u) : res;     /* +inf */
+  res = x < -104.0f ? 0.0f : res;                    /* below half the least subnormal */
+  return (x != x) ? x : res;                         /* NaN */
 }
 
 /* ------------------------------------------------------------------------ */
@@ -173,13 +199,33 @@ BX_HD double bx_log_d(double x) {
   return ed * LN2_HI + (ed * LN2_LO + lm);
 }
 
-/* float log with one final rounding. */
-BX_HD float bx_logf(float xf) {
-  if (xf != xf) return xf;                                  /* NaN */
-  if (xf < 0.0f) return bx_bitsf(0x7fc00000u);              /* NaN */
-  if (xf == 0.0f) return bx_bitsf(0xff800000u);             /* -inf */
-  if (bx_fbits(xf) == 0x7f800000u) return xf;               /* +inf */
-  return (float)bx_log_d((double)xf);
+/* float log (see header comment).  Branch-free like bx_expf. */
+BX_HD float bx_logf(float x) {
+  const float LN2_HI = 0x1.62e4p-1f;
+  const float LN2_LO = 0x1.7f7d1cp-20f;
+  const float SQRT2 = 0x1.6a09e6p+0f;
+  const bool sub = x < 0x1p-126f;                           /* subnormal (or non-positive) */
+  float xs = sub ? x * 0x1p23f : x;                          /* scale subnormals into the normal range */
+  uint32_t b = bx_fbits(xs);
+  int e = (int)((b >> 23) & 0xffu) - 127 - (sub ? 23 : 0);
+  float m = bx_bitsf((b & 0x007fffffu) | 0x3f800000u);      /* [1, 2) */
+  const bool hi = m > SQRT2;
+  m = hi ? m * 0.5f : m;
+  e = hi ? e + 1 : e;
+  float s = (m - 1.0f) / (m + 1.0f);                         /* |s| <= 0.1716 */
+  float z = s * s;
+  float p = 0x1.745d18p-3f;                                  /* 2/11 */
+  p = p * z + 0x1.c71c72p-3f;                                /* 2/9 */
+  p = p * z + 0x1.24924ap-2f;                                /* 2/7 */
+  p = p * z + 0x1.99999ap-2f;                                /* 2/5 */
+  p = p * z + 0x1.555556p-1f;                                /* 2/3 */
+  float lm = (s + s) + (s * z) * p;
+  float ef = (float)e;
+  float res = ef * LN2_HI + (ef * LN2_LO + lm);
+  res = (bx_fbits(x) == 0x7f800000u) ? x : res;              /* +inf */
+  res = (x == 0.0f) ? bx_bitsf(0xff800000u) : res;           /* -inf */
+  res = (x < 0.0f) ? bx_bitsf(0x7fc00000u) : res;            /* NaN */
+  return (x != x) ? x : res;                                 /* NaN */
 }
 
 /* ------------------------------------------------------------------------ */

@@ -6,6 +6,8 @@ run, for the 10x10 workload, the two-population workload with Poisson input
 noise, a reduced copy of the 100x100 workload, external spike replay, and the
 all-cells catch-up at every change of prn.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -16,11 +18,31 @@ from tests.harness import first_mismatch, load_workload, schedule, state
 pytestmark = pytest.mark.gpu
 
 
-def make_pair(w, directory, max_ticks=256, exchange=True):
+def gpu_net(*args, per_tick=False, **kw):
+    """a capi.Net on the persistent cooperative path (default) or on the
+    one-launch-per-tick path"""
+    old = os.environ.get("GSBN_PER_TICK")
+    os.environ["GSBN_PER_TICK"] = "1" if per_tick else "0"
+    try:
+        return capi.Net(*args, **kw)
+    finally:
+        if old is None:
+            del os.environ["GSBN_PER_TICK"]
+        else:
+            os.environ["GSBN_PER_TICK"] = old
+
+
+@pytest.fixture(params=["persistent", "per_tick"])
+def mode(request):
+    return request.param == "per_tick"
+
+
+def make_pair(w, directory, max_ticks=256, exchange=True, per_tick=False):
     sp, pops, projs, stim, conn, seed, phz = load_workload(w, str(directory))
     dt = float(np.float32(sp.gen_param.dt))
     orc = sim.OracleNet(pops, projs, dt, seed=seed, poisson_hz=phz)
-    gpu = capi.Net(pops, projs, dt, seed=seed, poisson_hz=phz, exchange=exchange, max_ticks=max_ticks)
+    gpu = gpu_net(pops, projs, dt, seed=seed, poisson_hz=phz, exchange=exchange, max_ticks=max_ticks,
+                  per_tick=per_tick)
     for k, (ii, di) in enumerate(conn):
         orc.set_conn(k, ii, di)
         gpu.set_conn(k, ii, di)
@@ -55,8 +77,8 @@ def compare_runs(pops, projs, orc, gpu, runs, full_every_run=True, limit=None):
     return n_spikes
 
 
-def test_config0_tick_by_tick(tmp_path):
-    sp, pops, projs, orc, gpu, runs = make_pair(workloads.config0(), tmp_path)
+def test_config0_tick_by_tick(tmp_path, mode):
+    sp, pops, projs, orc, gpu, runs = make_pair(workloads.config0(), tmp_path, per_tick=mode)
     ticks = 0
     for r in runs:
         orc.set_stimulus(r.lginp, r.wmask)
@@ -74,31 +96,31 @@ def test_config0_tick_by_tick(tmp_path):
     assert orc.counters() == gpu.counters()
 
 
-def test_config0_runs(tmp_path):
-    sp, pops, projs, orc, gpu, runs = make_pair(workloads.config0(), tmp_path)
+def test_config0_runs(tmp_path, mode):
+    sp, pops, projs, orc, gpu, runs = make_pair(workloads.config0(), tmp_path, per_tick=mode)
     n = compare_runs(pops, projs, orc, gpu, runs)
     assert n > 100
     assert orc.counters() == gpu.counters()
 
 
-def test_config2_two_projections_poisson(tmp_path):
+def test_config2_two_projections_poisson(tmp_path, mode):
     w = workloads.config2(n_patterns=12, train_ticks=80, recall_ticks=20)
-    sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path)
+    sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path, per_tick=mode)
     n = compare_runs(pops, projs, orc, gpu, runs)
     assert n > 100
     assert orc.counters() == gpu.counters()
 
 
-def test_reduced_100x100(tmp_path):
+def test_reduced_100x100(tmp_path, mode):
     w = workloads.small_scale(hcu=24, mcu=20, src=6, n_patterns=8, train_ticks=50, recall_ticks=30)
-    sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path)
+    sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path, per_tick=mode)
     compare_runs(pops, projs, orc, gpu, runs, full_every_run=False)
     assert orc.counters() == gpu.counters()
 
 
-def test_external_spike_replay(tmp_path):
+def test_external_spike_replay(tmp_path, mode):
     w = workloads.config0()
-    sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path)
+    sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path, per_tick=mode)
     rng = np.random.default_rng(7)
     table = {}
     for t in range(1, 2201):
@@ -112,7 +134,7 @@ def test_external_spike_replay(tmp_path):
 def test_no_exchange_keeps_si_zero(tmp_path):
     w = workloads.config0()
     sp, pops, projs, stim, conn, seed, phz = load_workload(w, str(tmp_path))
-    gpu = capi.Net(pops, projs, 0.001, seed=seed, exchange=False, max_ticks=256)
+    gpu = gpu_net(pops, projs, 0.001, seed=seed, exchange=False, max_ticks=256)
     for k, (ii, di) in enumerate(conn):
         gpu.set_conn(k, ii, di)
     r = schedule(sp, stim, pops, lambda x: np.float32(np.log(x)))[0]
@@ -122,12 +144,13 @@ def test_no_exchange_keeps_si_zero(tmp_path):
     assert gpu.counters()[0] == 0
 
 
-def test_determinism_and_graph_replay(tmp_path):
-    """the same run twice gives the same bits; a run cut into one-tick calls
-    gives the same bits as one call (graph replay of cached run lengths)."""
+def test_determinism_and_paths(tmp_path):
+    """a run on the persistent path and the same run cut into one-tick calls on
+    the per-tick path (CUDA-graph replay of cached run lengths) give the same
+    bits."""
     w = workloads.config0()
     sp, pops, projs, orc, a, runs = make_pair(w, tmp_path / "a")
-    _, _, _, _, b, _ = make_pair(w, tmp_path / "b")
+    _, _, _, _, b, _ = make_pair(w, tmp_path / "b", per_tick=True)
     for r in runs[:6]:
         for net in (a, b):
             net.set_stimulus(r.lginp, r.wmask)
