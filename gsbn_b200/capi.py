@@ -20,7 +20,7 @@ EXPORTS = (
     "bcpnn_net_create", "bcpnn_net_destroy", "bcpnn_set_conn", "bcpnn_set_stimulus", "bcpnn_upload_stimuli",
     "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
     "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_ss_flags",
-    "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_counters", "bcpnn_kernel_launches",
+    "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_read_state_noalloc", "bcpnn_counters", "bcpnn_kernel_launches",
     "bcpnn_last_error", "bcpnn_status_string",
 )
 
@@ -84,6 +84,7 @@ def load():
         "bcpnn_state_info": (ctypes.c_int, [vp, ctypes.c_char_p, P(i32), P(sz)]),
         "bcpnn_read_state": (ctypes.c_int, [vp, ctypes.c_char_p, vp, sz]),
         "bcpnn_write_state": (ctypes.c_int, [vp, ctypes.c_char_p, vp, sz]),
+        "bcpnn_read_state_noalloc": (ctypes.c_int, [vp, ctypes.c_char_p, vp, sz]),
         "bcpnn_counters": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_kernel_launches": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_last_error": (ctypes.c_char_p, [vp]),
@@ -212,6 +213,13 @@ class Net:
         t, n = self.info(name)
         out = np.zeros(n, dtype=_NP[t])
         self._check(self._lib.bcpnn_read_state(self._h, name.encode(), _ptr(out), out.nbytes))
+        return out
+
+    def read_noalloc(self, name):
+        """bcpnn_read_state_noalloc: the same read without any device allocation."""
+        t, n = self.info(name)
+        out = np.zeros(n, dtype=_NP[t])
+        self._check(self._lib.bcpnn_read_state_noalloc(self._h, name.encode(), _ptr(out), out.nbytes))
         return out
 
     def write(self, name, arr):

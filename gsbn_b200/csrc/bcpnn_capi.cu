@@ -1046,3 +1046,124 @@ int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out) {
 }
 
 }  // extern "C"
+
+/* ======================================================================== */
+/* Allocation-free read of a state vector                                    */
+/* ======================================================================== */
+
+/* Scratch of bcpnn_read_state_noalloc: a file-scope device array that every
+   GPU loading this library holds until the process exits.  Host code only
+   uses its device address from cudaGetSymbolAddress; the name itself is a
+   host-side stand-in. */
+static constexpr size_t kNoAllocScratchFloats = (size_t)1 << 20; /* 4 MiB */
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+static constexpr int kNoAllocMaxDevices = 64;
+static float* g_noalloc_scratch_dev[kNoAllocMaxDevices];  /* device address per ordinal, set on first use */
+
+namespace {
+
+/* name -> vector, like resolve() but without building any std::string; the
+   delay-queue view .siq_<proj> (assembled on the host) is not offered */
+bool resolve_noalloc(const bcpnn_net* net, const char* name, Resolved* r) {
+  const char* us = std::strrchr(name, '_');
+  if (!us || !us[1]) return false;
+  char base[16];
+  size_t blen = (size_t)(us - name);
+  if (blen == 0 || blen >= sizeof(base)) return false;
+  std::memcpy(base, name, blen);
+  base[blen] = '\0';
+  int id = 0;
+  for (const char* c = us + 1; *c; ++c) {
+    if (*c < '0' || *c > '9' || id > 100000) return false;
+    id = id * 10 + (*c - '0');
+  }
+  auto is = [&](const char* b) { return std::strcmp(base, b) == 0; };
+  r->proj = id;
+  if (id < (int)net->pops.size()) {
+    const PopHost& P = net->pops[id];
+    const PopDev& D = net->h.pops[id];
+    size_t n = (size_t)P.n;
+    auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
+    auto parity = [&](float* a, float* b, size_t count) { r->kind = K_PARITY; r->par[0] = a; r->par[1] = b; r->type = BCPNN_F32; r->count = count; return true; };
+    if (is("dsup")) return parity(D.dsup[0], D.dsup[1], n);
+    if (is("epsc")) return parity(D.epsc[0], D.epsc[1], n * P.dim_proj);
+    if (is("bj")) return parity(D.bj[0], D.bj[1], n * P.dim_proj);
+    if (is("act")) return plain(D.act, BCPNN_F32, n);
+    if (is("spike")) return plain(D.spike, BCPNN_I8, n);
+    if (is(".counter")) return plain(D.counter, BCPNN_I32, n);
+  }
+  if (id < (int)net->projs.size()) {
+    const ProjHost& J = net->projs[id];
+    const ProjDev& D = net->h.projs[id];
+    size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
+    auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
+    auto cell = [&](int f) { r->kind = K_CELL; r->field = f; r->cell = D.cell; r->type = BCPNN_F32; r->count = cells; return true; };
+    if (is("ii")) return plain(D.ii, BCPNN_I32, R);
+    if (is("di")) return plain(D.di, BCPNN_I32, R);
+    if (is("qi")) return plain(D.qi, BCPNN_I32, R);
+    if (is("pi")) return plain(D.pi, BCPNN_F32, R);
+    if (is("ei")) return plain(D.ei, BCPNN_F32, R);
+    if (is("zi")) return plain(D.zi, BCPNN_F32, R);
+    if (is("ti")) return plain(D.ti, BCPNN_I32, R);
+    if (is("pj")) return plain(D.pj, BCPNN_F32, HM);
+    if (is("ej")) return plain(D.ej, BCPNN_F32, HM);
+    if (is("zj")) return plain(D.zj, BCPNN_F32, HM);
+    if (is("tij")) return plain(D.tij, BCPNN_I32, cells);
+    if (is("wij")) return plain(D.wij, BCPNN_F32, cells);
+    if (is("pij")) return cell(0);
+    if (is("eij")) return cell(1);
+    if (is("zi2")) return cell(2);
+    if (is("zj2")) return cell(3);
+    if (is("si")) { r->kind = K_SI; r->par[0] = D.si[0]; r->par[1] = D.si[1]; r->type = BCPNN_I8; r->count = (size_t)J.Ns; return true; }
+  }
+  return false;
+}
+
+}  // namespace
+
+extern "C" int bcpnn_read_state_noalloc(bcpnn_net* net, const char* name, void* host, size_t bytes) {
+  if (!net) return BCPNN_ERR_INVALID;
+  Resolved r;
+  if (!name || !resolve_noalloc(net, name, &r))
+    return fail(net, BCPNN_ERR_NOT_FOUND, "bcpnn_read_state_noalloc: unknown state vector (or .siq_, not offered)");
+  if (!host || bytes != r.count * type_size(r.type))
+    return fail(net, BCPNN_ERR_SIZE, "bcpnn_read_state_noalloc: size mismatch");
+  if (r.kind == K_CELL && r.count > kNoAllocScratchFloats)
+    return fail(net, BCPNN_ERR_SIZE, "bcpnn_read_state_noalloc: the vector has more elements than the static "
+                                     "scratch holds (1048576 floats); use bcpnn_read_state");
+  if (net->device < 0 || net->device >= kNoAllocMaxDevices)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_read_state_noalloc: device ordinal beyond 63");
+  CU(cudaSetDevice(net->device));
+  const int last = (int)((net->k_total - 1) & 1);
+  switch (r.kind) {
+    case K_PLAIN:
+      CU(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    case K_PARITY:
+    case K_SI:
+      CU(cudaMemcpyAsync(host, r.par[last], bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    case K_CELL: {
+      /* set-up, once per device with that device current: the device address
+         of the static scratch */
+      float* scratch = g_noalloc_scratch_dev[net->device];
+      if (!scratch) {
+        void* p = nullptr;
+        CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        scratch = (float*)p;
+        g_noalloc_scratch_dev[net->device] = scratch;
+      }
+      /* every element read back is written by the gather first, so nothing
+         of an earlier call's contents is used */
+      cell_gather_kernel<<<grid_for(r.count, 256), 256, 0, net->stream>>>(r.cell, r.count, r.field, scratch);
+      CU(cudaGetLastError());
+      net->launches++;
+      CU(cudaMemcpyAsync(host, scratch, bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    }
+    default:
+      return fail(net, BCPNN_ERR_NOT_FOUND, "bcpnn_read_state_noalloc: vector not offered");
+  }
+  CU(cudaStreamSynchronize(net->stream));
+  return BCPNN_OK;
+}
