@@ -122,6 +122,21 @@ def build_schedule(work_dir):
     return w, sp, pops, projs, stim, conn, runs
 
 
+def combine_over_ranks(seconds, units, device):
+    """Whole-job figures of a replicated run: the slowest rank's time and the
+    units all ranks processed (torch.distributed must be initialised when
+    more than one rank runs)."""
+    import torch
+    if not torch.distributed.is_available() or not torch.distributed.is_initialized() or \
+            torch.distributed.get_world_size() == 1:
+        return seconds, units
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    torch.distributed.all_reduce(u, op=torch.distributed.ReduceOp.SUM)
+    return float(t[0]), float(u[0])
+
+
 def algorithmic_bytes(pops, projs, row_cells, col_cells, ticks):
     """Bytes the reference algorithm must move per tick, summed: 44 B per row
     cell, 40 B per column cell, 16 B per slot of the delay queue, 24 B per
@@ -197,12 +212,7 @@ def run_ours(args, rank, world, local_rank):
                 tk_ms += per_run[s][i][0].elapsed_time(per_run[s][i][1])
                 tk_ticks += r.n
     tick_us = tk_ms * 1e3 / max(1, tk_ticks)
-    if world > 1:
-        t = torch.tensor([ms, float(cells)], dtype=torch.float64, device=f"cuda:{dev}")
-        mx = t.clone()
-        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
-        ms, cells = float(mx[0]), float(t[1])
+    ms, cells = combine_over_ranks(ms, cells, f"cuda:{dev}")
 
     # e2e: host buffers through the C ABI, spike logs read back, recall on host
     pin_lg = [torch.empty(lgidx.shape[1], dtype=torch.int32, pin_memory=True).numpy() for r in runs]
@@ -236,12 +246,7 @@ def run_ours(args, rank, world, local_rank):
     net.sync()
     e_s = time.perf_counter() - t0
     e_cells = sum(net.counters()) - e0
-    if world > 1:
-        t = torch.tensor([e_s, float(e_cells)], dtype=torch.float64, device=f"cuda:{dev}")
-        mx = t.clone()
-        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
-        e_s, e_cells = float(mx[0]), float(t[1])
+    e_s, e_cells = combine_over_ranks(e_s, e_cells, f"cuda:{dev}")
 
     out = None
     if rank == 0:

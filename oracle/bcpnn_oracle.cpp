@@ -822,6 +822,28 @@ void oracle_counters(void* hp, unsigned long long* out3) {
 }
 
 float oracle_expf(int math, float x) { return Fn<float>::exp(math, x); }
+
+/* element-wise exp/log of an array (shared or libm definition) */
+void oracle_expf_array(int math, long long n, const float* in, float* out) {
+  for (long long i = 0; i < n; ++i) out[i] = Fn<float>::exp(math, in[i]);
+}
+void oracle_logf_array(int math, long long n, const float* in, float* out) {
+  for (long long i = 0; i < n; ++i) out[i] = Fn<float>::log(math, in[i]);
+}
+
+/* Philox4x32-10 block and the stream map, for the known-answer tests */
+void oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  bx_u32x4 c;
+  for (int i = 0; i < 4; ++i) c.v[i] = ctr[i];
+  bx_u32x4 o = bx_philox4x32_10(c, key[0], key[1]);
+  for (int i = 0; i < 4; ++i) out[i] = o.v[i];
+}
+void oracle_uniform_array(uint32_t seed, uint32_t pop, uint32_t tick, int n, float* out) {
+  for (int i = 0; i < n; ++i) out[i] = bx_uniform01(seed, pop, tick, (uint32_t)i);
+}
+void oracle_normal_array(uint32_t seed, uint32_t pop, uint32_t tick, int n, float* out) {
+  for (int i = 0; i < n; ++i) out[i] = bx_normal01(seed, pop, tick, (uint32_t)i);
+}
 float oracle_logf(int math, float x) { return Fn<float>::log(math, x); }
 double oracle_log_double(int math, double x) { return log_double(math, x); }
 

@@ -62,12 +62,51 @@ def load():
     lib.oracle_logf.argtypes = [i32, fl]
     lib.oracle_log_double.restype = ctypes.c_double
     lib.oracle_log_double.argtypes = [i32, ctypes.c_double]
+    lib.oracle_expf_array.argtypes = [i32, ctypes.c_longlong, vp, vp]
+    lib.oracle_logf_array.argtypes = [i32, ctypes.c_longlong, vp, vp]
+    lib.oracle_philox.argtypes = [vp, vp, vp]
+    lib.oracle_uniform_array.argtypes = [u32, u32, u32, i32, vp]
+    lib.oracle_normal_array.argtypes = [u32, u32, u32, i32, vp]
     _lib = lib
     return lib
 
 
 def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def expf(x, math=MATH_SHARED):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    load().oracle_expf_array(math, x.size, _p(x), _p(out))
+    return out
+
+
+def logf(x, math=MATH_SHARED):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    load().oracle_logf_array(math, x.size, _p(x), _p(out))
+    return out
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, np.uint32)
+    load().oracle_philox(_p(c), _p(k), _p(out))
+    return out
+
+
+def uniforms(seed, pop, tick, n):
+    out = np.zeros(n, np.float32)
+    load().oracle_uniform_array(seed, pop, tick, n, _p(out))
+    return out
+
+
+def normals(seed, pop, tick, n):
+    out = np.zeros(n, np.float32)
+    load().oracle_normal_array(seed, pop, tick, n, _p(out))
+    return out
 
 
 POP_KEYS = ("taum", "wtagain", "maxfq", "igain", "wgain", "lgbias", "snoise")

@@ -1,0 +1,72 @@
+"""The C ABI library without a GPU: it loads, exports every entry point that
+include/bcpnn.h declares, and rejects invalid network descriptions before it
+touches a device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from gsbn_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", h)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names |= set(re.findall(r"\b(bcpnn_[a-z_0-9]+)\s*\(", text))
+    return names
+
+
+def test_every_declared_entry_point_is_exported():
+    lib = capi.load()
+    names = declared()
+    assert len(names) >= 20
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert names <= set(capi.EXPORTS), sorted(names - set(capi.EXPORTS))
+
+
+def test_status_strings():
+    lib = capi.load()
+    assert lib.bcpnn_status_string(0) == b"ok"
+    assert lib.bcpnn_status_string(-3) == b"unknown state vector"
+    assert lib.bcpnn_status_string(-99) == b"unknown status"
+
+
+POP = dict(hcu_num=2, mcu_num=3, taum=0.01, wtagain=1.0, maxfq=100.0, igain=1.0, wgain=1.0, lgbias=0.0, snoise=0.0)
+PROJ = dict(src_pop=0, dest_pop=0, tauzi=0.01, tauzj=0.01, taue=0.02, taup=1.0, maxfq=100.0, bgain=1.0, wgain=1.0,
+            tauepsc=0.0, slot_num=6.0)
+
+
+@pytest.mark.parametrize("pops,projs,kw", [
+    ([], [], {}),
+    ([dict(POP, mcu_num=0)], [], {}),
+    ([dict(POP, mcu_num=513)], [], {}),
+    ([POP], [dict(PROJ, dest_pop=1)], {}),
+    ([POP], [dict(PROJ, slot_num=0.0)], {}),
+    ([POP], [PROJ] * 9, {}),
+    ([POP], [PROJ], dict(dt=0.0)),
+    ([POP], [PROJ], dict(max_ticks=0)),
+])
+def test_invalid_descriptions_are_rejected(pops, projs, kw):
+    args = dict(dt=0.001, max_ticks=16)
+    args.update(kw)
+    dt = args.pop("dt")
+    with pytest.raises(capi.BcpnnError) as e:
+        capi.Net(pops, projs, dt, **args)
+    assert e.value.status == -1
+
+
+def test_null_handle_calls_fail_cleanly():
+    lib = capi.load()
+    assert lib.bcpnn_run(None, 1, 1, 1.0, 0.0) == -1
+    assert lib.bcpnn_sync(None) == -1
+    assert lib.bcpnn_net_destroy(None) == -1
+    assert lib.bcpnn_last_error(None) == b"null handle"
+    out = ctypes.c_void_p()
+    assert lib.bcpnn_net_create(None, ctypes.byref(out)) == -1
