@@ -1,0 +1,169 @@
+"""The host engine end to end on the GPU: prototxt network descriptions run
+through the procedure registry (ProcExtGen, ProcUpdLazy, ProcExchangeSpike,
+ProcInitConn, ProcSpkRec, ProcCheck, ProcSnapshot) must write the same record
+files, byte for byte, as the CPU oracle's restatement of gsbn's procedures,
+whether ticks run one device launch per stimulus segment or one per tick.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from gsbn_b200 import engine, schema, workloads
+from oracle import sim
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GSBN_SIM = os.path.join(os.path.dirname(HERE), "gsbn_b200", "gsbn_sim")
+
+
+def write(w, directory, edit=None):
+    path = w.write(str(directory))
+    if edit:
+        with open(path) as f:
+            text = edit(f.read())
+        with open(path, "w") as f:
+            f.write(text)
+    with open(path) as f:
+        sp = schema.parse_prototxt(f.read())
+    return path, sp
+
+
+def rec_files(sp):
+    d = sp.rec_param.directory
+    out = {}
+    for sub in ("ProcSpkRec", "ProcCheck"):
+        p = os.path.join(d, sub)
+        if os.path.isdir(p):
+            for name in sorted(os.listdir(p)):
+                with open(os.path.join(p, name)) as f:
+                    out[f"{sub}/{name}"] = f.read()
+    return out
+
+
+def oracle_files(sp, directory, **kw):
+    ref = sim.simulate(sp, str(directory), **kw)
+    files = {f"ProcSpkRec/{k}": v for k, v in ref["rec"].items()}
+    if ref["check"]:
+        files["ProcCheck/check_result.txt"] = "\n".join(ref["check"]) + "\n"
+    return files, ref
+
+
+def run(path, windows=True, snapshot=None):
+    s = engine.Solver(path, snapshot)
+    s.run(windows)
+    st = s.stats()
+    s.close()
+    return st
+
+
+def test_config0_matches_oracle_files(tmp_path):
+    path, sp = write(workloads.config0(), tmp_path)
+    st = run(path)
+    got = rec_files(sp)
+    want, ref = oracle_files(sp, tmp_path)
+    assert set(got) == set(want)
+    for name in want:
+        assert got[name] == want[name], name
+    assert (st["correct"], st["patterns"]) == ref["correct"]
+    assert st["ticks"] == ref["simstep"]
+    assert st["windows"] < st["ticks"] / 20  # one device run per segment
+
+
+def test_windows_equal_ticks(tmp_path):
+    w = workloads.config0()
+    pa, spa = write(w, tmp_path / "a")
+    pb, spb = write(w, tmp_path / "b")
+    run(pa, windows=True)
+    st = run(pb, windows=False)
+    assert st["windows"] == 0
+    fa, fb = rec_files(spa), rec_files(spb)
+    assert fa == fb
+
+
+def test_two_populations_poisson(tmp_path):
+    w = workloads.config2(n_patterns=12, train_ticks=80, recall_ticks=20)
+    path, sp = write(w, tmp_path)
+    st = run(path)
+    got = rec_files(sp)
+    want, ref = oracle_files(sp, tmp_path)
+    for name in want:
+        assert got[name] == want[name], name
+    assert (st["correct"], st["patterns"]) == ref["correct"]
+
+
+def test_external_spike_file(tmp_path):
+    rng = np.random.default_rng(11)
+    lines = []
+    for t in range(1, 400):
+        k = int(rng.integers(0, 4))
+        idx = sorted(rng.choice(100, size=k, replace=False).tolist())
+        if idx:
+            lines.append(",".join(str(v) for v in [t, 0] + idx))
+    lines.append("5,0,1,2")  # a later line for a tick replaces the earlier one
+    ext = tmp_path / "ext.csv"
+    ext.write_text("\n".join(lines) + "\n")
+
+    def edit(text):
+        return text.replace('name: "ProcUpdLazy"', f'name: "ProcUpdLazy"\n  args {{ key: "external spike" val: "{ext}" }}')
+
+    path, sp = write(workloads.config0(), tmp_path, edit)
+    run(path)
+    got = rec_files(sp)
+    want, _ = oracle_files(sp, tmp_path)
+    assert got["ProcSpkRec/spk_pop_0.csv"] == want["ProcSpkRec/spk_pop_0.csv"]
+    assert "5,1,2\n" in got["ProcSpkRec/spk_pop_0.csv"]
+
+
+def test_snapshot_and_restore(tmp_path):
+    dt = np.float32(0.001)
+    t_snap = 1650
+    assert int(np.float32(np.float32(t_snap) * dt) / dt) == t_snap
+
+    def with_snapshot(text):
+        return text + f'proc_param {{ name: "ProcSnapshot" argi {{ key: "period" val: {t_snap} }} ' \
+                      f'argi {{ key: "offset" val: {t_snap} }} }}\n'
+
+    w = workloads.config0()
+    path, sp = write(w, tmp_path / "full", with_snapshot)
+    run(path)
+    snap_dir = os.path.join(sp.rec_param.directory, "ProcSnapshot")
+    names = os.listdir(snap_dir)
+    assert len(names) == 1 and names[0].startswith("Snapshot_1.65")
+    st = schema.SolverState()
+    with open(os.path.join(snap_dir, names[0]), "rb") as f:
+        st.ParseFromString(f.read())
+    assert st.prn == 0.0
+    vecs = {v.name: np.array(v.data, np.float32) for v in st.vector_state_f32}
+    vecs.update({v.name: np.array(v.data, np.int32) for v in st.vector_state_i32})
+    vecs.update({v.name: np.array(v.data, np.int8) for v in st.vector_state_i8})
+    # against the oracle's state after the same tick
+    ref = sim.simulate(sp, str(tmp_path / "full"), max_ticks=t_snap)
+    assert ref["simstep"] == t_snap
+    for name in ("pij_0", "eij_0", "zi2_0", "zj2_0", "tij_0", "wij_0", "pi_0", "ei_0", "zi_0", "ti_0", "pj_0",
+                 "ej_0", "zj_0", "qi_0", "ii_0", "di_0", "si_0", "dsup_0", "act_0", "epsc_0", "bj_0", "spike_0"):
+        a = ref["net"].read(name)
+        b = vecs[name].astype(a.dtype)
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), name
+    # restore and run to the end: the spikes after the snapshot match the uninterrupted run
+    path2, sp2 = write(w, tmp_path / "restored")
+    run(path2, snapshot=os.path.join(snap_dir, names[0]))
+    full = rec_files(sp)["ProcSpkRec/spk_pop_0.csv"].splitlines()
+    rest = rec_files(sp2)["ProcSpkRec/spk_pop_0.csv"].splitlines()
+    after = [l for l in full[1:] if int(l.split(",")[0]) > t_snap]
+    assert rest[0] == full[0]
+    assert rest[1:] == after
+    assert len(after) > 50
+
+
+def test_gsbn_sim_command(tmp_path):
+    path, sp = write(workloads.config0(), tmp_path)
+    r = subprocess.run([GSBN_SIM, "-n", path, "-m", "GPU"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "correct pattern:" in r.stdout and "Total time for [2.2" in r.stdout
+    want, _ = oracle_files(sp, tmp_path)
+    assert rec_files(sp)["ProcSpkRec/spk_pop_0.csv"] == want["ProcSpkRec/spk_pop_0.csv"]
+    bad = subprocess.run([GSBN_SIM, "-n", path, "-m", "CPU"], capture_output=True, text=True, timeout=300)
+    assert bad.returncode == 1 and "no CPU path" in bad.stderr
