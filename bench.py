@@ -15,7 +15,7 @@ timed with CUDA events on the library's stream, stimulus rows already
 resident in HBM.  `e2e` is the same metric through the C ABI with host
 buffers: per segment the stimulus is copied from pinned host memory and the
 segment's spike log is read back, and ProcCheck's recall evaluation runs on
-the host.  The network state (~0.5 GB) is larger than L2, so no flush is
+the host.  The network state (~0.25 GB) is larger than L2, so no flush is
 needed between steps.
 
 --impl reference times the CPU oracle (a restatement of gsbn's
@@ -273,7 +273,7 @@ def run_ours(args, rank, world, local_rank):
                                    "1e4 training + 1e4 recall ticks per step",
                        "ticks_per_step": n_ticks, "segments_per_step": len(runs),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "state 0.5 GB > 126 MB L2, no flush"},
+                       "l2": "state 0.25 GB > 126 MB L2, no flush"},
             "ticks_per_s": n_ticks * args.steps * world / (ms / 1e3),
             "recall": f"{recall[0]}/{recall[1]}",
             "gpu_launches": launches,

@@ -1045,6 +1045,25 @@ int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out) {
   return BCPNN_OK;
 }
 
+int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (limit_ns < 100000 || limit_ns > 2000000000) return fail(net, BCPNN_ERR_INVALID, "bcpnn_selftest_barrier_timeout: limit outside [1e5, 2e9] ns");
+  CU(cudaSetDevice(net->device));
+  unsigned int* bar = nullptr;
+  CU(cudaMalloc((void**)&bar, sizeof(unsigned int)));
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned int), net->stream);
+  /* two CTAs, each waiting for a third arrival that never comes */
+  if (e == cudaSuccess) {
+    barrier_probe_kernel<<<2, 32, 0, net->stream>>>(bar, net->h.err, (unsigned long long)limit_ns);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+  cudaFree(bar);
+  if (e != cudaSuccess) return fail(net, BCPNN_ERR_CUDA, std::string("barrier probe: ") + cudaGetErrorString(e));
+  net->launches += 1;
+  return check_device_error(net);
+}
+
 }  // extern "C"
 
 /* ======================================================================== */

@@ -248,7 +248,8 @@ __device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
    and returns false, and every CTA leaves its tick loop. */
 constexpr unsigned long long kBarrierNs = 2000000000ull;
 
-__device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int target, int* err, int* s_ok) {
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int target, int* err, int* s_ok,
+                                          unsigned long long limit_ns = kBarrierNs) {
   __syncthreads();
   if (threadIdx.x == 0) {
     atomic_add_release(bar, 1u);
@@ -259,7 +260,7 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int target
         ok = 0;
         break;
       }
-      if (globaltimer_ns() - t0 > kBarrierNs) {
+      if (globaltimer_ns() - t0 > limit_ns) {
         atomicOr(err, kErrBarrier);
         ok = 0;
         break;
@@ -270,6 +271,14 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int target
   }
   __syncthreads();
   return *s_ok != 0;
+}
+
+/* Failure-detection self-test: every CTA enters grid_sync with a target one
+   arrival above the grid size, which nothing provides, so each wait runs out
+   after limit_ns, sets kErrBarrier in *err and returns. */
+__global__ void barrier_probe_kernel(unsigned int* bar, int* err, unsigned long long limit_ns) {
+  __shared__ int s_ok;
+  grid_sync(bar, gridDim.x + 1u, err, &s_ok, limit_ns);
 }
 
 /* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */

@@ -208,6 +208,15 @@ int bcpnn_counters(bcpnn_net* net, uint64_t out[3]);
 /* Number of kernels this library launched for the network since creation. */
 int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out);
 
+/* Failure-detection self-test (no counterpart in the reference, whose
+   errors all abort): runs the bounded grid-barrier wait of the persistent tick
+   kernel on an arrival count that never completes.  Every wait gives up after
+   limit_ns (1e5 .. 2e9 ns) and sets the barrier bit of the network's error
+   word; the call then returns BCPNN_ERR_DEVICE with the timeout in
+   bcpnn_last_error, and the network stays usable.  Nothing traps or spins
+   without bound. */
+int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns);
+
 /* Message of the last failing call on this handle ("" if none). */
 const char* bcpnn_last_error(const bcpnn_net* net);
 
