@@ -1,0 +1,787 @@
+/*
+ * bcpnn_recall.cu -- replicate recall engine (include/bcpnn_recall.h).
+ *
+ * One launch per tick.  CTA tile = 128 replicates x 256 destination MCUs
+ * (four HCUs of 64, or more of fewer MCUs); the K loop runs over the N source
+ * MCUs in stages of 64.
+ *
+ *   warp 0      TMA producer: S(t-3) tile [128 x 64] and W^T tile [256 x 64]
+ *               (BF16, 128-byte swizzle) into a 4-stage shared-memory ring,
+ *               one mbarrier per stage with the transaction byte count;
+ *   warp 1      allocates 256 TMEM columns; one elected thread issues
+ *               tcgen05.mma.cta_group::1.kind::f16 (M=128, N=256, K=16, FP32
+ *               accumulate) per 16-wide K step and tcgen05.commit to free each
+ *               stage and, at the end, to signal the accumulator;
+ *   warps 2..5  epilogue, one replicate row per thread (TMEM lane = row):
+ *               while the contraction runs, the population update of tick t
+ *               from epsc(t-1) (support, softmax/WTA, Philox spikes) for the
+ *               tile's HCUs, writing dsup(t), the BF16 spike row S(t) and the
+ *               recall counters; then tcgen05.ld of the accumulator and
+ *               epsc(t) = epsc(t-1) * (1 - kepsc) + acc.
+ *
+ * Every mbarrier wait is bounded (1 s of %globaltimer); a wait that runs out
+ * sets an error bit and the CTA leaves its loops, waits (bounded) for its own
+ * outstanding copies and MMAs, frees TMEM and returns.  No cluster multicast.
+ */
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bcpnn_numerics.h"
+#include "bcpnn_recall.h"
+
+namespace bcpnn_recall_dev {
+
+constexpr int kTileM = 128, kTileN = 256, kTileK = 64, kStages = 4, kUmmaK = 16;
+constexpr int kThreads = 192;
+constexpr uint32_t kBytesA = kTileM * kTileK * 2; /* 16 KB */
+constexpr uint32_t kBytesB = kTileN * kTileK * 2; /* 32 KB */
+constexpr uint32_t kStageBytes = kBytesA + kBytesB;
+constexpr uint32_t kTmemCols = 256;
+constexpr int kErrWait = 4;
+constexpr unsigned long long kWaitNs = 1000000000ull;
+/* dynamic shared memory: ring (1024-aligned) + bj tile + barriers */
+constexpr size_t kSmemBytes = 1024 + kStages * kStageBytes + kTileN * 4 + 256;
+
+struct Params {
+  const float* dsup_prev;
+  float* dsup_cur;
+  const float* epsc_prev;
+  float* epsc_cur;
+  uint16_t* s_out; /* BF16 [R][N] spikes of this tick */
+  uint8_t* counts; /* [R][N] */
+  int count_on;
+  const float* bj;
+  const int32_t* lgidx; /* [R][H] */
+  const float* wmask;   /* [R][H] */
+  float lg_hit, lg_miss;
+  int N, H;
+  float taumdt, maxfqdt, wtagain, igain, wgain, lgbias, snoise, one_m_kepsc, pr;
+  uint32_t seed_base;
+  int simstep;
+  int poisson;
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+/* bounded wait; false when it ran out or another thread reported an error */
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  unsigned long long t0 = gtimer();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*(volatile int*)err) return false;
+    if (gtimer() - t0 > kWaitNs) {
+      atomicOr(err, kErrWait);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+/* shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row
+   core groups 1024 bytes apart, descriptor version 1 (sm_100) */
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                /* leading byte offset (unused for swizzled K-major) */
+  d |= (uint64_t)(1024 >> 4) << 32;      /* stride byte offset */
+  d |= (uint64_t)1 << 46;                /* version */
+  d |= (uint64_t)2 << 61;                /* SWIZZLE_128B */
+  return d;
+}
+
+/* instruction descriptor: D F32, A BF16, B BF16, both K-major, N=256, M=128 */
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTileN >> 3) << 17) |
+                            ((uint32_t)(kTileM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+/* 32 consecutive FP32 accumulator columns of this thread's lane */
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+/* population update of tick `simstep` for MCU 0 of the population (the
+   softmax max seed of every HCU, Pop.cpp:270) */
+__device__ __forceinline__ float dsup_mcu0(const Params& p, int row, uint32_t seed) {
+  const size_t base = (size_t)row * p.N;
+  float wsup = 0.0f;
+  wsup += p.bj[0] + p.epsc_prev[base];
+  float noise = 0.0f;
+  if (p.snoise != 0.0f) noise = p.snoise * bx_normal01(seed, 0u, (uint32_t)p.simstep, 0u);
+  float lginp = (p.lgidx[(size_t)row * p.H] == 0) ? p.lg_hit : p.lg_miss;
+  float sup = p.lgbias + p.igain * lginp + noise;
+  sup += (p.wgain * p.wmask[(size_t)row * p.H]) * wsup;
+  float d = p.dsup_prev[base];
+  return d + (sup - d) * p.taumdt;
+}
+
+/* one HCU (M MCUs starting at column c0) of replicate `row` */
+template <int M>
+__device__ __forceinline__ void hcu_update(const Params& p, const float* s_bj, int row, int c0, int cl, float seed0,
+                                           uint32_t seed) {
+  const size_t base = (size_t)row * p.N + c0;
+  const int h = c0 / M;
+  const int lg = p.lgidx[(size_t)row * p.H + h];
+  const float wm = p.wgain * p.wmask[(size_t)row * p.H + h];
+  float d[M];
+#pragma unroll
+  for (int m = 0; m < M; m += 4) {
+    float4 dp = *reinterpret_cast<const float4*>(p.dsup_prev + base + m);
+    float4 ep = *reinterpret_cast<const float4*>(p.epsc_prev + base + m);
+    float dpv[4] = {dp.x, dp.y, dp.z, dp.w}, epv[4] = {ep.x, ep.y, ep.z, ep.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float wsup = 0.0f;
+      wsup += s_bj[cl + m + k] + epv[k];
+      float noise = 0.0f;
+      if (p.snoise != 0.0f) noise = p.snoise * bx_normal01(seed, 0u, (uint32_t)p.simstep, (uint32_t)(c0 + m + k));
+      float lginp = (lg == m + k) ? p.lg_hit : p.lg_miss;
+      float sup = p.lgbias + p.igain * lginp + noise;
+      sup += wm * wsup;
+      d[m + k] = dpv[k] + (sup - dpv[k]) * p.taumdt;
+    }
+  }
+  float mx = (h == 0) ? d[0] : seed0;
+#pragma unroll
+  for (int m = 0; m < M; m++) mx = (d[m] > mx) ? d[m] : mx;
+  const float maxact = bx_expf(p.wtagain * mx);
+  float vsum = 0.0f;
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+    float a = bx_expf(p.wtagain * (d[m] - mx));
+    if (maxact < 1.0f) a *= maxact;
+    vsum += a;
+  }
+  /* spikes: recompute act (same bits), sample with one Philox call per four
+     MCUs (lane = MCU & 3) */
+  uint32_t bits[(M + 31) / 32];
+#pragma unroll
+  for (int i = 0; i < (M + 31) / 32; i++) bits[i] = 0u;
+#pragma unroll
+  for (int m = 0; m < M; m += 4) {
+    const uint32_t idx = (uint32_t)(c0 + m);
+    bx_u32x4 cu;
+    cu.v[0] = idx >> 2;
+    cu.v[1] = (uint32_t)p.simstep;
+    cu.v[2] = 0u;
+    cu.v[3] = 0u;
+    bx_u32x4 ou = bx_philox4x32_10(cu, seed, 0u * 16u + BX_STREAM_UNIFORM);
+    bx_u32x4 op;
+    if (p.poisson) op = bx_philox4x32_10(cu, seed, 0u * 16u + BX_STREAM_POISSON);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float a = bx_expf(p.wtagain * (d[m + k] - mx));
+      if (maxact < 1.0f) a *= maxact;
+      if (vsum > 1.0f) a /= vsum;
+      bool spk = bx_u01(ou.v[k]) < a * p.maxfqdt;
+      if (p.poisson && bx_u01(op.v[k]) < p.pr) spk = true;
+      if (spk) bits[(m + k) >> 5] |= 1u << ((m + k) & 31);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < M; m += 4)
+    *reinterpret_cast<float4*>(p.dsup_cur + base + m) = make_float4(d[m], d[m + 1], d[m + 2], d[m + 3]);
+  /* BF16 1.0 = 0x3F80 */
+#pragma unroll
+  for (int m = 0; m < M; m += 8) {
+    uint32_t w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t lo = (bits[(m + 2 * k) >> 5] >> ((m + 2 * k) & 31)) & 1u;
+      uint32_t hi = (bits[(m + 2 * k + 1) >> 5] >> ((m + 2 * k + 1) & 31)) & 1u;
+      w[k] = (lo ? 0x3F80u : 0u) | ((hi ? 0x3F80u : 0u) << 16);
+    }
+    *reinterpret_cast<uint4*>(p.s_out + base + m) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  if (p.count_on) {
+#pragma unroll
+    for (int m = 0; m < M; m += 4) {
+      uint32_t* c = reinterpret_cast<uint32_t*>(p.counts + base + m);
+      uint32_t v = *c, add = 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) add |= ((bits[(m + k) >> 5] >> ((m + k) & 31)) & 1u) << (8 * k);
+      *c = v + add; /* no carry between bytes: at most 255 counted ticks between clears */
+    }
+  }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kThreads, 1)
+    recall_tick_kernel(const __grid_constant__ CUtensorMap map_s, const __grid_constant__ CUtensorMap map_w,
+                       Params p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  float* s_bj = reinterpret_cast<float*>(ring + kStages * kStageBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(s_bj + kTileN);
+  uint64_t* empty = full + kStages;
+  uint64_t* acc_full = empty + kStages;
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acc_full + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * kTileN, m0 = blockIdx.y * kTileM;
+  const int kIters = p.N / kTileK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  for (int i = threadIdx.x; i < kTileN; i += kThreads) s_bj[i] = p.bj[n0 + i];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (warp == 0) {
+    /* ---------------- TMA producer ---------------- */
+    if (lane == 0) {
+      int issued = 0;
+      for (int k = 0; k < kIters; k++) {
+        const int s = k % kStages;
+        const uint32_t parity = ((k / kStages) & 1) ^ 1;
+        if (!mbar_wait(&empty[s], parity, p.err)) break;
+        uint8_t* a = ring + s * kStageBytes;
+        uint8_t* b = a + kBytesA;
+        mbar_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(a, &map_s, &full[s], k * kTileK, m0);
+        tma_load_2d(b, &map_w, &full[s], k * kTileK, n0);
+        issued = k + 1;
+      }
+      /* leave no copy in flight: each issued stage's barrier completes */
+      for (int k = (issued > kStages ? issued - kStages : 0); k < issued; k++)
+        if (!mbar_wait(&full[k % kStages], (k / kStages) & 1, p.err)) {
+          /* bounded: give the copies the same limit once more, ignoring the error word */
+          unsigned long long t0 = gtimer();
+          while (!mbar_try_wait(&full[k % kStages], (k / kStages) & 1) && gtimer() - t0 < kWaitNs) {
+          }
+        }
+    }
+  } else if (warp == 1) {
+    /* ---------------- MMA issuer ---------------- */
+    if (lane == 0) {
+      bool ok = true;
+      for (int k = 0; k < kIters && ok; k++) {
+        const int s = k % kStages;
+        if (!mbar_wait(&full[s], (k / kStages) & 1, p.err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a = smem_u32(ring + s * kStageBytes);
+        const uint32_t b = a + kBytesA;
+#pragma unroll
+        for (int kk = 0; kk < kTileK / kUmmaK; kk++) {
+          /* +32 bytes along K inside the 128-byte swizzled row */
+          umma(tmem, smem_desc(a + kk * 32), smem_desc(b + kk * 32), (k > 0 || kk > 0) ? 1u : 0u);
+        }
+        umma_commit(&empty[s]);
+      }
+      /* the accumulator barrier tracks every MMA issued so far */
+      umma_commit(acc_full);
+    }
+  } else {
+    /* ---------------- epilogue: one replicate row per thread ---------------- */
+    const int q = warp & 3; /* TMEM lane quarter this warp may access */
+    const int row = m0 + q * 32 + lane;
+    const uint32_t seed = p.seed_base + (uint32_t)row;
+    const float seed0 = dsup_mcu0(p, row, seed);
+    for (int c = 0; c < kTileN; c += M) hcu_update<M>(p, s_bj, row, n0 + c, c, seed0, seed);
+    /* warp-uniform: tcgen05.ld is .sync.aligned */
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(acc_full, 0, p.err) ? 1 : 0) != 0;
+    tc_fence_after();
+    if (ok) {
+      const size_t base = (size_t)row * p.N + n0;
+      for (int c = 0; c < kTileN; c += 32) {
+        float acc[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, acc);
+#pragma unroll
+        for (int i = 0; i < 32; i += 4) {
+          float4 e = *reinterpret_cast<const float4*>(p.epsc_prev + base + c + i);
+          float4 o;
+          o.x = e.x * p.one_m_kepsc + acc[i];
+          o.y = e.y * p.one_m_kepsc + acc[i + 1];
+          o.z = e.z * p.one_m_kepsc + acc[i + 2];
+          o.w = e.w * p.one_m_kepsc + acc[i + 3];
+          *reinterpret_cast<float4*>(p.epsc_cur + base + c + i) = o;
+        }
+      }
+    }
+  }
+  /* every tcgen05 operation of this CTA is complete before TMEM is freed:
+     the epilogue waited for the accumulator barrier; on an error path the
+     MMA thread's last commit is waited for here (bounded) */
+  if (warp == 1 && lane == 0) {
+    unsigned long long t0 = gtimer();
+    while (!mbar_try_wait(acc_full, 0) && gtimer() - t0 < kWaitNs) {
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+__global__ void broadcast_spikes_kernel(uint16_t* s, int R, int N, const int8_t* row) {
+  size_t n = (size_t)R * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    s[i] = row[i % N] ? 0x3F80u : 0u;
+}
+
+__global__ void broadcast_f32_kernel(float* dst, int R, int N, const float* row) {
+  size_t n = (size_t)R * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = row[i % N];
+}
+
+}  // namespace bcpnn_recall_dev
+
+using namespace bcpnn_recall_dev;
+
+struct bcpnn_recall {
+  bcpnn_recall_desc d;
+  int N = 0;
+  cudaStream_t stream = nullptr;
+  float* dsup[2] = {nullptr, nullptr};
+  float* epsc[2] = {nullptr, nullptr};
+  uint16_t* s[4] = {nullptr, nullptr, nullptr, nullptr}; /* spike ring, by tick mod 4 */
+  uint16_t* wt = nullptr; /* W^T BF16 [N][N] */
+  uint8_t* counts = nullptr;
+  float* bj = nullptr;
+  int32_t* lgidx = nullptr;
+  float* wmask = nullptr;
+  int* err = nullptr;
+  float lg_hit = 0.f, lg_miss = 0.f;
+  bool loaded = false, cued = false;
+  long long kk = 0; /* ticks run since load */
+  int counted = 0;   /* counted ticks since the counters were cleared */
+  CUtensorMap map_s[4];
+  CUtensorMap map_w;
+  uint64_t launches = 0;
+  std::string last_error;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+int fail(bcpnn_recall* r, int code, const std::string& msg) {
+  if (r) r->last_error = msg;
+  return code;
+}
+
+#define RCU(call)                                                                             \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(r, BCPNN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_map(bcpnn_recall* r, CUtensorMap* map, void* base, int rows, int cols, int box_rows) {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    RCU(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) return fail(r, BCPNN_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+    fn = (EncodeTiled)p;
+  }
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  cuuint32_t box[2] = {(cuuint32_t)kTileK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult e = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (e != CUDA_SUCCESS) return fail(r, BCPNN_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)e));
+  return BCPNN_OK;
+}
+
+template <typename T>
+int dalloc(bcpnn_recall* r, T** p, size_t count) {
+  *p = nullptr;
+  RCU(cudaMalloc((void**)p, (count ? count : 1) * sizeof(T)));
+  r->allocs.push_back((void*)*p);
+  return BCPNN_OK;
+}
+
+uint16_t to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)((u >> 16) | ((u & 0xFFFFu) ? 0x40u : 0u));
+  u += 0x7FFFu + ((u >> 16) & 1u); /* round to nearest even */
+  return (uint16_t)(u >> 16);
+}
+
+int check_err(bcpnn_recall* r) {
+  int e = 0;
+  RCU(cudaMemcpyAsync(&e, r->err, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+  RCU(cudaStreamSynchronize(r->stream));
+  if (e) {
+    RCU(cudaMemsetAsync(r->err, 0, sizeof(int), r->stream));
+    return fail(r, BCPNN_ERR_DEVICE, "recall kernel reported error word " + std::to_string(e) +
+                                         ((e & kErrWait) ? ": an mbarrier wait timed out" : ""));
+  }
+  return BCPNN_OK;
+}
+
+int mod4(long long v) { return (int)(v & 3); }
+
+}  // namespace
+
+extern "C" {
+
+int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
+  if (!d || !out) return BCPNN_ERR_INVALID;
+  *out = nullptr;
+  const int H = d->hcu_num, M = d->mcu_num, R = d->replicates;
+  if (H < 1 || M < 1 || R < kTileM || R % kTileM) return BCPNN_ERR_INVALID;
+  const long long N = (long long)H * M;
+  if (N % kTileN || kTileN % M || (M != 16 && M != 32 && M != 64) || N > 65536) return BCPNN_ERR_INVALID;
+  if (!(d->dt > 0.f) || !(d->pop.taum > 0.f) || d->poisson_noise_hz < 0.f) return BCPNN_ERR_INVALID;
+  bcpnn_recall* r = new bcpnn_recall();
+  r->d = *d;
+  r->N = (int)N;
+  auto bad = [&](int rc) {
+    bcpnn_recall_destroy(r);
+    return rc;
+  };
+  if (cudaSetDevice(d->device) != cudaSuccess) return bad(BCPNN_ERR_CUDA);
+  int major = 0, minor = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d->device);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, d->device);
+  if (major != 10 || minor != 0) return bad(BCPNN_ERR_DEVICE);
+  if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(BCPNN_ERR_CUDA);
+  size_t RN = (size_t)R * N;
+  int rc = BCPNN_OK;
+  for (int i = 0; i < 2 && !rc; i++) rc = dalloc(r, &r->dsup[i], RN);
+  for (int i = 0; i < 2 && !rc; i++) rc = dalloc(r, &r->epsc[i], RN);
+  for (int i = 0; i < 4 && !rc; i++) rc = dalloc(r, &r->s[i], RN);
+  if (!rc) rc = dalloc(r, &r->wt, (size_t)N * N);
+  if (!rc) rc = dalloc(r, &r->counts, RN);
+  if (!rc) rc = dalloc(r, &r->bj, (size_t)N);
+  if (!rc) rc = dalloc(r, &r->lgidx, (size_t)R * H);
+  if (!rc) rc = dalloc(r, &r->wmask, (size_t)R * H);
+  if (!rc) rc = dalloc(r, &r->err, 1);
+  if (rc) return bad(rc);
+  if (cudaMemset(r->err, 0, sizeof(int)) != cudaSuccess || cudaMemset(r->counts, 0, RN) != cudaSuccess)
+    return bad(BCPNN_ERR_CUDA);
+  for (int i = 0; i < 4 && !rc; i++) rc = encode_map(r, &r->map_s[i], r->s[i], R, (int)N, kTileM);
+  if (!rc) rc = encode_map(r, &r->map_w, r->wt, (int)N, (int)N, kTileN);
+  if (rc) return bad(rc);
+  cudaError_t e = cudaSuccess;
+  if (M == 16) e = cudaFuncSetAttribute(recall_tick_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  if (M == 32) e = cudaFuncSetAttribute(recall_tick_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  if (M == 64) e = cudaFuncSetAttribute(recall_tick_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  if (e != cudaSuccess) return bad(BCPNN_ERR_CUDA);
+  *out = r;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_destroy(bcpnn_recall* r) {
+  if (!r) return BCPNN_ERR_INVALID;
+  cudaSetDevice(r->d.device);
+  if (r->stream) cudaStreamSynchronize(r->stream);
+  for (void* p : r->allocs) cudaFree(p);
+  if (r->stream) cudaStreamDestroy(r->stream);
+  delete r;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_load(bcpnn_recall* r, const float* w, const float* bj, const float* epsc, const float* dsup,
+                      const int8_t* spikes_tm3, const int8_t* spikes_tm2, const int8_t* spikes_tm1) {
+  if (!r) return BCPNN_ERR_INVALID;
+  if (!w || !bj || !epsc || !dsup || !spikes_tm3 || !spikes_tm2 || !spikes_tm1)
+    return fail(r, BCPNN_ERR_INVALID, "null buffer");
+  const int N = r->N, R = r->d.replicates;
+  RCU(cudaSetDevice(r->d.device));
+  /* W^T in BF16: row j = destination MCU, K-contiguous over source MCUs */
+  std::vector<uint16_t> wt((size_t)N * N);
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) wt[(size_t)j * N + i] = to_bf16(w[(size_t)i * N + j]);
+  RCU(cudaMemcpy(r->wt, wt.data(), wt.size() * 2, cudaMemcpyHostToDevice));
+  RCU(cudaMemcpy(r->bj, bj, (size_t)N * 4, cudaMemcpyHostToDevice));
+  float* row_f = nullptr;
+  int8_t* row_s = nullptr;
+  RCU(cudaMalloc((void**)&row_f, (size_t)N * 4));
+  RCU(cudaMalloc((void**)&row_s, (size_t)N * 3));
+  r->kk = 0;
+  const int prev = 1; /* parity buffer read by the next tick (kk = 0) */
+  cudaError_t e = cudaMemcpy(row_f, epsc, (size_t)N * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    broadcast_f32_kernel<<<592, 256, 0, r->stream>>>(r->epsc[prev], R, N, row_f);
+    e = cudaStreamSynchronize(r->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(row_f, dsup, (size_t)N * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    broadcast_f32_kernel<<<592, 256, 0, r->stream>>>(r->dsup[prev], R, N, row_f);
+    e = cudaStreamSynchronize(r->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(row_s, spikes_tm3, (size_t)N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(row_s + N, spikes_tm2, (size_t)N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(row_s + 2 * N, spikes_tm1, (size_t)N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    for (int k = 0; k < 3; k++)
+      broadcast_spikes_kernel<<<592, 256, 0, r->stream>>>(r->s[mod4(k - 3)], R, N, row_s + (size_t)k * N);
+    e = cudaStreamSynchronize(r->stream);
+  }
+  cudaFree(row_f);
+  cudaFree(row_s);
+  if (e != cudaSuccess) return fail(r, BCPNN_ERR_CUDA, std::string("recall load: ") + cudaGetErrorString(e));
+  r->launches += 5;
+  r->loaded = true;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_set_cues(bcpnn_recall* r, const int32_t* lgidx, float eps, const float* wmask) {
+  if (!r) return BCPNN_ERR_INVALID;
+  if (!lgidx || !wmask) return fail(r, BCPNN_ERR_INVALID, "null buffer");
+  const size_t n = (size_t)r->d.replicates * r->d.hcu_num;
+  RCU(cudaSetDevice(r->d.device));
+  RCU(cudaMemcpyAsync(r->lgidx, lgidx, n * 4, cudaMemcpyHostToDevice, r->stream));
+  RCU(cudaMemcpyAsync(r->wmask, wmask, n * 4, cudaMemcpyHostToDevice, r->stream));
+  RCU(cudaStreamSynchronize(r->stream));
+  r->lg_hit = bx_logf(1 + eps);
+  r->lg_miss = bx_logf(0 + eps);
+  r->cued = true;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_clear_counts(bcpnn_recall* r) {
+  if (!r) return BCPNN_ERR_INVALID;
+  RCU(cudaSetDevice(r->d.device));
+  RCU(cudaMemsetAsync(r->counts, 0, (size_t)r->d.replicates * r->N, r->stream));
+  r->counted = 0;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t count_first, int32_t count_last) {
+  if (!r) return BCPNN_ERR_INVALID;
+  if (!r->loaded || !r->cued) return fail(r, BCPNN_ERR_STATE, "bcpnn_recall_run before load and set_cues");
+  if (n_ticks < 0 || first < 0) return fail(r, BCPNN_ERR_INVALID, "bad tick range");
+  int counted = 0;
+  for (int t = first; t < first + n_ticks; t++) counted += (t >= count_first && t <= count_last);
+  if (r->counted + counted > 255)
+    return fail(r, BCPNN_ERR_INVALID, "more than 255 counted ticks since the last clear (uint8 counters)");
+  RCU(cudaSetDevice(r->d.device));
+  const bcpnn_recall_desc& d = r->d;
+  Params p;
+  p.counts = r->counts;
+  p.bj = r->bj;
+  p.lgidx = r->lgidx;
+  p.wmask = r->wmask;
+  p.lg_hit = r->lg_hit;
+  p.lg_miss = r->lg_miss;
+  p.N = r->N;
+  p.H = d.hcu_num;
+  p.taumdt = d.dt / d.pop.taum;   /* Pop.cpp:34 */
+  p.maxfqdt = d.pop.maxfq * d.dt; /* Pop.cpp:36 */
+  p.wtagain = d.pop.wtagain;
+  p.igain = d.pop.igain;
+  p.wgain = d.pop.wgain;
+  p.lgbias = d.pop.lgbias;
+  p.snoise = d.pop.snoise;
+  p.one_m_kepsc = 1.0f - d.kepsc;
+  p.pr = d.poisson_noise_hz * d.dt;
+  p.poisson = d.poisson_noise_hz > 0.f;
+  p.seed_base = d.seed_base;
+  p.err = r->err;
+  dim3 grid(r->N / kTileN, d.replicates / kTileM);
+  for (int i = 0; i < n_ticks; i++) {
+    const long long kk = r->kk + i;
+    const int cur = (int)(kk & 1), prev = cur ^ 1;
+    p.dsup_prev = r->dsup[prev];
+    p.dsup_cur = r->dsup[cur];
+    p.epsc_prev = r->epsc[prev];
+    p.epsc_cur = r->epsc[cur];
+    p.s_out = r->s[mod4(kk)];
+    p.simstep = first + i;
+    p.count_on = (first + i >= count_first && first + i <= count_last) ? 1 : 0;
+    const CUtensorMap& ms = r->map_s[mod4(kk - 3)];
+    if (d.mcu_num == 16) recall_tick_kernel<16><<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
+    if (d.mcu_num == 32) recall_tick_kernel<32><<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
+    if (d.mcu_num == 64) recall_tick_kernel<64><<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
+    RCU(cudaGetLastError());
+  }
+  r->kk += n_ticks;
+  r->counted += counted;
+  r->launches += (uint64_t)n_ticks;
+  return check_err(r);
+}
+
+static int resolve_rows(bcpnn_recall* r, const char* name, int32_t row0, int32_t n_rows, size_t bytes, void** base,
+                        size_t* elem, int* kind) {
+  if (!name) return fail(r, BCPNN_ERR_INVALID, "null name");
+  const int R = r->d.replicates;
+  if (row0 < 0 || n_rows < 0 || row0 + (long long)n_rows > R) return fail(r, BCPNN_ERR_INVALID, "rows out of range");
+  std::string s(name);
+  const long long last = r->kk - 1; /* last tick run */
+  *kind = 0;
+  if (s == "dsup") {
+    *base = r->dsup[(int)(last & 1) & 1];
+    *elem = 4;
+  } else if (s == "epsc") {
+    *base = r->epsc[(int)(last & 1) & 1];
+    *elem = 4;
+  } else if (s == "counts") {
+    *base = r->counts;
+    *elem = 1;
+  } else if (s == "spike" || s == "spike_tm1") {
+    *base = r->s[mod4(last)];
+    *elem = 2;
+    *kind = 1;
+  } else if (s == "spike_tm2") {
+    *base = r->s[mod4(last - 1)];
+    *elem = 2;
+    *kind = 1;
+  } else if (s == "spike_tm3") {
+    *base = r->s[mod4(last - 2)];
+    *elem = 2;
+    *kind = 1;
+  } else {
+    return fail(r, BCPNN_ERR_NOT_FOUND, "unknown recall array " + s);
+  }
+  size_t want = (size_t)n_rows * r->N * (*kind ? 1 : *elem);
+  if (bytes != want) return fail(r, BCPNN_ERR_SIZE, "buffer size does not match rows x N");
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_read(bcpnn_recall* r, const char* name, int32_t row0, int32_t n_rows, void* host, size_t bytes) {
+  if (!r || !host) return BCPNN_ERR_INVALID;
+  void* base;
+  size_t elem;
+  int kind;
+  int rc = resolve_rows(r, name, row0, n_rows, bytes, &base, &elem, &kind);
+  if (rc) return rc;
+  RCU(cudaSetDevice(r->d.device));
+  const size_t off = (size_t)row0 * r->N * elem, n = (size_t)n_rows * r->N;
+  if (kind == 1) {
+    std::vector<uint16_t> tmp(n);
+    RCU(cudaMemcpyAsync(tmp.data(), (uint8_t*)base + off, n * 2, cudaMemcpyDeviceToHost, r->stream));
+    RCU(cudaStreamSynchronize(r->stream));
+    int8_t* o = (int8_t*)host;
+    for (size_t i = 0; i < n; i++) o[i] = tmp[i] ? 1 : 0;
+  } else {
+    RCU(cudaMemcpyAsync(host, (uint8_t*)base + off, n * elem, cudaMemcpyDeviceToHost, r->stream));
+    RCU(cudaStreamSynchronize(r->stream));
+  }
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_write(bcpnn_recall* r, const char* name, int32_t row0, int32_t n_rows, const void* host,
+                       size_t bytes) {
+  if (!r || !host) return BCPNN_ERR_INVALID;
+  if (name && std::string(name) == "counts") return fail(r, BCPNN_ERR_INVALID, "counts are cleared, not written");
+  void* base;
+  size_t elem;
+  int kind;
+  int rc = resolve_rows(r, name, row0, n_rows, bytes, &base, &elem, &kind);
+  if (rc) return rc;
+  RCU(cudaSetDevice(r->d.device));
+  const size_t off = (size_t)row0 * r->N * elem, n = (size_t)n_rows * r->N;
+  if (kind == 1) {
+    std::vector<uint16_t> tmp(n);
+    const int8_t* in = (const int8_t*)host;
+    for (size_t i = 0; i < n; i++) tmp[i] = in[i] ? 0x3F80u : 0u;
+    RCU(cudaMemcpyAsync((uint8_t*)base + off, tmp.data(), n * 2, cudaMemcpyHostToDevice, r->stream));
+    RCU(cudaStreamSynchronize(r->stream));
+  } else {
+    RCU(cudaMemcpyAsync((uint8_t*)base + off, host, n * elem, cudaMemcpyHostToDevice, r->stream));
+    RCU(cudaStreamSynchronize(r->stream));
+  }
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_get_stream(const bcpnn_recall* r, void** stream) {
+  if (!r || !stream) return BCPNN_ERR_INVALID;
+  *stream = (void*)r->stream;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_launches(const bcpnn_recall* r, uint64_t* out) {
+  if (!r || !out) return BCPNN_ERR_INVALID;
+  *out = r->launches;
+  return BCPNN_OK;
+}
+
+const char* bcpnn_recall_last_error(const bcpnn_recall* r) { return r ? r->last_error.c_str() : ""; }
+
+}  // extern "C"

@@ -164,7 +164,8 @@ def _mcu_conn(rng, dest_hcus, n_src, n_slots, proj, delay=1):
 
 
 def single_pop(name, hcu, mcu, n_patterns, train_ticks, rest_ticks, recall_ticks, cue_frac, src_hcus_per_dest,
-               seed=0, dt=0.001, eps=1e-4, tauz=0.01, taue=0.02, taup=1.0, taum=0.005, record=True, check=True):
+               seed=0, dt=0.001, eps=1e-4, tauz=0.01, taue=0.02, taup=1.0, taum=0.005, record=True, check=True,
+               poisson_hz=0.0):
     """One population with a recurrent projection: the 10x10 and 100x100
     workloads.  Training segments (prn 1, mask 0) of train_ticks, optional
     rest segments (prn 1, rest row) and recall segments (prn 0, cue rows,
@@ -193,9 +194,9 @@ def single_pop(name, hcu, mcu, n_patterns, train_ticks, rest_ticks, recall_ticks
     text = "\n".join([
         "gen_param {", '  stim_file: "@STIM@"', f"  dt: {fmt(dt)}", f"  eps: {fmt(eps)}"] + modes + ["}",
         "net_param {", pop_block(hcu, mcu, taum), proj_block(0, 0, tauz, tauz, taue, taup, C), "}",
-        'rec_param { directory: "@REC@" }', procs("@CONN@", seed, record=record, check=check)]) + "\n"
+        'rec_param { directory: "@REC@" }', procs("@CONN@", seed, poisson_hz, record=record, check=check)]) + "\n"
     meta = dict(H=hcu, M=mcu, C=C, patterns=n_patterns, ticks=t, n_cued=n_cued, seed=seed,
-                cells=hcu * C * mcu)
+                cells=hcu * C * mcu, poisson_hz=poisson_hz)
     return Workload(name, text, stim, conn, meta)
 
 
@@ -212,6 +213,16 @@ def config1(seed=0, record=True, check=True, n_patterns=100, train_ticks=100, re
     100 recalls of 100 ticks with 30% of HCUs cued."""
     return single_pop("100x100 density 0.1", 100, 100, n_patterns, train_ticks, 0, recall_ticks, 0.3, 10, seed=seed,
                       record=record, check=check)
+
+
+def config4(seed=0, hcu=64, mcu=64, n_patterns=16, train_ticks=100, rest_ticks=20, recall_ticks=200,
+            cue_frac=0.25, poisson_hz=20.0, record=False, check=False):
+    """The network of the replicate recall workload: 64x64 HCU/MCU, full
+    recurrent projection (C = 4096, 4096 x 4096 weights), patterns trained
+    100 ticks each with rests, 20 Hz Poisson input noise; the recall segments
+    (25% of HCUs cued, 200 ticks) are what the replicates run."""
+    return single_pop(f"{hcu}x{mcu} full recurrent", hcu, mcu, n_patterns, train_ticks, rest_ticks, recall_ticks,
+                      cue_frac, hcu, seed=seed, record=record, check=check, poisson_hz=poisson_hz)
 
 
 def small_scale(seed=0, hcu=20, mcu=20, src=5, n_patterns=10, train_ticks=60, recall_ticks=40, record=True,

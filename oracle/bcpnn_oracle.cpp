@@ -841,6 +841,9 @@ void oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
 void oracle_uniform_array(uint32_t seed, uint32_t pop, uint32_t tick, int n, float* out) {
   for (int i = 0; i < n; ++i) out[i] = bx_uniform01(seed, pop, tick, (uint32_t)i);
 }
+void oracle_uniform_poisson_array(uint32_t seed, uint32_t pop, uint32_t tick, int n, float* out) {
+  for (int i = 0; i < n; ++i) out[i] = bx_uniform01_poisson(seed, pop, tick, (uint32_t)i);
+}
 void oracle_normal_array(uint32_t seed, uint32_t pop, uint32_t tick, int n, float* out) {
   for (int i = 0; i < n; ++i) out[i] = bx_normal01(seed, pop, tick, (uint32_t)i);
 }

@@ -66,6 +66,7 @@ def load():
     lib.oracle_logf_array.argtypes = [i32, ctypes.c_longlong, vp, vp]
     lib.oracle_philox.argtypes = [vp, vp, vp]
     lib.oracle_uniform_array.argtypes = [u32, u32, u32, i32, vp]
+    lib.oracle_uniform_poisson_array.argtypes = [u32, u32, u32, i32, vp]
     lib.oracle_normal_array.argtypes = [u32, u32, u32, i32, vp]
     _lib = lib
     return lib
@@ -100,6 +101,12 @@ def philox(ctr, key):
 def uniforms(seed, pop, tick, n):
     out = np.zeros(n, np.float32)
     load().oracle_uniform_array(seed, pop, tick, n, _p(out))
+    return out
+
+
+def uniforms_poisson(seed, pop, tick, n):
+    out = np.zeros(n, np.float32)
+    load().oracle_uniform_poisson_array(seed, pop, tick, n, _p(out))
     return out
 
 

@@ -12,23 +12,35 @@ from gsbn_b200 import capi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared():
+def declared(prefix="bcpnn_"):
     names = set()
     for h in os.listdir(os.path.join(ROOT, "include")):
         if h.endswith(".h"):
             text = open(os.path.join(ROOT, "include", h)).read()
             text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-            names |= set(re.findall(r"\b(bcpnn_[a-z_0-9]+)\s*\(", text))
+            names |= set(re.findall(r"\b(" + prefix + r"[a-z_0-9]+)\s*\(", text))
     return names
 
 
 def test_every_declared_entry_point_is_exported():
+    from gsbn_b200 import engine, recall
     lib = capi.load()
-    names = declared()
-    assert len(names) >= 20
+    names = declared("bcpnn_") | declared("gsbn_")
+    assert len(names) >= 40
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
-    assert names <= set(capi.EXPORTS), sorted(names - set(capi.EXPORTS))
+    bound = set(capi.EXPORTS) | set(recall.RECALL_EXPORTS) | set(engine.ENGINE_EXPORTS)
+    assert names <= bound, sorted(names - bound)
+
+
+def test_recall_rejects_bad_shapes_before_the_device():
+    from gsbn_b200 import recall
+    pop = dict(hcu_num=8, mcu_num=32, taum=0.005, wtagain=1.0, maxfq=100.0, igain=1.0, wgain=1.0, lgbias=0.0,
+               snoise=0.0)
+    for H, M, R in [(8, 32, 100), (3, 32, 128), (8, 48, 128), (5, 64, 128), (8, 32, 0)]:
+        with pytest.raises(capi.BcpnnError) as e:
+            recall.Recall(H, M, R, dict(pop, hcu_num=H, mcu_num=M), 0.001, 0.1)
+        assert e.value.status == -1
 
 
 def test_status_strings():
