@@ -291,6 +291,144 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
+RECALL_STATE = ("pij_0", "eij_0", "zi2_0", "zj2_0", "tij_0", "wij_0", "pi_0", "ei_0", "zi_0", "ti_0", "pj_0", "ej_0",
+                "zj_0", "qi_0", "ii_0", "di_0", "si_0", ".siq_0", "dsup_0", "act_0", "epsc_0", "bj_0", "spike_0",
+                ".counter_0")
+
+
+def profile_value(name, key):
+    """a `key: value` line of a committed summary under profiles/"""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith(key + ":"):
+                    return json.loads(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_sample=8):
+    """The precision extension: recall of a trained 64x64 network (4096 x 4096
+    weights) by 4096 noise replicates (25% cue, 20 Hz Poisson noise, 200
+    ticks) with the support as a BF16 tcgen05 contraction, against the plain
+    FP32 path running the same replicates one network per launch."""
+    import torch
+    from gsbn_b200 import capi, recall, workloads
+    work = workloads.config4()
+    tr = recall.Trained(work, tempfile.mkdtemp(prefix="gsbn_recall_"), device=dev)
+    trained = tr.snapshot(RECALL_STATE)
+    W, st = tr.recall_inputs()
+    R, T, seed_base = replicates, ticks, 1
+    lg, wm, expected = tr.cues(R)
+    eng = recall.Recall(tr.H, tr.M, R, tr.pops[0], tr.dt, recall.kepsc_of(tr.projs[0], tr.dt), seed_base,
+                        tr.poisson_hz, dev)
+    eng.set_cues(lg, tr.eps, wm)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
+    count = (tr.t0, tr.t0 + T - 2)  # ProcCheck counts ticks strictly inside a T-tick segment
+
+    def load():
+        eng.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
+        eng.clear_counts()
+
+    load()
+    eng.run(tr.t0, T, *count)
+    ok = recall.recall_decisions(eng.read("counts"), tr.H, tr.M, expected)
+    for _ in range(max(0, warmup - 1)):
+        load()
+        eng.run(tr.t0, T)
+    l0 = eng.launches()
+    times = []
+    for _ in range(steps):
+        load()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        eng.run(tr.t0, T)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    launches = eng.launches() - l0 - 5 * steps  # the per-load broadcast kernels are not in the timed region
+    eng.close()
+    ms = statistics.mean(times)
+    N = tr.H * tr.M
+    flops = 2.0 * R * N * N * T
+    tflops = flops / (ms * 1e-3) / 1e12
+    pk, pk_kind = peaks()
+
+    # the plain FP32 path, one network per replicate
+    plain_ms, plain_ok, plain_cells = [], [], 0
+    for r in range(plain_sample):
+        net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=tr.poisson_hz, device=dev,
+                       max_ticks=T)
+        for n, a in trained.items():
+            net.write(n, a)
+        net.set_stimulus_idx(lg[r], tr.eps, wm[r])
+        ps = torch.cuda.ExternalStream(net.stream(), device=dev)
+        c0 = sum(net.counters())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(ps)
+        net.run(tr.t0, T, 0.0, tr.old_prn)
+        e1.record(ps)
+        net.sync()
+        torch.cuda.synchronize()
+        plain_ms.append(e0.elapsed_time(e1))
+        plain_cells += sum(net.counters()) - c0
+        bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
+        counts = bits[: T - 1].sum(axis=0)[None, :]
+        plain_ok.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
+        net.close()
+    plain_rate = T / (statistics.mean(plain_ms) * 1e-3)
+    value = R * T / (ms * 1e-3)
+
+    # the same trained weights recalled without input noise, where recall is
+    # not drowned (noise spikes reach the recurrent projection like any spike)
+    quiet = recall.Recall(tr.H, tr.M, R, tr.pops[0], tr.dt, recall.kepsc_of(tr.projs[0], tr.dt), seed_base, 0.0, dev)
+    quiet.set_cues(lg, tr.eps, wm)
+    quiet.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
+    quiet.run(tr.t0, T, *count)
+    ok_q = recall.recall_decisions(quiet.read("counts"), tr.H, tr.M, expected)
+    quiet.close()
+    plain_q = []
+    for r in range(plain_sample):
+        net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=0.0, device=dev, max_ticks=T)
+        for n, a in trained.items():
+            net.write(n, a)
+        net.set_stimulus_idx(lg[r], tr.eps, wm[r])
+        net.run(tr.t0, T, 0.0, tr.old_prn)
+        bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
+        counts = bits[: T - 1].sum(axis=0)[None, :]
+        plain_q.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
+        net.close()
+    fp64 = profile_value("recall_precision_64x64.md", "fp64_error")
+    return {
+        "workload": f"64x64 HCU/MCU full recurrent (4096 x 4096 weights), {work.meta['patterns']} trained patterns, "
+                    f"{R} noise replicates, 25% cue, 20 Hz Poisson noise, {T} recall ticks",
+        "metric": "replicate ticks/s", "value": value, "unit": "replicate-ticks/s", "steps": steps,
+        "ms_per_step": ms, "us_per_tick": ms * 1e3 / T, "gpu_launches_per_step": launches / max(1, steps),
+        "dtype": "bf16 weights x exact 0/1 spikes, fp32 accumulate; fp32 state",
+        "roofline": {"bound": "tensor", "kernel": "recall_tick_kernel", "achieved": tflops, "peak": pk["bf16_tflops"],
+                     "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"], "peak_kind": pk_kind + " (burst)",
+                     "flops_per_tick": 2.0 * R * N * N},
+        "plain_fp32": {"value": plain_rate, "unit": "replicate-ticks/s", "replicates_timed": plain_sample,
+                       "ms_per_replicate": statistics.mean(plain_ms),
+                       "cell_updates_per_s": plain_cells / (sum(plain_ms) * 1e-3)},
+        "speedup_vs_plain_fp32": value / plain_rate,
+        "recall": {"bf16_all": f"{int(ok.sum())}/{R}", "bf16_sample": f"{int(ok[:plain_sample].sum())}/{plain_sample}",
+                   "plain_fp32_sample": f"{sum(plain_ok)}/{plain_sample}",
+                   "decisions_agree_sample": f"{sum(int(a == b) for a, b in zip(ok[:plain_sample], plain_ok))}"
+                                             f"/{plain_sample}",
+                   "without_noise": {"bf16_all": f"{int(ok_q.sum())}/{R}",
+                                     "bf16_sample": f"{int(ok_q[:plain_sample].sum())}/{plain_sample}",
+                                     "plain_fp32_sample": f"{sum(plain_q)}/{plain_sample}",
+                                     "decisions_agree_sample":
+                                         f"{sum(int(a == b) for a, b in zip(ok_q[:plain_sample], plain_q))}"
+                                         f"/{plain_sample}"}},
+        "fp64_error": fp64,
+    }
+
+
 def cpu_sample(sample_ticks=600):
     """The oracle on a bounded sample of the workload: the first
     `sample_ticks` training ticks (with the start-of-run all-cells pass), then
@@ -379,6 +517,9 @@ def main():
     ap.add_argument("--ref-ticks", type=int, default=400)
     ap.add_argument("--cpu-ticks", type=int, default=3600)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extensions", action="store_true")
+    ap.add_argument("--only-extensions", action="store_true", help="run the extension workloads alone (profiling)")
+    ap.add_argument("--recall-replicates", type=int, default=4096)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -393,7 +534,15 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.only_extensions:
+        if rank == 0:
+            ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates)}
+            print(json.dumps({"extensions": ext}), flush=True)
+        return
     out = run_ours(args, rank, world, local_rank)
+    if rank == 0 and not args.no_extensions:
+        out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
+                                                                 args.recall_replicates)}
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, sample, secs = cpu_sample(args.cpu_ticks)

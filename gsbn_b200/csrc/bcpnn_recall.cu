@@ -41,11 +41,13 @@ constexpr int kThreads = 192;
 constexpr uint32_t kBytesA = kTileM * kTileK * 2; /* 16 KB */
 constexpr uint32_t kBytesB = kTileN * kTileK * 2; /* 32 KB */
 constexpr uint32_t kStageBytes = kBytesA + kBytesB;
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512; /* two 128 x 256 FP32 accumulators */
+constexpr int kEpiThreads = 128;
 constexpr int kErrWait = 4;
+constexpr int kErrAlign = 8; /* a self-check found a misaligned or out-of-range access (skipped) */
 constexpr unsigned long long kWaitNs = 1000000000ull;
-/* dynamic shared memory: ring (1024-aligned) + bj tile + barriers */
-constexpr size_t kSmemBytes = 1024 + kStages * kStageBytes + kTileN * 4 + 256;
+/* dynamic shared memory: ring (1024-aligned) + barriers + TMEM address */
+constexpr size_t kSmemBytes = 1024 + kStages * kStageBytes + 256;
 
 struct Params {
   const float* dsup_prev;
@@ -59,7 +61,7 @@ struct Params {
   const int32_t* lgidx; /* [R][H] */
   const float* wmask;   /* [R][H] */
   float lg_hit, lg_miss;
-  int N, H;
+  int N, H, R;
   float taumdt, maxfqdt, wtagain, igain, wgain, lgbias, snoise, one_m_kepsc, pr;
   uint32_t seed_base;
   int simstep;
@@ -181,110 +183,143 @@ __device__ __forceinline__ float dsup_mcu0(const Params& p, int row, uint32_t se
   return d + (sup - d) * p.taumdt;
 }
 
-/* one HCU (M MCUs starting at column c0) of replicate `row` */
+/* Population update of tick `simstep` (Pop.cpp:229-323) for one quarter of
+   one HCU of one replicate: four consecutive lanes hold the four quarters of
+   an HCU (Q = M/4 MCUs each).  The HCU maximum is a shuffle max (exact); the
+   activity sum keeps gsbn's serial MCU order by passing the running sum from
+   lane to lane; one Philox call per four MCUs and stream. */
 template <int M>
-__device__ __forceinline__ void hcu_update(const Params& p, const float* s_bj, int row, int c0, int cl, float seed0,
-                                           uint32_t seed) {
-  const size_t base = (size_t)row * p.N + c0;
-  const int h = c0 / M;
-  const int lg = p.lgidx[(size_t)row * p.H + h];
-  const float wm = p.wgain * p.wmask[(size_t)row * p.H + h];
-  float d[M];
+__global__ void __launch_bounds__(256) recall_pop_kernel(Params p) {
+  constexpr int Q = M / 4;
+  const int lane = threadIdx.x & 31;
+  const int tid = blockIdx.x * 256 + threadIdx.x;
+  const int g = tid >> 2, q = tid & 3;
+  const int h = g % p.H, r = g / p.H;
+  const uint32_t seed = p.seed_base + (uint32_t)r;
+  const size_t row = (size_t)r * p.N;
+  const int c0 = h * M + q * Q;
+  /* self-check: every vector access below is in bounds and aligned */
+  {
+    const size_t n = (size_t)p.R * p.N;
+    const bool bad = r >= p.R || row + c0 + Q > n || ((row + c0) & 3) != 0 || (c0 + Q) > p.N ||
+                     (reinterpret_cast<uintptr_t>(p.dsup_prev) & 15) || (reinterpret_cast<uintptr_t>(p.dsup_cur) & 15) ||
+                     (reinterpret_cast<uintptr_t>(p.epsc_prev) & 15) || (reinterpret_cast<uintptr_t>(p.bj) & 15) ||
+                     (reinterpret_cast<uintptr_t>(p.s_out) & 15) || (reinterpret_cast<uintptr_t>(p.counts) & 15);
+    if (bad) {
+      if (atomicOr(p.err, kErrAlign) == 0) p.err[1] = tid;
+      return;
+    }
+  }
+  const float seed0 = dsup_mcu0(p, r, seed);
+  const int lg = p.lgidx[(size_t)r * p.H + h];
+  const float wm = p.wgain * p.wmask[(size_t)r * p.H + h];
+  float d[Q];
 #pragma unroll
-  for (int m = 0; m < M; m += 4) {
-    float4 dp = *reinterpret_cast<const float4*>(p.dsup_prev + base + m);
-    float4 ep = *reinterpret_cast<const float4*>(p.epsc_prev + base + m);
-    float dpv[4] = {dp.x, dp.y, dp.z, dp.w}, epv[4] = {ep.x, ep.y, ep.z, ep.w};
+  for (int m = 0; m < Q; m += 4) {
+    float4 dp = *reinterpret_cast<const float4*>(p.dsup_prev + row + c0 + m);
+    float4 ep = *reinterpret_cast<const float4*>(p.epsc_prev + row + c0 + m);
+    float4 bb = *reinterpret_cast<const float4*>(p.bj + c0 + m);
+    float dpv[4] = {dp.x, dp.y, dp.z, dp.w}, epv[4] = {ep.x, ep.y, ep.z, ep.w}, bjv[4] = {bb.x, bb.y, bb.z, bb.w};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       float wsup = 0.0f;
-      wsup += s_bj[cl + m + k] + epv[k];
+      wsup += bjv[k] + epv[k];
       float noise = 0.0f;
       if (p.snoise != 0.0f) noise = p.snoise * bx_normal01(seed, 0u, (uint32_t)p.simstep, (uint32_t)(c0 + m + k));
-      float lginp = (lg == m + k) ? p.lg_hit : p.lg_miss;
+      float lginp = (lg == q * Q + m + k) ? p.lg_hit : p.lg_miss;
       float sup = p.lgbias + p.igain * lginp + noise;
       sup += wm * wsup;
       d[m + k] = dpv[k] + (sup - dpv[k]) * p.taumdt;
     }
   }
-  float mx = (h == 0) ? d[0] : seed0;
+  float mx = seed0; /* the new dsup of population MCU 0 (also d[0] of HCU 0's first quarter) */
 #pragma unroll
-  for (int m = 0; m < M; m++) mx = (d[m] > mx) ? d[m] : mx;
+  for (int m = 0; m < Q; m++) mx = (d[m] > mx) ? d[m] : mx;
+  mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+  mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
   const float maxact = bx_expf(p.wtagain * mx);
-  float vsum = 0.0f;
+  float a[Q];
 #pragma unroll
-  for (int m = 0; m < M; m++) {
-    float a = bx_expf(p.wtagain * (d[m] - mx));
-    if (maxact < 1.0f) a *= maxact;
-    vsum += a;
+  for (int m = 0; m < Q; m++) {
+    a[m] = bx_expf(p.wtagain * (d[m] - mx));
+    if (maxact < 1.0f) a[m] *= maxact;
   }
-  /* spikes: recompute act (same bits), sample with one Philox call per four
-     MCUs (lane = MCU & 3) */
-  uint32_t bits[(M + 31) / 32];
+  float vs = 0.0f;
 #pragma unroll
-  for (int i = 0; i < (M + 31) / 32; i++) bits[i] = 0u;
+  for (int s = 0; s < 4; s++) {
+    if (q == s) {
 #pragma unroll
-  for (int m = 0; m < M; m += 4) {
-    const uint32_t idx = (uint32_t)(c0 + m);
+      for (int m = 0; m < Q; m++) vs += a[m];
+    }
+    vs = __shfl_sync(0xffffffffu, vs, (lane & ~3) | s);
+  }
+  uint32_t bits = 0u;
+#pragma unroll
+  for (int m = 0; m < Q; m += 4) {
     bx_u32x4 cu;
-    cu.v[0] = idx >> 2;
+    cu.v[0] = (uint32_t)(c0 + m) >> 2;
     cu.v[1] = (uint32_t)p.simstep;
     cu.v[2] = 0u;
     cu.v[3] = 0u;
-    bx_u32x4 ou = bx_philox4x32_10(cu, seed, 0u * 16u + BX_STREAM_UNIFORM);
+    const bx_u32x4 ou = bx_philox4x32_10(cu, seed, 0u * 16u + BX_STREAM_UNIFORM);
     bx_u32x4 op;
     if (p.poisson) op = bx_philox4x32_10(cu, seed, 0u * 16u + BX_STREAM_POISSON);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      float a = bx_expf(p.wtagain * (d[m + k] - mx));
-      if (maxact < 1.0f) a *= maxact;
-      if (vsum > 1.0f) a /= vsum;
-      bool spk = bx_u01(ou.v[k]) < a * p.maxfqdt;
+      float act = a[m + k];
+      if (vs > 1.0f) act /= vs;
+      bool spk = bx_u01(ou.v[k]) < act * p.maxfqdt;
       if (p.poisson && bx_u01(op.v[k]) < p.pr) spk = true;
-      if (spk) bits[(m + k) >> 5] |= 1u << ((m + k) & 31);
+      if (spk) bits |= 1u << (m + k);
     }
   }
 #pragma unroll
-  for (int m = 0; m < M; m += 4)
-    *reinterpret_cast<float4*>(p.dsup_cur + base + m) = make_float4(d[m], d[m + 1], d[m + 2], d[m + 3]);
-  /* BF16 1.0 = 0x3F80 */
+  for (int m = 0; m < Q; m += 4)
+    *reinterpret_cast<float4*>(p.dsup_cur + row + c0 + m) = make_float4(d[m], d[m + 1], d[m + 2], d[m + 3]);
+  /* BF16 1.0 = 0x3F80; four MCUs per 8-byte store (Q is a multiple of 4) */
 #pragma unroll
-  for (int m = 0; m < M; m += 8) {
-    uint32_t w[4];
+  for (int m = 0; m < Q; m += 4) {
+    uint32_t w[2];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint32_t lo = (bits[(m + 2 * k) >> 5] >> ((m + 2 * k) & 31)) & 1u;
-      uint32_t hi = (bits[(m + 2 * k + 1) >> 5] >> ((m + 2 * k + 1) & 31)) & 1u;
-      w[k] = (lo ? 0x3F80u : 0u) | ((hi ? 0x3F80u : 0u) << 16);
-    }
-    *reinterpret_cast<uint4*>(p.s_out + base + m) = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int k = 0; k < 2; k++)
+      w[k] = (((bits >> (m + 2 * k)) & 1u) ? 0x3F80u : 0u) | ((((bits >> (m + 2 * k + 1)) & 1u) ? 0x3F80u : 0u) << 16);
+    *reinterpret_cast<uint2*>(p.s_out + row + c0 + m) = make_uint2(w[0], w[1]);
   }
   if (p.count_on) {
 #pragma unroll
-    for (int m = 0; m < M; m += 4) {
-      uint32_t* c = reinterpret_cast<uint32_t*>(p.counts + base + m);
-      uint32_t v = *c, add = 0;
+    for (int m = 0; m < Q; m += 4) {
+      uint32_t* c = reinterpret_cast<uint32_t*>(p.counts + row + c0 + m);
+      uint32_t add = 0;
 #pragma unroll
-      for (int k = 0; k < 4; k++) add |= ((bits[(m + k) >> 5] >> ((m + k) & 31)) & 1u) << (8 * k);
-      *c = v + add; /* no carry between bytes: at most 255 counted ticks between clears */
+      for (int k = 0; k < 4; k++) add |= ((bits >> (m + k)) & 1u) << (8 * k);
+      *c = *c + add; /* no carry between bytes: at most 255 counted ticks between clears */
     }
   }
 }
 
-template <int M>
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+/* Persistent contraction + epsc epilogue: one CTA per SM walks the output
+   tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (tile t = M-tile t / nN,
+   N-tile t % nN).  The stage ring runs on across tiles; two TMEM accumulators
+   of 256 columns alternate, so the epilogue of one tile overlaps the MMAs of
+   the next (acc_full: MMA -> epilogue, acc_empty: epilogue -> MMA). */
 __global__ void __launch_bounds__(kThreads, 1)
     recall_tick_kernel(const __grid_constant__ CUtensorMap map_s, const __grid_constant__ CUtensorMap map_w,
                        Params p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  float* s_bj = reinterpret_cast<float*>(ring + kStages * kStageBytes);
-  uint64_t* full = reinterpret_cast<uint64_t*>(s_bj + kTileN);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* acc_full = empty + kStages;
-  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acc_full + 1);
+  uint64_t* acc_full = empty + kStages;   /* [2] */
+  uint64_t* acc_empty = acc_full + 2;     /* [2] */
+  uint64_t* mma_done = acc_empty + 2;
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(mma_done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * kTileN, m0 = blockIdx.y * kTileM;
+  const int nN = p.N / kTileN, nM = p.R / kTileM, n_tiles = nN * nM;
   const int kIters = p.N / kTileK;
 
   if (threadIdx.x == 0) {
@@ -292,7 +327,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(acc_full, 1);
+    for (int j = 0; j < 2; j++) {
+      mbar_init(&acc_full[j], 1);
+      mbar_init(&acc_empty[j], kEpiThreads);
+    }
+    mbar_init(mma_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -301,74 +340,90 @@ __global__ void __launch_bounds__(kThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  for (int i = threadIdx.x; i < kTileN; i += kThreads) s_bj[i] = p.bj[n0 + i];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
+  /* self-check of the set-up every access below relies on: ring and barrier
+     alignment, the accumulators' TMEM columns, whole tiles */
+  const bool setup_ok = (smem_u32(ring) & 1023u) == 0 && (smem_u32(full) & 7u) == 0 && (tmem >> 16) == 0 &&
+                        (tmem & 0xFFFFu) + kTmemCols <= 512u && p.N % kTileN == 0 && p.R % kTileM == 0 &&
+                        (reinterpret_cast<uintptr_t>(p.epsc_prev) & 15) == 0 &&
+                        (reinterpret_cast<uintptr_t>(p.epsc_cur) & 15) == 0;
+  if (!setup_ok && threadIdx.x == 0 && atomicOr(p.err, kErrAlign) == 0) p.err[1] = -1 - (int)blockIdx.x;
 
-  if (warp == 0) {
+  if (setup_ok && warp == 0) {
     /* ---------------- TMA producer ---------------- */
     if (lane == 0) {
-      int issued = 0;
-      for (int k = 0; k < kIters; k++) {
-        const int s = k % kStages;
-        const uint32_t parity = ((k / kStages) & 1) ^ 1;
-        if (!mbar_wait(&empty[s], parity, p.err)) break;
-        uint8_t* a = ring + s * kStageBytes;
-        uint8_t* b = a + kBytesA;
-        mbar_expect_tx(&full[s], kStageBytes);
-        tma_load_2d(a, &map_s, &full[s], k * kTileK, m0);
-        tma_load_2d(b, &map_w, &full[s], k * kTileK, n0);
-        issued = k + 1;
-      }
-      /* leave no copy in flight: each issued stage's barrier completes */
-      for (int k = (issued > kStages ? issued - kStages : 0); k < issued; k++)
-        if (!mbar_wait(&full[k % kStages], (k / kStages) & 1, p.err)) {
-          /* bounded: give the copies the same limit once more, ignoring the error word */
-          unsigned long long t0 = gtimer();
-          while (!mbar_try_wait(&full[k % kStages], (k / kStages) & 1) && gtimer() - t0 < kWaitNs) {
+      long long it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const int m0 = (t / nN) * kTileM, n0 = (t % nN) * kTileN;
+        for (int k = 0; k < kIters; k++, it++) {
+          const int s = (int)(it % kStages);
+          if (!mbar_wait(&empty[s], (uint32_t)(((it / kStages) & 1) ^ 1), p.err)) {
+            ok = false;
+            break;
           }
+          uint8_t* a = ring + s * kStageBytes;
+          mbar_expect_tx(&full[s], kStageBytes);
+          tma_load_2d(a, &map_s, &full[s], k * kTileK, m0);
+          tma_load_2d(a + kBytesA, &map_w, &full[s], k * kTileK, n0);
         }
+      }
+      /* leave no copy in flight: the last use of every slot completes */
+      for (long long j = (it > kStages ? it - kStages : 0); j < it; j++) {
+        unsigned long long t0 = gtimer();
+        while (!mbar_try_wait(&full[j % kStages], (uint32_t)((j / kStages) & 1)) && gtimer() - t0 < kWaitNs) {
+        }
+      }
     }
-  } else if (warp == 1) {
+  } else if (setup_ok && warp == 1) {
     /* ---------------- MMA issuer ---------------- */
     if (lane == 0) {
+      long long it = 0;
       bool ok = true;
-      for (int k = 0; k < kIters && ok; k++) {
-        const int s = k % kStages;
-        if (!mbar_wait(&full[s], (k / kStages) & 1, p.err)) {
-          ok = false;
-          break;
-        }
+      int li = 0;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, li++) {
+        const int j = li & 1;
+        if (!mbar_wait(&acc_empty[j], (uint32_t)(((li >> 1) & 1) ^ 1), p.err)) break;
         tc_fence_after();
-        const uint32_t a = smem_u32(ring + s * kStageBytes);
-        const uint32_t b = a + kBytesA;
+        const uint32_t acc = tmem + (uint32_t)(j * kTileN);
+        for (int k = 0; k < kIters; k++, it++) {
+          const int s = (int)(it % kStages);
+          if (!mbar_wait(&full[s], (uint32_t)((it / kStages) & 1), p.err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a = smem_u32(ring + s * kStageBytes);
+          const uint32_t b = a + kBytesA;
 #pragma unroll
-        for (int kk = 0; kk < kTileK / kUmmaK; kk++) {
-          /* +32 bytes along K inside the 128-byte swizzled row */
-          umma(tmem, smem_desc(a + kk * 32), smem_desc(b + kk * 32), (k > 0 || kk > 0) ? 1u : 0u);
+          for (int kk = 0; kk < kTileK / kUmmaK; kk++) {
+            /* +32 bytes along K inside the 128-byte swizzled row */
+            umma(acc, smem_desc(a + kk * 32), smem_desc(b + kk * 32), (k > 0 || kk > 0) ? 1u : 0u);
+          }
+          umma_commit(&empty[s]);
         }
-        umma_commit(&empty[s]);
+        if (ok) umma_commit(&acc_full[j]);
       }
-      /* the accumulator barrier tracks every MMA issued so far */
-      umma_commit(acc_full);
     }
-  } else {
+  } else if (setup_ok) {
     /* ---------------- epilogue: one replicate row per thread ---------------- */
     const int q = warp & 3; /* TMEM lane quarter this warp may access */
-    const int row = m0 + q * 32 + lane;
-    const uint32_t seed = p.seed_base + (uint32_t)row;
-    const float seed0 = dsup_mcu0(p, row, seed);
-    for (int c = 0; c < kTileN; c += M) hcu_update<M>(p, s_bj, row, n0 + c, c, seed0, seed);
-    /* warp-uniform: tcgen05.ld is .sync.aligned */
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(acc_full, 0, p.err) ? 1 : 0) != 0;
-    tc_fence_after();
-    if (ok) {
+    int li = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, li++) {
+      const int j = li & 1;
+      const int m0 = (t / nN) * kTileM, n0 = (t % nN) * kTileN;
+      /* warp-uniform: tcgen05.ld is .sync.aligned */
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[j], (uint32_t)((li >> 1) & 1), p.err) ? 1 : 0) != 0;
+      if (!ok) break;
+      tc_fence_after();
+      const int row = m0 + q * 32 + lane;
       const size_t base = (size_t)row * p.N + n0;
       for (int c = 0; c < kTileN; c += 32) {
         float acc[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, acc);
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(j * kTileN + c), acc);
 #pragma unroll
         for (int i = 0; i < 32; i += 4) {
           float4 e = *reinterpret_cast<const float4*>(p.epsc_prev + base + c + i);
@@ -380,14 +435,16 @@ __global__ void __launch_bounds__(kThreads, 1)
           *reinterpret_cast<float4*>(p.epsc_cur + base + c + i) = o;
         }
       }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[j]);
     }
   }
-  /* every tcgen05 operation of this CTA is complete before TMEM is freed:
-     the epilogue waited for the accumulator barrier; on an error path the
-     MMA thread's last commit is waited for here (bounded) */
+  /* every tcgen05 operation of this CTA completes before TMEM is freed: the
+     MMA thread's last commit (all MMAs it issued) is waited for, bounded */
   if (warp == 1 && lane == 0) {
+    umma_commit(mma_done);
     unsigned long long t0 = gtimer();
-    while (!mbar_try_wait(acc_full, 0) && gtimer() - t0 < kWaitNs) {
+    while (!mbar_try_wait(mma_done, 0) && gtimer() - t0 < kWaitNs) {
     }
   }
   tc_fence_before();
@@ -416,7 +473,9 @@ using namespace bcpnn_recall_dev;
 struct bcpnn_recall {
   bcpnn_recall_desc d;
   int N = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      /* contraction + epsc; the handle's stream */
+  cudaStream_t pop_stream = nullptr;  /* population update, concurrent with it */
+  cudaEvent_t ev_pop = nullptr, ev_gemm = nullptr;
   float* dsup[2] = {nullptr, nullptr};
   float* epsc[2] = {nullptr, nullptr};
   uint16_t* s[4] = {nullptr, nullptr, nullptr, nullptr}; /* spike ring, by tick mod 4 */
@@ -433,6 +492,7 @@ struct bcpnn_recall {
   CUtensorMap map_s[4];
   CUtensorMap map_w;
   uint64_t launches = 0;
+  int sms = 148;
   std::string last_error;
   std::vector<void*> allocs;
 };
@@ -492,13 +552,15 @@ uint16_t to_bf16(float f) {
 }
 
 int check_err(bcpnn_recall* r) {
-  int e = 0;
-  RCU(cudaMemcpyAsync(&e, r->err, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+  int e[2] = {0, 0};
+  RCU(cudaMemcpyAsync(e, r->err, sizeof(e), cudaMemcpyDeviceToHost, r->stream));
   RCU(cudaStreamSynchronize(r->stream));
-  if (e) {
-    RCU(cudaMemsetAsync(r->err, 0, sizeof(int), r->stream));
-    return fail(r, BCPNN_ERR_DEVICE, "recall kernel reported error word " + std::to_string(e) +
-                                         ((e & kErrWait) ? ": an mbarrier wait timed out" : ""));
+  if (e[0]) {
+    RCU(cudaMemsetAsync(r->err, 0, sizeof(e), r->stream));
+    std::string why;
+    if (e[0] & kErrWait) why += " an mbarrier wait timed out;";
+    if (e[0] & kErrAlign) why += " a self-check skipped a misaligned or out-of-range access (thread " + std::to_string(e[1]) + ");";
+    return fail(r, BCPNN_ERR_DEVICE, "recall kernel reported error word " + std::to_string(e[0]) + ":" + why);
   }
   return BCPNN_OK;
 }
@@ -529,6 +591,8 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d->device);
   cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, d->device);
   if (major != 10 || minor != 0) return bad(BCPNN_ERR_DEVICE);
+  cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, d->device);
+  if (r->sms < 1) r->sms = 1;
   if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(BCPNN_ERR_CUDA);
   size_t RN = (size_t)R * N;
   int rc = BCPNN_OK;
@@ -540,18 +604,20 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
   if (!rc) rc = dalloc(r, &r->bj, (size_t)N);
   if (!rc) rc = dalloc(r, &r->lgidx, (size_t)R * H);
   if (!rc) rc = dalloc(r, &r->wmask, (size_t)R * H);
-  if (!rc) rc = dalloc(r, &r->err, 1);
+  if (!rc) rc = dalloc(r, &r->err, 2);
   if (rc) return bad(rc);
-  if (cudaMemset(r->err, 0, sizeof(int)) != cudaSuccess || cudaMemset(r->counts, 0, RN) != cudaSuccess)
+  if (cudaMemset(r->err, 0, 2 * sizeof(int)) != cudaSuccess || cudaMemset(r->counts, 0, RN) != cudaSuccess)
     return bad(BCPNN_ERR_CUDA);
   for (int i = 0; i < 4 && !rc; i++) rc = encode_map(r, &r->map_s[i], r->s[i], R, (int)N, kTileM);
   if (!rc) rc = encode_map(r, &r->map_w, r->wt, (int)N, (int)N, kTileN);
   if (rc) return bad(rc);
   cudaError_t e = cudaSuccess;
-  if (M == 16) e = cudaFuncSetAttribute(recall_tick_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-  if (M == 32) e = cudaFuncSetAttribute(recall_tick_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-  if (M == 64) e = cudaFuncSetAttribute(recall_tick_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  e = cudaFuncSetAttribute(recall_tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
   if (e != cudaSuccess) return bad(BCPNN_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&r->pop_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&r->ev_pop, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&r->ev_gemm, cudaEventDisableTiming) != cudaSuccess)
+    return bad(BCPNN_ERR_CUDA);
   *out = r;
   return BCPNN_OK;
 }
@@ -560,7 +626,11 @@ int bcpnn_recall_destroy(bcpnn_recall* r) {
   if (!r) return BCPNN_ERR_INVALID;
   cudaSetDevice(r->d.device);
   if (r->stream) cudaStreamSynchronize(r->stream);
+  if (r->pop_stream) cudaStreamSynchronize(r->pop_stream);
   for (void* p : r->allocs) cudaFree(p);
+  if (r->ev_pop) cudaEventDestroy(r->ev_pop);
+  if (r->ev_gemm) cudaEventDestroy(r->ev_gemm);
+  if (r->pop_stream) cudaStreamDestroy(r->pop_stream);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
   return BCPNN_OK;
@@ -652,6 +722,7 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
   p.lg_miss = r->lg_miss;
   p.N = r->N;
   p.H = d.hcu_num;
+  p.R = d.replicates;
   p.taumdt = d.dt / d.pop.taum;   /* Pop.cpp:34 */
   p.maxfqdt = d.pop.maxfq * d.dt; /* Pop.cpp:36 */
   p.wtagain = d.pop.wtagain;
@@ -664,7 +735,16 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
   p.poisson = d.poisson_noise_hz > 0.f;
   p.seed_base = d.seed_base;
   p.err = r->err;
-  dim3 grid(r->N / kTileN, d.replicates / kTileM);
+  const int n_tiles = (r->N / kTileN) * (d.replicates / kTileM);
+  const int grid = n_tiles < r->sms ? n_tiles : r->sms;
+  const int pop_blocks = (int)((size_t)d.replicates * d.hcu_num * 4 / 256);
+  /* Tick kk: the population update needs epsc(kk-1) and dsup(kk-1); the
+     contraction needs S(kk-3) and epsc(kk-1).  So both wait only for tick
+     kk-1 and run side by side: pop(kk) after gemm(kk-1) (it also must not
+     overwrite S(kk) = S(kk-4) while gemm(kk-1) reads it), gemm(kk) after
+     pop(kk-1) (which last read the epsc buffer gemm(kk) writes). */
+  RCU(cudaEventRecord(r->ev_gemm, r->stream));
+  RCU(cudaStreamWaitEvent(r->pop_stream, r->ev_gemm, 0));
   for (int i = 0; i < n_ticks; i++) {
     const long long kk = r->kk + i;
     const int cur = (int)(kk & 1), prev = cur ^ 1;
@@ -676,14 +756,22 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
     p.simstep = first + i;
     p.count_on = (first + i >= count_first && first + i <= count_last) ? 1 : 0;
     const CUtensorMap& ms = r->map_s[mod4(kk - 3)];
-    if (d.mcu_num == 16) recall_tick_kernel<16><<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
-    if (d.mcu_num == 32) recall_tick_kernel<32><<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
-    if (d.mcu_num == 64) recall_tick_kernel<64><<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
+    if (d.mcu_num == 16) recall_pop_kernel<16><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
+    if (d.mcu_num == 32) recall_pop_kernel<32><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
+    if (d.mcu_num == 64) recall_pop_kernel<64><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
     RCU(cudaGetLastError());
+    recall_tick_kernel<<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
+    RCU(cudaGetLastError());
+    /* both kernels of tick kk are queued: each stream waits for the other's
+       kernel of this tick before its kernel of tick kk+1 */
+    RCU(cudaEventRecord(r->ev_pop, r->pop_stream));
+    RCU(cudaEventRecord(r->ev_gemm, r->stream));
+    RCU(cudaStreamWaitEvent(r->stream, r->ev_pop, 0));
+    RCU(cudaStreamWaitEvent(r->pop_stream, r->ev_gemm, 0));
   }
   r->kk += n_ticks;
   r->counted += counted;
-  r->launches += (uint64_t)n_ticks;
+  r->launches += 2 * (uint64_t)n_ticks;
   return check_err(r);
 }
 
