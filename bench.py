@@ -429,6 +429,77 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     }
 
 
+def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
+    """The batching extension: 256 independent networks of uneven size (HCUs
+    8-64, MCUs 5-50, full recurrent), 20 patterns each, advanced together under
+    the schedule the tuner picks, against the plain path (one network per
+    launch, one after the other) on the same first ticks."""
+    import torch
+    from gsbn_b200 import batch
+    members = batch.make_members(n_nets)
+    runs = batch.schedule(20, train_ticks=100, recall_ticks=50)
+    ticks = sum(r[1] for r in runs)
+    cache = os.path.join(tempfile.mkdtemp(prefix="gsbn_tune_"), "tune.json")
+    best, tune_times = batch.tune(members, device=dev, probe_ticks=20, cache=cache)
+
+    def timed(b, rs):
+        """device time of the runs rs: events on every group's stream, from the
+        first start to the last end"""
+        torch.cuda.synchronize()
+        starts, ends = [], []
+        for g in b.groups:
+            st = torch.cuda.ExternalStream(g.net.stream(), device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            starts.append(e0)
+            ends.append((e1, st))
+        for r in rs:
+            b.run_segment(*r)
+        for e1, st in ends:
+            e1.record(st)
+        torch.cuda.synchronize()
+        return max(starts[0].elapsed_time(e1) for e1, _ in ends) * 1e-3
+
+    groups = batch.partition(members, *best)
+    b = batch.Batch(members, groups, device=dev)
+    b.run_segment(*runs[0])  # warm-up (graphs, tables)
+    b.sync()
+    l0, c0 = b.launches(), b.counters()
+    secs = []
+    for _ in range(steps):
+        b.reset()
+        secs.append(timed(b, runs))
+    cells = (b.counters() - c0) / steps
+    launches = (b.launches() - l0) / steps
+    head = [r for r in runs if r[0] <= head_ticks]
+    n_head = sum(r[1] for r in head)
+    b.reset()
+    t_head_best = timed(b, head)
+    b.close()
+    plain = batch.Batch(members, batch.partition(members, "plain"), device=dev)
+    plain.run_segment(*runs[0])
+    plain.sync()
+    plain.reset()
+    c1 = plain.counters()
+    t_head_plain = timed(plain, head)
+    plain_cells = plain.counters() - c1
+    plain.close()
+    sec = statistics.mean(secs)
+    return {
+        "workload": f"{n_nets} independent networks, HCUs 8-64 x MCUs 5-50 (uniform), full recurrent, "
+                    f"{sum(m.cells for m in members) / 1e6:.0f}M cells, 20 patterns each: "
+                    f"{ticks} ticks (20 x 100 training + 20 x 50 recall)",
+        "metric": "network ticks/s", "value": n_nets * ticks / sec, "unit": "network-ticks/s",
+        "cell_updates_per_s": cells / sec, "ms_per_step": sec * 1e3, "steps": steps,
+        "schedule": f"{best[0]}{best[1]}", "groups": len(groups), "gpu_launches_per_step": launches,
+        "tuner_probe_s": tune_times,
+        "plain_one_network_per_launch": {"network_ticks_per_s": n_nets * n_head / t_head_plain,
+                                         "cell_updates_per_s": plain_cells / t_head_plain, "ticks_timed": n_head},
+        "batched_same_ticks": {"network_ticks_per_s": n_nets * n_head / t_head_best},
+        "speedup_vs_plain_same_ticks": t_head_plain / t_head_best,
+    }
+
+
 def cpu_sample(sample_ticks=600):
     """The oracle on a bounded sample of the workload: the first
     `sample_ticks` training ticks (with the start-of-run all-cells pass), then
@@ -536,13 +607,15 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.only_extensions:
         if rank == 0:
-            ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates)}
+            ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates),
+                   "batched": run_batch_extension(local_rank, max(1, args.steps // 2))}
             print(json.dumps({"extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank)
     if rank == 0 and not args.no_extensions:
         out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
-                                                                 args.recall_replicates)}
+                                                                 args.recall_replicates),
+                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2))}
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, sample, secs = cpu_sample(args.cpu_ticks)

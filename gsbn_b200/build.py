@@ -42,14 +42,14 @@ def build(verbose_ptxas=False):
         objs.append(obj)
     for src in _sources("engine", ".cpp"):
         obj = os.path.join(objdir, "engine_" + os.path.basename(src) + ".o")
-        _run([nvcc] + COMMON + ["-x", "c++", "-c", src, "-o", obj])
+        _run([nvcc] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", "-c", src, "-o", obj])
         objs.append(obj)
     lib = os.path.join(HERE, "libgsbn_b200.so")
     _run([nvcc] + ARCH + ["-shared", "-o", lib] + objs + ["-cudart", "static"])
     main = os.path.join(CSRC, "engine", "main", "gsbn_sim.cpp")
     if os.path.exists(main):
         exe = os.path.join(HERE, "gsbn_sim")
-        _run([nvcc] + COMMON + ["-x", "c++", main, "-o", exe, "-L" + HERE, "-lgsbn_b200",
+        _run([nvcc] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", main, "-o", exe, "-L" + HERE, "-lgsbn_b200",
                                 "-Xlinker", "-rpath=$ORIGIN"])
     return lib
 

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -59,6 +60,12 @@ struct bcpnn_net {
   std::vector<PopHost> pops;
   std::vector<ProjHost> projs;
   NetDev h;                 /* host image of the device descriptor */
+  std::vector<PopDev> hp;   /* host images of the per-population descriptors */
+  std::vector<ProjDev> hq;  /* host images of the per-projection descriptors */
+  std::vector<TabRef> tabs; /* host image of the run's decay-table references */
+  PopDev* d_pops = nullptr;
+  ProjDev* d_projs = nullptr;
+  TabRef* d_tabs = nullptr;
   NetDev* d_net = nullptr;
   RunParams rp;             /* host image of the run parameters */
   RunParams* d_rp = nullptr;
@@ -88,6 +95,8 @@ struct bcpnn_net {
 };
 
 namespace {
+
+constexpr int kMaxDevices = 64; /* device ordinals the per-device kernel attributes track */
 
 int fail(bcpnn_net* net, int code, const std::string& msg) {
   if (net) net->err = msg;
@@ -135,7 +144,7 @@ int check_device_error(bcpnn_net* net) {
    with at least `need` entries */
 int fill_slot(bcpnn_net* net, int p, int s, float prn, int need) {
   ProjHost& J = net->projs[p];
-  const ProjDev& D = net->h.projs[p];
+  const ProjDev& D = net->hq[p];
   float kp = D.taupdt * prn;
   TableSlot& T = J.slot[s];
   if (T.ptr && T.kp_bits == bx_fbits(kp) && T.len >= need) return BCPNN_OK;
@@ -161,7 +170,7 @@ int fill_slot(bcpnn_net* net, int p, int s, float prn, int need) {
 int prepare_tables(bcpnn_net* net, int p, float prn, float old_prn, bool with_all, int need_cur, int need_old,
                    int* s_cur, int* s_old) {
   ProjHost& J = net->projs[p];
-  const ProjDev& D = net->h.projs[p];
+  const ProjDev& D = net->hq[p];
   uint32_t b_cur = bx_fbits(D.taupdt * prn), b_old = bx_fbits(D.taupdt * old_prn);
   auto lookup = [&](uint32_t b) {
     for (int s = 0; s < 2; ++s)
@@ -205,10 +214,9 @@ int dzero(bcpnn_net* net, void* p, size_t bytes) {
    vector; connectivity (ii, di), stimulus and replay tables are kept. */
 int reset_state(bcpnn_net* net) {
   int rc;
-  NetDev& H = net->h;
   for (size_t p = 0; p < net->pops.size(); ++p) {
     const PopHost& P = net->pops[p];
-    PopDev& D = H.pops[p];
+    PopDev& D = net->hp[p];
     size_t n = P.n, ne = n * std::max(1, P.dim_proj);
     for (int b = 0; b < 2; ++b) {
       if ((rc = dset(net, D.dsup[b], n, (float)bx_log_d(1.0 / P.M)))) return rc;   /* log(1.0/M), Pop.cpp:59 */
@@ -221,7 +229,7 @@ int reset_state(bcpnn_net* net) {
   }
   for (size_t q = 0; q < net->projs.size(); ++q) {
     const ProjHost& J = net->projs[q];
-    ProjDev& D = H.projs[q];
+    ProjDev& D = net->hq[q];
     size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
     if ((rc = dzero(net, D.qi, R * sizeof(int)))) return rc;
     if ((rc = dset(net, D.pi, R, (float)(1.0 / J.C)))) return rc;                  /* Proj.cpp:91 */
@@ -311,7 +319,7 @@ bool resolve(const bcpnn_net* net, const char* cname, Resolved* r) {
   r->proj = id;
   if (id < (int)net->pops.size()) {
     const PopHost& P = net->pops[id];
-    const PopDev& D = net->h.pops[id];
+    const PopDev& D = net->hp[id];
     size_t n = (size_t)P.n;
     auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
     auto parity = [&](float* a, float* b, size_t count) { r->kind = K_PARITY; r->par[0] = a; r->par[1] = b; r->type = BCPNN_F32; r->count = count; return true; };
@@ -324,7 +332,7 @@ bool resolve(const bcpnn_net* net, const char* cname, Resolved* r) {
   }
   if (id < (int)net->projs.size()) {
     const ProjHost& J = net->projs[id];
-    const ProjDev& D = net->h.projs[id];
+    const ProjDev& D = net->hq[id];
     size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
     auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
     auto cell = [&](int f) { r->kind = K_CELL; r->field = f; r->cell = D.cell; r->type = BCPNN_F32; r->count = cells; return true; };
@@ -385,7 +393,7 @@ const char* bcpnn_last_error(const bcpnn_net* net) { return net ? net->err.c_str
 int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   if (!out) return BCPNN_ERR_INVALID;
   *out = nullptr;
-  if (!desc || desc->n_pops <= 0 || desc->n_pops > 16 || desc->n_projs < 0 || desc->n_projs > kMaxProj ||
+  if (!desc || desc->n_pops <= 0 || desc->n_pops > kMaxPops || desc->n_projs < 0 || desc->n_projs > kMaxProj ||
       (desc->n_pops && !desc->pops) || (desc->n_projs && !desc->projs) || !(desc->dt > 0.0f) ||
       desc->max_ticks_per_run <= 0)
     return BCPNN_ERR_INVALID;
@@ -430,6 +438,9 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   H.dt = desc->dt;
   H.poisson_hz = desc->poisson_noise_hz;
   H.seed = desc->seed;
+  net->hp.assign(desc->n_pops, PopDev());
+  net->hq.assign(desc->n_projs, ProjDev());
+  net->tabs.assign(std::max(1, desc->n_projs), TabRef());
   for (int p = 0; p < desc->n_pops; ++p) {
     PopHost P;
     P.d = desc->pops[p];
@@ -501,9 +512,11 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   std::vector<int> idx_lists;
   for (int p = 0; p < desc->n_pops; ++p) {
     PopHost& P = net->pops[p];
-    PopDev& D = H.pops[p];
+    PopDev& D = net->hp[p];
     D.H = P.H; D.M = P.M; D.n = P.n; D.hcu_start = P.hcu_start; D.mcu_start = P.mcu_start;
     D.dim_proj = P.dim_proj; D.id = p;
+    D.rng_seed = desc->seed; /* Philox key (seed, p*16 + stream); bcpnn_set_pop_rng overrides it */
+    D.rng_pop = (uint32_t)p;
     D.taumdt = dt / P.d.taum;                  /* Pop.cpp:34 */
     D.wtagain = P.d.wtagain;
     D.maxfqdt = P.d.maxfq * dt;                /* Pop.cpp:36 */
@@ -545,13 +558,13 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
       return bail(BCPNN_ERR_CUDA);
     }
     for (int p = 0; p < desc->n_pops; ++p) {
-      H.pops[p].in_proj = dl + off[p].first;
-      H.pops[p].out_proj = dl + off[p].second;
+      net->hp[p].in_proj = dl + off[p].first;
+      net->hp[p].out_proj = dl + off[p].second;
     }
   }
   for (int q = 0; q < desc->n_projs; ++q) {
     ProjHost& J = net->projs[q];
-    ProjDev& D = H.projs[q];
+    ProjDev& D = net->hq[q];
     const bcpnn_proj_desc& d = J.d;
     D.src = d.src_pop; D.dest = d.dest_pop; D.H = J.H; D.M = J.M; D.C = J.C; D.Ns = J.Ns;
     D.proj_in_pop = J.proj_in_pop;
@@ -589,8 +602,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   for (int q = 0; q < desc->n_projs; ++q) {
     const ProjHost& J = net->projs[q];
     size_t R = (size_t)J.H * J.C;
-    if ((rc = dset(net, H.projs[q].ii, R, -1))) return bail(rc);                   /* Proj.cpp:88 */
-    if ((rc = dzero(net, H.projs[q].di, R * sizeof(int)))) return bail(rc);
+    if ((rc = dset(net, net->hq[q].ii, R, -1))) return bail(rc);                   /* Proj.cpp:88 */
+    if ((rc = dzero(net, net->hq[q].di, R * sizeof(int)))) return bail(rc);
   }
   if ((rc = dzero(net, lg, (size_t)net->total_mcu * sizeof(float)))) return bail(rc);
   if ((rc = dzero(net, wm, (size_t)net->total_hcu * sizeof(float)))) return bail(rc);
@@ -616,7 +629,16 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   }
   if ((rc = dalloc(net, &net->d_net, 1))) return bail(rc);
   if ((rc = dalloc(net, &net->d_rp, 1))) return bail(rc);
-  if (cudaMemcpy(net->d_net, &net->h, sizeof(NetDev), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if ((rc = dalloc(net, &net->d_pops, net->hp.size()))) return bail(rc);
+  if ((rc = dalloc(net, &net->d_projs, std::max<size_t>(1, net->hq.size())))) return bail(rc);
+  if ((rc = dalloc(net, &net->d_tabs, net->tabs.size()))) return bail(rc);
+  H.pops = net->d_pops;
+  H.projs = net->d_projs;
+  net->rp.tabs = net->d_tabs;
+  if (cudaMemcpy(net->d_pops, net->hp.data(), net->hp.size() * sizeof(PopDev), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (!net->hq.empty() &&
+       cudaMemcpy(net->d_projs, net->hq.data(), net->hq.size() * sizeof(ProjDev), cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(net->d_net, &net->h, sizeof(NetDev), cudaMemcpyHostToDevice) != cudaSuccess) {
     net->err = "copy of network descriptor failed";
     return bail(BCPNN_ERR_CUDA);
   }
@@ -635,9 +657,22 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     return bail(BCPNN_ERR_INVALID);
   }
   net->tick_smem = smem;
-  if (cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-    net->err = "cannot raise the shared memory limit of tick_kernel";
-    return bail(BCPNN_ERR_CUDA);
+  /* the limit is an attribute of the kernel, shared by every network of the
+     process: only ever raise it, per device, so that a network created later
+     with a smaller need does not lower it under an earlier one */
+  {
+    static std::mutex mu;
+    static size_t raised[kMaxDevices] = {0};
+    std::lock_guard<std::mutex> lock(mu);
+    const int dev = net->device;
+    if (dev < 0 || dev >= kMaxDevices) { net->err = "device ordinal out of range"; return bail(BCPNN_ERR_INVALID); }
+    if (smem > raised[dev]) {
+      if (cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        net->err = "cannot raise the shared memory limit of tick_kernel";
+        return bail(BCPNN_ERR_CUDA);
+      }
+      raised[dev] = smem;
+    }
   }
   /* persistent path: every CTA of the grid must be resident at once */
   {
@@ -687,7 +722,7 @@ int bcpnn_set_conn(bcpnn_net* net, int32_t proj, const int32_t* ii, const int32_
       return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_conn: delay outside [1, 31] ticks");
   }
   CU(cudaSetDevice(net->device));
-  const ProjDev& D = net->h.projs[proj];
+  const ProjDev& D = net->hq[proj];
   CU(cudaMemcpyAsync(D.ii, ii, n_slots * sizeof(int), cudaMemcpyHostToDevice, net->stream));
   CU(cudaMemcpyAsync(D.di, di, n_slots * sizeof(int), cudaMemcpyHostToDevice, net->stream));
   CU(cudaStreamSynchronize(net->stream));
@@ -828,13 +863,25 @@ int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* 
   if (!flat.empty()) CU(cudaMemcpy(P.ext_idx, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
   net->allocs.push_back(P.ext_off);
   net->allocs.push_back(P.ext_idx);
-  PopDev& D = net->h.pops[pop];
+  PopDev& D = net->hp[pop];
   D.ext = 1;
   D.ext_off = P.ext_off;
   D.ext_idx = P.ext_idx;
   D.ext_t0 = t0;
   D.ext_t1 = t1;
-  CU(cudaMemcpy(net->d_net, &net->h, sizeof(NetDev), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(net->d_pops + pop, &D, sizeof(PopDev), cudaMemcpyHostToDevice));
+  return BCPNN_OK;
+}
+
+int bcpnn_set_pop_rng(bcpnn_net* net, int32_t pop, uint32_t seed, uint32_t key_pop) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (pop < 0 || pop >= (int)net->pops.size()) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_pop_rng: no such population");
+  CU(cudaSetDevice(net->device));
+  CU(cudaStreamSynchronize(net->stream));
+  PopDev& D = net->hp[pop];
+  D.rng_seed = seed;
+  D.rng_pop = key_pop;
+  CU(cudaMemcpy(net->d_pops + pop, &D, sizeof(PopDev), cudaMemcpyHostToDevice));
   return BCPNN_OK;
 }
 
@@ -851,14 +898,14 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     int s = 0, so = -1, rc;
     if ((rc = prepare_tables(net, p, prn, old_prn, with_all, need, first_simstep + 1, &s, &so))) return rc;
     const ProjHost& J = net->projs[p];
-    net->rp.tab[p] = J.slot[s].ptr;
-    net->rp.tab_len[p] = J.slot[s].len;
+    net->tabs[p].tab = J.slot[s].ptr;
+    net->tabs[p].len = J.slot[s].len;
     if (with_all) {
-      net->rp.tab_old[p] = J.slot[so].ptr;
-      net->rp.tab_old_len[p] = J.slot[so].len;
+      net->tabs[p].tab_old = J.slot[so].ptr;
+      net->tabs[p].old_len = J.slot[so].len;
     } else {
-      net->rp.tab_old[p] = nullptr;
-      net->rp.tab_old_len[p] = 0;
+      net->tabs[p].tab_old = nullptr;
+      net->tabs[p].old_len = 0;
     }
   }
   net->rp.simstep0 = first_simstep;
@@ -868,6 +915,8 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   net->rp.old_prn = old_prn;
   net->rp.lginp = net->cur_lg;
   net->rp.wmask = net->cur_wm;
+  CU(cudaMemcpyAsync(net->d_tabs, net->tabs.data(), net->tabs.size() * sizeof(TabRef), cudaMemcpyHostToDevice,
+                     net->stream));
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));
   if (net->direct || net->persistent) {
     enqueue_run(net, n_ticks, with_all);
@@ -965,7 +1014,7 @@ int bcpnn_read_state(bcpnn_net* net, const char* name, void* host, size_t bytes)
     }
     case K_SIQ: {
       const ProjHost& J = net->projs[r.proj];
-      const ProjDev& D = net->h.projs[r.proj];
+      const ProjDev& D = net->hq[r.proj];
       std::vector<int> cnt(J.H), list((size_t)J.H * J.C);
       CU(cudaMemcpyAsync(cnt.data(), D.list_cnt, J.H * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
       CU(cudaMemcpyAsync(list.data(), D.list, list.size() * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
@@ -1010,7 +1059,7 @@ int bcpnn_write_state(bcpnn_net* net, const char* name, const void* host, size_t
     }
     case K_SIQ: {
       const ProjHost& J = net->projs[r.proj];
-      const ProjDev& D = net->h.projs[r.proj];
+      const ProjDev& D = net->hq[r.proj];
       const int8_t* in = (const int8_t*)host;
       std::vector<int> cnt(J.H, 0), list((size_t)J.H * J.C, 0);
       for (int hh = 0; hh < J.H; ++hh)
@@ -1100,7 +1149,7 @@ bool resolve_noalloc(const bcpnn_net* net, const char* name, Resolved* r) {
   r->proj = id;
   if (id < (int)net->pops.size()) {
     const PopHost& P = net->pops[id];
-    const PopDev& D = net->h.pops[id];
+    const PopDev& D = net->hp[id];
     size_t n = (size_t)P.n;
     auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
     auto parity = [&](float* a, float* b, size_t count) { r->kind = K_PARITY; r->par[0] = a; r->par[1] = b; r->type = BCPNN_F32; r->count = count; return true; };
@@ -1113,7 +1162,7 @@ bool resolve_noalloc(const bcpnn_net* net, const char* name, Resolved* r) {
   }
   if (id < (int)net->projs.size()) {
     const ProjHost& J = net->projs[id];
-    const ProjDev& D = net->h.projs[id];
+    const ProjDev& D = net->hq[id];
     size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
     auto plain = [&](void* p, int type, size_t count) { r->kind = K_PLAIN; r->ptr = p; r->type = type; r->count = count; return true; };
     auto cell = [&](int f) { r->kind = K_CELL; r->field = f; r->cell = D.cell; r->type = BCPNN_F32; r->count = cells; return true; };

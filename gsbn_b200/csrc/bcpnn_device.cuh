@@ -42,7 +42,8 @@ namespace bcpnn {
 
 constexpr int kBlock = 512;         /* threads of tick_kernel                  */
 constexpr int kWarps = kBlock / 32;
-constexpr int kMaxProj = 64;        /* projections per network                 */
+constexpr int kMaxPops = 4096;      /* populations per network (batches of networks) */
+constexpr int kMaxProj = 4096;      /* projections per network                 */
 constexpr int kRowChunkCells = kBlock; /* row cells staged per chunk (one per thread) */
 constexpr int kColU = 2;            /* column cells per thread per batch         */
 constexpr int kMaxIn = 8;           /* incoming projections per population       */
@@ -53,6 +54,7 @@ constexpr int kErrBarrier = 2;      /* a grid barrier wait ran out of time      
 
 struct PopDev {
   int H, M, n, hcu_start, mcu_start, dim_proj, id;
+  uint32_t rng_seed, rng_pop; /* Philox key of this population's streams: (rng_seed, rng_pop*16 + stream) */
   float taumdt, wtagain, maxfqdt, igain, wgain, lgbias, snoise;
   float* dsup[2];   /* [n], by tick parity                                  */
   float* act;       /* [n]                                                  */
@@ -91,8 +93,8 @@ struct NetDev {
   int n_pops, n_projs;
   float dt, poisson_hz;
   uint32_t seed;
-  PopDev pops[16];
-  ProjDev projs[kMaxProj];
+  const PopDev* pops;   /* [n_pops], device array  */
+  const ProjDev* projs; /* [n_projs], device array */
   const int* cta_pop;   /* CTA -> population */
   const int* cta_hcu;   /* CTA -> HCU        */
   float* lginp;         /* [total MCUs] host-set stimulus */
@@ -118,10 +120,14 @@ struct RunParams {
   float prn, old_prn;
   const float* lginp;   /* stimulus of the run: [total MCUs] */
   const float* wmask;   /* [total HCUs] */
-  const float4* tab[kMaxProj];      /* kp = taupdt*prn     */
-  const float4* tab_old[kMaxProj];  /* kp = taupdt*old_prn */
-  int tab_len[kMaxProj];
-  int tab_old_len[kMaxProj];
+  const struct TabRef* tabs;  /* [n_projs] decay tables of the run */
+};
+
+/* decay tables of one projection for a run */
+struct TabRef {
+  const float4* tab;      /* kp = taupdt*prn     */
+  const float4* tab_old;  /* kp = taupdt*old_prn */
+  int len, old_len;
 };
 
 /* constants of the closed form for one kp */
@@ -278,8 +284,8 @@ __global__ void all_rows_kernel(const NetDev* __restrict__ net, const RunParams*
   int simstep = rp->simstep0 - 1;
   float kp = J.taupdt * rp->old_prn;
   Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-  const float4* tab = rp->tab_old[p];
-  int len = rp->tab_old_len[p];
+  const float4* tab = rp->tabs[p].tab_old;
+  int len = rp->tabs[p].old_len;
   int R = J.H * J.C;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
     int pdt = simstep - J.ti[r];
@@ -303,8 +309,8 @@ __global__ void all_cells_kernel(const NetDev* __restrict__ net, const RunParams
   int simstep = rp->simstep0 - 1;
   float kp = J.taupdt * rp->old_prn;
   Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-  const float4* tab = rp->tab_old[p];
-  int len = rp->tab_old_len[p];
+  const float4* tab = rp->tabs[p].tab_old;
+  int len = rp->tabs[p].old_len;
   size_t ncell = (size_t)J.H * J.C * J.M;
   for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (size_t)gridDim.x * blockDim.x) {
     int pdt = simstep - J.tij[c];

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
     QView V = qview(sm, L, 0, M, J.C);
     int nr = V.nlist[cur0] < row_chunk_rows(M) ? V.nlist[cur0] : row_chunk_rows(M);
     const int p0 = pop.in_proj[0];
-    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, rp->tab[p0], rp->tab_len[p0], sm, L, tid,
+    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, rp->tabs[p0].tab, rp->tabs[p0].len, sm, L, tid,
                kBlock);
   }
 
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
         int idx = h * M + j;
         float noise = 0.0f;
         if (pop.snoise != 0.0f)
-          noise = pop.snoise * dev_normal01(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
+          noise = pop.snoise * dev_normal01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
         float sup = pop.lgbias + pop.igain * lginp[idx] + noise;
         sup += (pop.wgain * wmask[h]) * wsup;
         float d = st_dsup[j];
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
           offset += n;
         }
         float noise = 0.0f;
-        if (pop.snoise != 0.0f) noise = pop.snoise * dev_normal01(net->seed, (uint32_t)P, (uint32_t)simstep, 0u);
+        if (pop.snoise != 0.0f) noise = pop.snoise * dev_normal01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, 0u);
         float sup = pop.lgbias + pop.igain * lginp[0] + noise;
         sup += (pop.wgain * wmask[0]) * wsup;
         float d = __ldcg(pop.dsup[prev]);
@@ -456,10 +456,10 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
         if (vsum > 1.0f) a /= vsum;
         st_act[j] = a;
         st_dsup[j] = w_dsup[j];
-        float u = bx_uniform01(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
+        float u = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
         int8_t spk = (int8_t)(u < a * pop.maxfqdt);
         if (net->poisson_hz > 0.0f) {
-          float up = bx_uniform01_poisson(net->seed, (uint32_t)P, (uint32_t)simstep, (uint32_t)idx);
+          float up = bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
           if (up < pr) spk = 1;
         }
         st_cnt[j] += spk;
@@ -510,8 +510,8 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
         QView V = qview(sm, L, q, M, C);
         const float kp = J.taupdt * prn;
         const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-        const float4* tab = rp->tab[p];
-        const int tlen = rp->tab_len[p];
+        const float4* tab = rp->tabs[p].tab;
+        const int tlen = rp->tabs[p].len;
         const size_t eoff = (size_t)J.proj_in_pop * n;
 
         /* j-traces and bias, Proj.cpp:310-363 */
@@ -683,8 +683,8 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
           QView V = qview(sm, L, q, M, C);
           const float kp = J.taupdt * prn;
           const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-          const float4* tab = rp->tab[p];
-          const int tlen = rp->tab_len[p];
+          const float4* tab = rp->tabs[p].tab;
+          const int tlen = rp->tabs[p].len;
           const uint32_t* cbits = V.bits + cur * V.W;
           const int* clist = V.list + cur * C;
           const int ncol = (pass == 0) ? nspk * C : V.nlist[cur] * nspk;
@@ -756,7 +756,7 @@ __global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restric
       const ProjDev& J = net->projs[p0];
       QView V = qview(sm, L, 0, M, J.C);
       int nr = V.nlist[nxt] < row_chunk_rows(M) ? V.nlist[nxt] : row_chunk_rows(M);
-      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, rp->tab[p0], rp->tab_len[p0], sm, L, tid, kBlock);
+      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, rp->tabs[p0].tab, rp->tabs[p0].len, sm, L, tid, kBlock);
     }
   }
 

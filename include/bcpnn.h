@@ -90,7 +90,7 @@ typedef struct bcpnn_net_desc {
 } bcpnn_net_desc;
 
 /* Build a network on the device with gsbn's initial values.  Limits: at most
-   16 populations, 64 projections, 8 projections into one population, 512
+   4096 populations, 4096 projections, 8 projections into one population, 512
    MCUs per HCU, and one HCU's resident state must fit in shared memory.
    Replaces ProcUpdLazy::init_new (ProcUpdLazy.cpp:8-46), Pop::init_new
    (ProcUpdLazy/Pop.cpp:8-65) and Proj::init_new (ProcUpdLazy/Proj.cpp:6-107). */
@@ -134,6 +134,14 @@ int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t
    Once set, every tick is overridden (ticks not listed give no spikes). */
 int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* ticks, const int32_t* offsets,
                          const int32_t* idx);
+
+/* Key of population `pop`'s random streams: Philox key (seed, key_pop*16 +
+   stream) instead of (desc->seed, pop*16 + stream).  Lets a population of a
+   batch (many independent networks built as one multi-population network)
+   draw exactly the numbers it would draw as population key_pop of a network
+   of its own with that seed.  No counterpart in the reference (its RNG is
+   unseeded, src/gsbn/Random.cpp:5-13). */
+int bcpnn_set_pop_rng(bcpnn_net* net, int32_t pop, uint32_t seed, uint32_t key_pop);
 
 /* Advance n_ticks ticks with simstep first_simstep, first_simstep+1, ... .
    prn is the plasticity of every tick of the run; old_prn is the value of
