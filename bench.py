@@ -333,7 +333,9 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
 
     load()
     eng.run(tr.t0, T, *count)
-    ok = recall.recall_decisions(eng.read("counts"), tr.H, tr.M, expected)
+    counts_all = eng.read("counts")
+    ok = recall.recall_decisions(counts_all, tr.H, tr.M, expected)
+    acc = recall.hcu_accuracy(counts_all, tr.H, tr.M, expected)
     for _ in range(max(0, warmup - 1)):
         load()
         eng.run(tr.t0, T)
@@ -357,7 +359,7 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     pk, pk_kind = peaks()
 
     # the plain FP32 path, one network per replicate
-    plain_ms, plain_ok, plain_cells = [], [], 0
+    plain_ms, plain_ok, plain_acc, plain_cells = [], [], [], 0
     for r in range(plain_sample):
         net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=tr.poisson_hz, device=dev,
                        max_ticks=T)
@@ -378,6 +380,7 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
         bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
         counts = bits[: T - 1].sum(axis=0)[None, :]
         plain_ok.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
+        plain_acc.append(float(recall.hcu_accuracy(counts, tr.H, tr.M, expected[r:r + 1])[0]))
         net.close()
     plain_rate = T / (statistics.mean(plain_ms) * 1e-3)
     value = R * T / (ms * 1e-3)
@@ -388,9 +391,11 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     quiet.set_cues(lg, tr.eps, wm)
     quiet.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
     quiet.run(tr.t0, T, *count)
-    ok_q = recall.recall_decisions(quiet.read("counts"), tr.H, tr.M, expected)
+    counts_q = quiet.read("counts")
+    ok_q = recall.recall_decisions(counts_q, tr.H, tr.M, expected)
+    acc_q = recall.hcu_accuracy(counts_q, tr.H, tr.M, expected)
     quiet.close()
-    plain_q = []
+    plain_q, plain_q_acc = [], []
     for r in range(plain_sample):
         net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=0.0, device=dev, max_ticks=T)
         for n, a in trained.items():
@@ -400,6 +405,7 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
         bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
         counts = bits[: T - 1].sum(axis=0)[None, :]
         plain_q.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
+        plain_q_acc.append(float(recall.hcu_accuracy(counts, tr.H, tr.M, expected[r:r + 1])[0]))
         net.close()
     fp64 = profile_value("recall_precision_64x64.md", "fp64_error")
     return {
@@ -419,12 +425,18 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
                    "plain_fp32_sample": f"{sum(plain_ok)}/{plain_sample}",
                    "decisions_agree_sample": f"{sum(int(a == b) for a, b in zip(ok[:plain_sample], plain_ok))}"
                                              f"/{plain_sample}",
+                   "hcu_accuracy_bf16_all": float(acc.mean()),
+                   "hcu_accuracy_bf16_sample": float(acc[:plain_sample].mean()),
+                   "hcu_accuracy_plain_fp32_sample": float(np.mean(plain_acc)),
                    "without_noise": {"bf16_all": f"{int(ok_q.sum())}/{R}",
                                      "bf16_sample": f"{int(ok_q[:plain_sample].sum())}/{plain_sample}",
                                      "plain_fp32_sample": f"{sum(plain_q)}/{plain_sample}",
                                      "decisions_agree_sample":
                                          f"{sum(int(a == b) for a, b in zip(ok_q[:plain_sample], plain_q))}"
-                                         f"/{plain_sample}"}},
+                                         f"/{plain_sample}",
+                                     "hcu_accuracy_bf16_all": float(acc_q.mean()),
+                                     "hcu_accuracy_bf16_sample": float(acc_q[:plain_sample].mean()),
+                                     "hcu_accuracy_plain_fp32_sample": float(np.mean(plain_q_acc))}},
         "fp64_error": fp64,
     }
 
@@ -460,8 +472,8 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
         torch.cuda.synchronize()
         return max(starts[0].elapsed_time(e1) for e1, _ in ends) * 1e-3
 
-    groups = batch.partition(members, *best)
-    b = batch.Batch(members, groups, device=dev)
+    groups = batch.partition(members, best[0], best[1])
+    b = batch.Batch(members, groups, device=dev, threads=best[2])
     b.run_segment(*runs[0])  # warm-up (graphs, tables)
     b.sync()
     l0, c0 = b.launches(), b.counters()
@@ -491,7 +503,7 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
                     f"{ticks} ticks (20 x 100 training + 20 x 50 recall)",
         "metric": "network ticks/s", "value": n_nets * ticks / sec, "unit": "network-ticks/s",
         "cell_updates_per_s": cells / sec, "ms_per_step": sec * 1e3, "steps": steps,
-        "schedule": f"{best[0]}{best[1]}", "groups": len(groups), "gpu_launches_per_step": launches,
+        "schedule": batch.cand_name(best), "groups": len(groups), "gpu_launches_per_step": launches,
         "tuner_probe_s": tune_times,
         "plain_one_network_per_launch": {"network_ticks_per_s": n_nets * n_head / t_head_plain,
                                          "cell_updates_per_s": plain_cells / t_head_plain, "ticks_timed": n_head},

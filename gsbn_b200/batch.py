@@ -11,12 +11,14 @@ by side on their own CUDA streams (one CUDA-graph-captured launch per tick
 each); a lone group whose HCUs all fit on the GPU at once runs one persistent
 launch per segment.
 
-The schedule (which members go together) is chosen by `tune`: it times each
-candidate partition on the first training ticks and keeps the fastest, cached
-by the member shapes.  Candidates: everything in one group; k groups of
-similar size (sorted by slots per HCU, so that a group's shared memory is
-sized for members like it); one group per member run one after the other
-(one network per launch, the plain path).
+The schedule (which members go together, and the CTA size of the tick
+kernel) is chosen by `tune`: it times each candidate on the first training
+ticks and keeps the fastest, cached by the member shapes.  Candidates:
+everything in one group; k groups of similar size (sorted by slots per HCU,
+so that a group's shared memory is sized for members like it); one group per
+member run one after the other (one network per launch, the plain path);
+each with 512-thread CTAs (one per SM) or 256-thread CTAs (two per SM, for
+small HCUs).
 """
 import hashlib
 import json
@@ -82,14 +84,14 @@ class Group:
     that run side by side on several streams use: a persistent launch relies
     on every CTA of its grid being resident at once."""
 
-    def __init__(self, members, dt=0.001, eps=1e-4, device=0, max_ticks=128, per_tick=False):
+    def __init__(self, members, dt=0.001, eps=1e-4, device=0, max_ticks=128, per_tick=False, threads=512):
         self.members = members
         pops = [m.pop for m in members]
         projs = [dict(m.proj, src_pop=i, dest_pop=i) for i, m in enumerate(members)]
         old = os.environ.get("GSBN_PER_TICK")
         os.environ["GSBN_PER_TICK"] = "1" if per_tick else "0"
         try:
-            self.net = capi.Net(pops, projs, dt, seed=0, device=device, max_ticks=max_ticks)
+            self.net = capi.Net(pops, projs, dt, seed=0, device=device, max_ticks=max_ticks, tick_threads=threads)
         finally:
             if old is None:
                 del os.environ["GSBN_PER_TICK"]
@@ -130,7 +132,13 @@ def partition(members, kind, k=1):
     return groups
 
 
-CANDIDATES = [("one", 1), ("buckets", 2), ("buckets", 4), ("buckets", 8), ("buckets", 16), ("plain", 1)]
+# (partition kind, groups, tick-kernel CTA size)
+CANDIDATES = [("one", 1, 512), ("one", 1, 256), ("buckets", 4, 512), ("buckets", 4, 256), ("buckets", 8, 256),
+              ("buckets", 16, 256), ("buckets", 16, 512), ("plain", 1, 512)]
+
+
+def cand_name(c):
+    return f"{c[0]}{c[1]}/t{c[2]}"
 
 
 class Batch:
@@ -138,11 +146,13 @@ class Batch:
     side on their own streams (one launch per tick each); otherwise one group
     after the other (a group may then use the persistent launch)."""
 
-    def __init__(self, members, groups, device=0, concurrent=None):
+    def __init__(self, members, groups, device=0, concurrent=None, threads=512):
         self.members = members
         self.groups_idx = groups
         self.concurrent = (1 < len(groups) <= 64) if concurrent is None else concurrent
-        self.groups = [Group([members[i] for i in g], device=device, per_tick=self.concurrent) for g in groups]
+        self.threads = threads
+        self.groups = [Group([members[i] for i in g], device=device, per_tick=self.concurrent, threads=threads)
+                       for g in groups]
 
     def run_segment(self, first, n, prn, old_prn, lg_row, wm_row):
         for g in self.groups:
@@ -185,7 +195,7 @@ def shape_key(members):
 
 def tune(members, device=0, probe_ticks=20, cache=None, candidates=CANDIDATES):
     """Time every candidate schedule on the first `probe_ticks` training ticks
-    from the initial state; return (best (kind, k), {name: seconds}).  With
+    from the initial state; return (best (kind, k, threads), {name: seconds}).  With
     `cache` (a JSON path), a result for the same member shapes is reused."""
     key = shape_key(members)
     if cache and os.path.exists(cache):
@@ -194,16 +204,17 @@ def tune(members, device=0, probe_ticks=20, cache=None, candidates=CANDIDATES):
         if key in known:
             return tuple(known[key]["best"]), known[key]["times"]
     times = {}
-    for kind, k in candidates:
-        b = Batch(members, partition(members, kind, k), device)
+    for c in candidates:
+        kind, k, threads = c
+        b = Batch(members, partition(members, kind, k), device, threads=threads)
         b.run_segment(1, 2, 1.0, 0.0, 0, 0)  # warm-up: graphs, tables, the first catch-up
         b.sync()
         t0 = time.perf_counter()
         b.run_segment(3, probe_ticks, 1.0, 1.0, 0, 0)
         b.sync()
-        times[f"{kind}{k}"] = time.perf_counter() - t0
+        times[cand_name(c)] = time.perf_counter() - t0
         b.close()
-    best = min(candidates, key=lambda c: times[f"{c[0]}{c[1]}"])
+    best = min(candidates, key=lambda c: times[cand_name(c)])
     if cache:
         known = {}
         if os.path.exists(cache):

@@ -20,7 +20,16 @@
 
 #include "bcpnn.h"
 #include "bcpnn_device.cuh"
+#define BCPNN_TICK_THREADS 512
+#define BCPNN_TICK_NS t512
 #include "bcpnn_tick.cuh"
+#undef BCPNN_TICK_THREADS
+#undef BCPNN_TICK_NS
+#define BCPNN_TICK_THREADS 256
+#define BCPNN_TICK_NS t256
+#include "bcpnn_tick.cuh"
+#undef BCPNN_TICK_THREADS
+#undef BCPNN_TICK_NS
 #include "bcpnn_numerics.h"
 
 using namespace bcpnn;
@@ -79,6 +88,8 @@ struct bcpnn_net {
   bool direct = false;      /* GSBN_DIRECT_LAUNCH=1: launch kernels one by one (profilers) */
   bool persistent = false;  /* one cooperative launch per run (else one launch per tick) */
   size_t tick_smem = 0;     /* dynamic shared memory of tick_kernel */
+  int threads = 512;        /* CTA size of the tick kernel (512 or 256) */
+  const void* tick_fn = nullptr; /* the tick kernel variant of that size */
   unsigned int* bar = nullptr; /* grid barrier arrival counter of the persistent kernel */
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   uint64_t launches = 0;
@@ -268,11 +279,14 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
     cudaMemsetAsync(net->bar, 0, sizeof(unsigned int), net->stream);
     int it0 = 0, n = n_ticks;
     void* args[] = {(void*)&net->d_net, (void*)&net->d_rp, (void*)&it0, (void*)&n, (void*)&net->bar};
-    cudaLaunchCooperativeKernel((const void*)tick_kernel, dim3(net->total_hcu), dim3(kBlock), args, smem,
-                                net->stream);
+    cudaLaunchCooperativeKernel(net->tick_fn, dim3(net->total_hcu), dim3(net->threads), args, smem, net->stream);
   } else {
-    for (int it = 0; it < n_ticks; ++it)
-      tick_kernel<<<net->total_hcu, kBlock, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+    for (int it = 0; it < n_ticks; ++it) {
+      if (net->threads == 256)
+        t256::tick_kernel<<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+      else
+        t512::tick_kernel<<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+    }
   }
 }
 
@@ -395,10 +409,11 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   *out = nullptr;
   if (!desc || desc->n_pops <= 0 || desc->n_pops > kMaxPops || desc->n_projs < 0 || desc->n_projs > kMaxProj ||
       (desc->n_pops && !desc->pops) || (desc->n_projs && !desc->projs) || !(desc->dt > 0.0f) ||
-      desc->max_ticks_per_run <= 0)
+      desc->max_ticks_per_run <= 0 || (desc->tick_threads != 0 && desc->tick_threads != 256 && desc->tick_threads != 512))
     return BCPNN_ERR_INVALID;
   for (int p = 0; p < desc->n_pops; ++p)
-    if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 || desc->pops[p].mcu_num > kBlock)
+    if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 ||
+        desc->pops[p].mcu_num > (desc->tick_threads == 256 ? 256 : 512))
       return BCPNN_ERR_INVALID;
   {
     std::vector<int> n_in(desc->n_pops, 0);
@@ -417,6 +432,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   net->device = desc->device;
   net->max_ticks = desc->max_ticks_per_run;
   net->exchange = desc->exchange_spikes != 0;
+  net->threads = desc->tick_threads == 256 ? 256 : 512;
+  net->tick_fn = net->threads == 256 ? (const void*)t256::tick_kernel : (const void*)t512::tick_kernel;
   {
     const char* e = std::getenv("GSBN_DIRECT_LAUNCH");
     net->direct = e && e[0] == '1';
@@ -647,7 +664,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   for (const PopHost& P : net->pops) {
     int C[kMaxIn] = {0};
     for (size_t q = 0; q < P.in_proj.size(); ++q) C[q] = net->projs[P.in_proj[q]].C;
-    smem = std::max(smem, tick_smem_bytes_for(P.M, (int)P.in_proj.size(), C));
+    smem = std::max(smem, net->threads == 256 ? t256::tick_smem_bytes_for(P.M, (int)P.in_proj.size(), C)
+                                              : t512::tick_smem_bytes_for(P.M, (int)P.in_proj.size(), C));
   }
   int smem_max = 0;
   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, net->device);
@@ -662,16 +680,16 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
      with a smaller need does not lower it under an earlier one */
   {
     static std::mutex mu;
-    static size_t raised[kMaxDevices] = {0};
+    static size_t raised[2][kMaxDevices] = {{0}};
     std::lock_guard<std::mutex> lock(mu);
-    const int dev = net->device;
+    const int dev = net->device, v = net->threads == 256 ? 1 : 0;
     if (dev < 0 || dev >= kMaxDevices) { net->err = "device ordinal out of range"; return bail(BCPNN_ERR_INVALID); }
-    if (smem > raised[dev]) {
-      if (cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (smem > raised[v][dev]) {
+      if (cudaFuncSetAttribute(net->tick_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         net->err = "cannot raise the shared memory limit of tick_kernel";
         return bail(BCPNN_ERR_CUDA);
       }
-      raised[dev] = smem;
+      raised[v][dev] = smem;
     }
   }
   /* persistent path: every CTA of the grid must be resident at once */
@@ -679,7 +697,7 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     int coop = 0, sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, net->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tick_kernel, kBlock, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, net->tick_fn, net->threads, smem);
     const char* e = std::getenv("GSBN_PER_TICK");
     bool forced = e && e[0] == '1';
     net->persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu;
@@ -1103,7 +1121,7 @@ int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns) {
   cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned int), net->stream);
   /* two CTAs, each waiting for a third arrival that never comes */
   if (e == cudaSuccess) {
-    barrier_probe_kernel<<<2, 32, 0, net->stream>>>(bar, net->h.err, (unsigned long long)limit_ns);
+    t512::barrier_probe_kernel<<<2, 32, 0, net->stream>>>(bar, net->h.err, (unsigned long long)limit_ns);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);

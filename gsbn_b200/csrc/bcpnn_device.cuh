@@ -40,7 +40,8 @@
 
 namespace bcpnn {
 
-constexpr int kBlock = 512;         /* threads of tick_kernel                  */
+constexpr int kBlock = 512;         /* threads of the block-wide helpers below; the
+                                       tick kernel defines its own CTA size  */
 constexpr int kWarps = kBlock / 32;
 constexpr int kMaxPops = 4096;      /* populations per network (batches of networks) */
 constexpr int kMaxProj = 4096;      /* projections per network                 */

@@ -27,12 +27,25 @@
  * is staged into shared memory before the barrier, so its loads overlap the
  * wait.
  */
-#ifndef BCPNN_TICK_CUH
-#define BCPNN_TICK_CUH
 
 #include "bcpnn_device.cuh"
 
+/* This header is compiled once per CTA size: the includer defines
+   BCPNN_TICK_THREADS (512 or 256) and BCPNN_TICK_NS, the namespace the
+   variant lives in.  512 threads suit large HCUs (one CTA per SM); 256
+   threads let two CTAs share an SM, for batches of small HCUs. */
+#ifndef BCPNN_TICK_THREADS
+#define BCPNN_TICK_THREADS 512
+#define BCPNN_TICK_NS t512
+#endif
+
 namespace bcpnn {
+namespace BCPNN_TICK_NS {
+
+constexpr int kBlock = BCPNN_TICK_THREADS;
+constexpr int kWarps = kBlock / 32;
+constexpr int kRowChunkCells = kBlock; /* row cells staged per chunk (one per thread) */
+constexpr int kMinBlocks = kBlock <= 256 ? 2 : 1;
 
 /* The CTA is split in two warp groups that run concurrently inside a tick:
    group A (warps 0-7): support, softmax, spikes, j-traces, active rows;
@@ -282,7 +295,7 @@ __global__ void barrier_probe_kernel(unsigned int* bar, int* err, unsigned long 
 }
 
 /* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */
-__global__ void __launch_bounds__(kBlock, 1) tick_kernel(const NetDev* __restrict__ net,
+__global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* __restrict__ net,
                                                          const RunParams* __restrict__ rp, int it0, int n_ticks,
                                                          unsigned int* bar) {
   extern __shared__ __align__(16) float sm[];
@@ -801,6 +814,5 @@ inline size_t tick_smem_bytes_for(int M, int n_in, const int* C) {
   return (size_t)L.total * 4;
 }
 
+}  // namespace BCPNN_TICK_NS
 }  // namespace bcpnn
-
-#endif /* BCPNN_TICK_CUH */

@@ -238,6 +238,18 @@ class Trained:
         return lg, wm, expected
 
 
+def hcu_accuracy(counts, H, M, expected):
+    """per replicate row: the fraction of cued-pattern HCUs (expected >= 0)
+    whose most-spiking MCU (first on ties, none if silent) is the expected
+    one -- a graded view of the decision ProcCheck takes over all HCUs"""
+    c = counts.reshape(counts.shape[0], H, M).astype(np.int64)
+    mx = c.max(axis=2)
+    idx = np.where(mx > 0, c.argmax(axis=2), -1)
+    exp = expected.astype(np.int64)
+    valid = exp >= 0
+    return ((idx == exp) & valid).sum(axis=1) / np.maximum(valid.sum(axis=1), 1)
+
+
 def recall_decisions(counts, H, M, expected, threshold=0):
     """ProcCheck's per-segment decision (ProcCheck.cpp:185-199, Pop.cpp:35-52)
     for each replicate row: most-spiking MCU per HCU (first on ties, -1 if

@@ -87,6 +87,8 @@ typedef struct bcpnn_net_desc {
   int32_t exchange_spikes;   /* 1: ProcExchangeSpike runs every tick          */
   int32_t device;            /* CUDA device ordinal                           */
   int32_t max_ticks_per_run; /* capacity of the per-run spike log             */
+  int32_t tick_threads;      /* CTA size of the tick kernel: 512 (0 = default)
+                                or 256 (two CTAs per SM, HCUs of <= 256 MCUs) */
 } bcpnn_net_desc;
 
 /* Build a network on the device with gsbn's initial values.  Limits: at most

@@ -22,11 +22,14 @@ def standalone(m):
     return net
 
 
-@pytest.mark.parametrize("groups,concurrent", [([[0, 1, 2, 3, 4]], False), ([[0, 3], [1, 2, 4]], True)])
-def test_members_match_standalone(groups, concurrent):
+@pytest.mark.parametrize("groups,concurrent,threads", [([[0, 1, 2, 3, 4]], False, 512),
+                                                        ([[0, 3], [1, 2, 4]], True, 512),
+                                                        ([[0, 1, 2, 3, 4]], False, 256),
+                                                        ([[0, 3], [1, 2, 4]], True, 256)])
+def test_members_match_standalone(groups, concurrent, threads):
     ms = batch.make_members(n=5, seed=3, hcu=(8, 14), mcu=(5, 12), n_patterns=3)
     runs = batch.schedule(3, train_ticks=30, recall_ticks=20)
-    b = batch.Batch(ms, groups, concurrent=concurrent)
+    b = batch.Batch(ms, groups, concurrent=concurrent, threads=threads)
     singles = [standalone(m) for m in ms]
     for first, n, prn, old, lg, wm in runs:
         b.run_segment(first, n, prn, old, lg, wm)
@@ -45,9 +48,9 @@ def test_members_match_standalone(groups, concurrent):
 def test_tuner_picks_and_caches(tmp_path):
     ms = batch.make_members(n=6, seed=5, hcu=(8, 12), mcu=(5, 8), n_patterns=2)
     cache = str(tmp_path / "tune.json")
-    cands = [("one", 1), ("buckets", 2), ("plain", 1)]
+    cands = [("one", 1, 512), ("buckets", 2, 256), ("plain", 1, 512)]
     best, times = batch.tune(ms, probe_ticks=5, cache=cache, candidates=cands)
-    assert best in cands and set(times) == {"one1", "buckets2", "plain1"}
+    assert best in cands and set(times) == {"one1/t512", "buckets2/t256", "plain1/t512"}
     with open(cache) as f:
         assert batch.shape_key(ms) in json.load(f)
     again, times2 = batch.tune(ms, probe_ticks=5, cache=cache, candidates=cands)

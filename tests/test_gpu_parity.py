@@ -20,8 +20,12 @@ pytestmark = pytest.mark.gpu
 
 def gpu_net(*args, per_tick=False, **kw):
     """a capi.Net on the persistent cooperative path (default) or on the
-    one-launch-per-tick path"""
+    one-launch-per-tick path; per_tick="t256" is the persistent path with
+    256-thread CTAs"""
     old = os.environ.get("GSBN_PER_TICK")
+    if per_tick == "t256":
+        kw["tick_threads"] = 256
+        per_tick = False
     os.environ["GSBN_PER_TICK"] = "1" if per_tick else "0"
     try:
         return capi.Net(*args, **kw)
@@ -32,9 +36,9 @@ def gpu_net(*args, per_tick=False, **kw):
             os.environ["GSBN_PER_TICK"] = old
 
 
-@pytest.fixture(params=["persistent", "per_tick"])
+@pytest.fixture(params=["persistent", "per_tick", "t256"])
 def mode(request):
-    return request.param == "per_tick"
+    return {"persistent": False, "per_tick": True, "t256": "t256"}[request.param]
 
 
 def make_pair(w, directory, max_ticks=256, exchange=True, per_tick=False):
