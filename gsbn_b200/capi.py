@@ -21,7 +21,8 @@ EXPORTS = (
     "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
     "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_ss_flags",
     "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_read_state_noalloc", "bcpnn_counters", "bcpnn_kernel_launches",
-    "bcpnn_selftest_barrier_timeout", "bcpnn_set_pop_rng", "bcpnn_last_error", "bcpnn_status_string",
+    "bcpnn_selftest_barrier_timeout", "bcpnn_set_pop_rng", "bcpnn_prune", "bcpnn_last_error",
+    "bcpnn_status_string",
 )
 
 
@@ -89,6 +90,7 @@ def load():
         "bcpnn_kernel_launches": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_selftest_barrier_timeout": (ctypes.c_int, [vp, ctypes.c_int64]),
         "bcpnn_set_pop_rng": (ctypes.c_int, [vp, i32, ctypes.c_uint32, ctypes.c_uint32]),
+        "bcpnn_prune": (ctypes.c_int, [vp, i32, i32, ctypes.c_float, ctypes.c_float, vp, sz, P(i32)]),
         "bcpnn_last_error": (ctypes.c_char_p, [vp]),
         "bcpnn_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     }
@@ -234,6 +236,14 @@ class Net:
         out = (ctypes.c_uint64 * 3)()
         self._check(self._lib.bcpnn_counters(self._h, out))
         return [int(out[0]), int(out[1]), int(out[2])]
+
+    def prune(self, proj, threshold_t, wp, wn):
+        """disconnect weak or stale rows; returns their source MCUs in row order"""
+        n_slots = self.info(f"ii_{proj}")[1]
+        out = np.zeros(max(1, n_slots), np.int32)
+        n = ctypes.c_int32()
+        self._check(self._lib.bcpnn_prune(self._h, proj, threshold_t, wp, wn, _ptr(out), out.size, ctypes.byref(n)))
+        return out[:n.value].copy()
 
     def set_pop_rng(self, pop, seed, key_pop):
         self._check(self._lib.bcpnn_set_pop_rng(self._h, pop, seed, key_pop))

@@ -1092,6 +1092,32 @@ int bcpnn_write_state(bcpnn_net* net, const char* name, const void* host, size_t
   return BCPNN_OK;
 }
 
+int bcpnn_prune(bcpnn_net* net, int32_t proj, int32_t threshold_t, float wp, float wn, int32_t* removed_src,
+                size_t cap, int32_t* n_removed) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (proj < 0 || proj >= (int)net->projs.size() || !removed_src || !n_removed)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_prune: bad projection or null buffer");
+  if (!(wp > wn)) return fail(net, BCPNN_ERR_INVALID, "bcpnn_prune: w+ must be larger than w-");
+  const ProjHost& J = net->projs[proj];
+  const size_t R = (size_t)J.H * J.C;
+  if (cap < R) return fail(net, BCPNN_ERR_SIZE, "bcpnn_prune: removed_src must hold H*C entries");
+  CU(cudaSetDevice(net->device));
+  int rc = ensure_scratch(net, R);
+  if (rc) return rc;
+  int* out = reinterpret_cast<int*>(net->scratch);
+  prune_rows_kernel<<<grid_for(R * 32, 256), 256, 0, net->stream>>>(net->d_projs, proj, threshold_t, wp, wn, out);
+  CU(cudaGetLastError());
+  net->launches += 1;
+  std::vector<int> all(R);
+  CU(cudaMemcpyAsync(all.data(), out, R * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  int32_t n = 0;
+  for (size_t r = 0; r < R; ++r)
+    if (all[r] >= 0) removed_src[n++] = all[r];
+  *n_removed = n;
+  return BCPNN_OK;
+}
+
 int bcpnn_counters(bcpnn_net* net, uint64_t out[3]) {
   if (!net || !out) return BCPNN_ERR_INVALID;
   CU(cudaSetDevice(net->device));

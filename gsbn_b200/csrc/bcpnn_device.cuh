@@ -409,6 +409,54 @@ __global__ void cell_scatter_kernel(float4* cell, size_t n, int field, const flo
   }
 }
 
+/* Structural-plasticity pruning of one projection, one warp per row
+   (ProcStructuralPlasticity/Prj.cpp:130-165 prune, :69-92 remove_conn).  A
+   connected row (ii >= 0) goes when its row tick ti is below threshold_t, or
+   when none of its weights reaches wp or wn (w >= wp or w <= wn; a NaN weight
+   reaches neither).  A removed row gets ii = -1, di = 0, ti = 0, pi = 0,
+   ei = 0 and pij = eij = zj2 = 0 in its cells; zi, zi2, tij, wij and the delay
+   queue stay as they are, as in gsbn.  out[r] = the removed source MCU, or -1. */
+__global__ void prune_rows_kernel(const ProjDev* __restrict__ projs, int p, int threshold_t, float wp, float wn,
+                                  int* __restrict__ out) {
+  const ProjDev& J = projs[p];
+  const int R = J.H * J.C, M = J.M;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < R; r += nw) {
+    const int src = J.ii[r];
+    bool removed = false;
+    if (src >= 0) {
+      if (J.ti[r] < threshold_t) {
+        removed = true;
+      } else {
+        bool strong = false;
+        for (int j = lane; j < M; j += 32) {
+          const float w = J.wij[(size_t)r * M + j];
+          strong |= (w >= wp || w <= wn);
+        }
+        removed = !__any_sync(0xffffffffu, strong);
+      }
+    }
+    if (removed) {
+      for (int j = lane; j < M; j += 32) {
+        float4 c = J.cell[(size_t)r * M + j];
+        c.x = 0.0f; /* pij */
+        c.y = 0.0f; /* eij */
+        c.w = 0.0f; /* zj2 */
+        J.cell[(size_t)r * M + j] = c;
+      }
+      if (lane == 0) {
+        J.ii[r] = -1;
+        J.di[r] = 0;
+        J.ti[r] = 0;
+        J.pi[r] = 0.0f;
+        J.ei[r] = 0.0f;
+      }
+    }
+    if (lane == 0) out[r] = removed ? src : -1;
+  }
+}
+
 }  // namespace bcpnn
 
 #endif /* BCPNN_DEVICE_CUH */

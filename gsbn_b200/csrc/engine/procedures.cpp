@@ -8,6 +8,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
@@ -904,5 +905,286 @@ class ProcSnapshot : public ProcedureBase {
   int _offset = 0, _period = 1;
 };
 REGISTERIMPL(ProcSnapshot)
+
+/* =================================================================
+ * ProcStructuralPlasticity (src/gsbn/procedures/ProcStructuralPlasitcity.cpp:8-631,
+ * ProcStructuralPlasticity/Prj.cpp, Pop.cpp): every `pruning-period` ticks,
+ * disconnect slot rows that are stale (row tick older than `t-th` ticks) or
+ * weak (no weight reaches `wp` or `wn`), on the device (bcpnn_prune), and
+ * give each removed row's source MCU its fanout back; every `period` ticks,
+ * connect active source MCUs to active destination HCUs through free slots.
+ * Only during plastic segments (mode_param plasticity != 0).
+ *
+ * Kept from gsbn: the loop order and every selection rule, including two
+ * quirks: a destination HCU counts as having a free slot when HCU 0 has one
+ * (Prj.cpp:111-117 scans the first dim_conn slots for every HCU), and the
+ * HCU-activity threshold 0.5 is passed as an int, i.e. 0 (:426).  Reading a
+ * source MCU's activity clears the population's spike counters (Pop.cpp:60-70).
+ * Changed: gsbn draws from std::random_device (unreplayable); here every
+ * draw comes from a Philox4x32-10 stream keyed (argi "seed", 0x5350), draw i
+ * at counter (i, i >> 32, 0x53505241, 0), uniform (x >> 8) * 2^-24, and
+ * shuffles are Fisher-Yates from the back with j = floor(u * (i + 1)).
+ * Geometric delays (enable-geometry) must land in 1..31 ticks.
+ * ================================================================= */
+class ProcStructuralPlasticity : public ProcedureBase {
+  REGISTER(ProcStructuralPlasticity)
+ public:
+  void init_new(SolverParam sp, Database& db) override {
+    _db = &db;
+    _net = db.require_net("ProcStructuralPlasticity");
+    Parser par(get_proc_param(sp));
+    _glv.getf("dt", _dt);
+    if (par.argf("d-norm", _d_norm) && _d_norm < 0) _d_norm = 0;
+    if (par.argf("v-cond", _v_cond) && _v_cond <= 0) _v_cond = 1;
+    if (par.argi("t-th", _t_th) && _t_th <= 0) _t_th = 100;
+    if (par.argi("period", _period) && _period <= 0) _period = 100;
+    if (par.argi("pruning-period", _pruning_period) && _pruning_period <= 0) _pruning_period = 1000;
+    if (par.argi("enable-geometry", _geometry) && _geometry != 0) _geometry = 1;
+    if (par.argi("enable-init-conn", _init_conn) && _init_conn != 0) _init_conn = 1;
+    par.argf("wp", _wp);
+    par.argf("wn", _wn);
+    int seed = 0;
+    par.argi("seed", seed);
+    _seed = (uint32_t)seed;
+    if (!(_wp > _wn)) fatal("ProcStructuralPlasticity: w+ should be larger than w- !!");
+    for (const PopParam& pp : sp.net_param.pop_param)
+      for (uint32_t k = 0; k < pp.pop_num; k++) {
+        PopInfo P;
+        P.H = (int)pp.hcu_num;
+        P.M = (int)pp.mcu_num;
+        P.fanout.assign((size_t)P.H * P.M, (int)pp.fanout_num);
+        P.shape.assign(pp.shape.begin(), pp.shape.end());
+        P.position.assign(pp.position.begin(), pp.position.end());
+        _pops.push_back(P);
+      }
+    for (size_t k = 0; k < db.projs.size(); k++) {
+      const bcpnn_proj_desc& q = db.projs[k];
+      PrjInfo J;
+      J.src = q.src_pop;
+      J.dest = q.dest_pop;
+      J.H = _pops[J.dest].H;
+      J.M = _pops[J.dest].M;
+      J.C = (int)std::min<long long>((long long)_pops[J.src].H * _pops[J.src].M, (long long)q.slot_num);
+      _prjs.push_back(J);
+      _pops[J.src].out.push_back((int)k);
+    }
+    if (_init_conn) grow(-1, -1);
+  }
+  void init_copy(SolverParam sp, Database& db) override { init_new(sp, db); }
+  void update_cpu() override { update_gpu(); }
+  void update_gpu() override {
+    int cf = 0, t = 0;
+    _glv.geti("cycle-flag", cf);
+    _glv.geti("simstep", t);
+    if (cf == 1) at_tick(t);
+  }
+  bool supports_runs() const override { return true; }
+  /* the work happens right after ticks that are multiples of the periods */
+  int run_horizon(int t) override {
+    auto next = [&](int period) { int r = t % period; return r ? t + period - r : t; };
+    return std::min(next(_period), next(_pruning_period)) - t + 1;
+  }
+  void update_run(RunWindow& w) override {
+    if (w.cycle_flag != 1) return;
+    at_tick(w.first + w.n - 1);
+  }
+
+ private:
+  struct PopInfo {
+    int H = 0, M = 0;
+    std::vector<int> fanout;
+    std::vector<int> shape, position;
+    std::vector<int> out; /* projections with this population as source, in id order */
+  };
+  struct PrjInfo {
+    int src = 0, dest = 0, H = 0, M = 0, C = 0;
+  };
+
+  void at_tick(int t) {
+    bool plastic = false;
+    _glv.getb("plasticity", plastic);
+    if (!plastic) return;
+    if (t % _pruning_period == 0) prune(t);
+    if (t % _period == 0) grow(0, (int)(0.2 * _period * 100 * _dt)); /* ProcStructuralPlasitcity.cpp:426-458 */
+  }
+
+  /* stages 1-2 (ProcStructuralPlasitcity.cpp:275-350) */
+  void prune(int t) {
+    for (size_t k = 0; k < _prjs.size(); k++) {
+      const PrjInfo& J = _prjs[k];
+      std::vector<int32_t> removed((size_t)J.H * J.C + 1);
+      int32_t n = 0;
+      int st = bcpnn_prune(_net, (int32_t)k, t - _t_th, _wp, _wn, removed.data(), removed.size(), &n);
+      if (st != BCPNN_OK) fatal(std::string("bcpnn_prune: ") + bcpnn_last_error(_net));
+      std::vector<int>& fan = _pops[J.src].fanout;
+      for (int32_t i = 0; i < n; i++) fan[removed[i]] += 1;
+    }
+  }
+
+  std::vector<int32_t> read_i32(const std::string& name) {
+    std::vector<uint8_t> b = _db->read_state(name);
+    std::vector<int32_t> v(b.size() / 4);
+    if (!v.empty()) std::memcpy(v.data(), b.data(), b.size());
+    return v;
+  }
+  std::vector<float> read_f32(const std::string& name) {
+    std::vector<uint8_t> b = _db->read_state(name);
+    std::vector<float> v(b.size() / 4);
+    if (!v.empty()) std::memcpy(v.data(), b.data(), b.size());
+    return v;
+  }
+
+  float uniform() {
+    bx_u32x4 c;
+    c.v[0] = (uint32_t)_draws;
+    c.v[1] = (uint32_t)(_draws >> 32);
+    c.v[2] = 0x53505241u;
+    c.v[3] = 0u;
+    _draws++;
+    return bx_u01(bx_philox4x32_10(c, _seed, 0x5350u).v[0]);
+  }
+  void shuffle(std::vector<int>& a) {
+    for (size_t i = a.size(); i-- > 1;) {
+      size_t j = (size_t)((double)uniform() * (double)(i + 1));
+      if (j > i) j = i;
+      std::swap(a[i], a[j]);
+    }
+  }
+
+  /* stages 3-5 (ProcStructuralPlasitcity.cpp:352-560; init_conn :113-258 with
+     thresholds -1) */
+  void grow(int hcu_threshold, int mcu_threshold) {
+    const size_t np = _prjs.size();
+    std::vector<std::vector<int32_t>> local(np), avail_hcu(np);
+    for (size_t k = 0; k < np; k++) {
+      const PrjInfo& J = _prjs[k];
+      local[k] = read_i32("ii_" + std::to_string(k));
+      std::vector<float> ej = read_f32("ej_" + std::to_string(k));
+      bool free_slot = false; /* gsbn scans HCU 0's slots for every HCU (Prj.cpp:111-117) */
+      for (int j = 0; j < J.C; j++)
+        if (local[k][j] < 0) {
+          free_slot = true;
+          break;
+        }
+      for (int i = 0; i < J.H; i++) {
+        float acc = 0;
+        for (int j = 0; j < J.M; j++) acc += ej[(size_t)i * J.M + j];
+        if (acc > (float)hcu_threshold && free_slot) avail_hcu[k].push_back(i);
+      }
+    }
+    for (size_t pi = 0; pi < _pops.size(); pi++) {
+      PopInfo& P = _pops[pi];
+      /* active source MCUs; the counters are cleared as they are read (Pop.cpp:60-70) */
+      const std::string cname = ".counter_" + std::to_string(pi);
+      std::vector<int32_t> cnt = read_i32(cname);
+      std::vector<int> active;
+      for (size_t i = 0; i < cnt.size(); i++)
+        if (cnt[i] > mcu_threshold) active.push_back((int)i);
+      std::vector<int32_t> zero(cnt.size(), 0);
+      _db->write_state(cname, zero.data(), zero.size() * 4);
+      std::vector<int> prjs = P.out;
+      while (!prjs.empty() && !active.empty()) {
+        float u = uniform();
+        size_t idx = (size_t)(int)(u * (float)prjs.size());
+        if (idx >= prjs.size()) idx = prjs.size() - 1;
+        const int k = prjs[idx];
+        const PrjInfo& J = _prjs[k];
+        std::vector<int> hcus(avail_hcu[k].begin(), avail_hcu[k].end());
+        if (hcus.empty()) break;
+        shuffle(hcus);
+        for (int h : hcus) {
+          std::vector<int> cand = active;
+          for (int s = 0; s < J.C; s++) {
+            int c = local[k][(size_t)h * J.C + s];
+            if (c >= 0) cand.erase(std::remove(cand.begin(), cand.end(), c), cand.end());
+          }
+          if (cand.empty()) continue;
+          shuffle(cand);
+          size_t l = 0;
+          for (int s = 0; s < J.C && l < cand.size(); s++) {
+            int32_t& slot = local[k][(size_t)h * J.C + s];
+            if (slot < 0) slot = cand[l++];
+          }
+          for (size_t i = 0; i < l; i++) {
+            int mcu = cand[i];
+            if (--P.fanout[mcu] <= 0) active.erase(std::remove(active.begin(), active.end(), mcu), active.end());
+          }
+        }
+        prjs.erase(prjs.begin() + idx);
+      }
+    }
+    /* stage 5: new rows into the first free slot of their HCU (add_row, :576-588) */
+    for (size_t k = 0; k < np; k++) {
+      const PrjInfo& J = _prjs[k];
+      std::vector<int32_t> ii = read_i32("ii_" + std::to_string(k));
+      std::vector<int32_t> di = read_i32("di_" + std::to_string(k));
+      const std::vector<int32_t> cur = ii;
+      bool changed = false;
+      for (int h = 0; h < J.H; h++)
+        for (int s = 0; s < J.C; s++) {
+          const size_t index = (size_t)h * J.C + s;
+          if (cur[index] >= 0 || ii[index] >= 0 || local[k][index] < 0) continue;
+          const int src = local[k][index];
+          const int delay = _geometry ? delay_cycle(J, src, h) : 1;
+          for (int f = 0; f < J.C; f++) {
+            if (ii[(size_t)h * J.C + f] < 0) {
+              ii[(size_t)h * J.C + f] = src;
+              di[(size_t)h * J.C + f] = delay;
+              changed = true;
+              break;
+            }
+          }
+        }
+      if (changed) {
+        int st = bcpnn_set_conn(_net, (int32_t)k, ii.data(), di.data(), ii.size());
+        if (st != BCPNN_OK) fatal(std::string("ProcStructuralPlasticity: ") + bcpnn_last_error(_net));
+      }
+    }
+  }
+
+  std::vector<int> hcu_coor(const PopInfo& P, int hcu) const { /* Pop.cpp:72-91 */
+    std::vector<int> coor(P.shape.size());
+    int index = hcu;
+    for (size_t i = 0; i < P.shape.size(); i++) {
+      if (P.shape[i] <= 0) fatal("ProcStructuralPlasticity: population shape entries must be > 0");
+      coor[i] = index % P.shape[i];
+      index /= P.shape[i];
+    }
+    for (size_t i = 0; i < P.position.size(); i++) {
+      if (i < coor.size())
+        coor[i] += P.position[i];
+      else
+        coor.push_back(P.position[i]);
+    }
+    return coor;
+  }
+
+  int delay_cycle(const PrjInfo& J, int src_mcu, int dest_hcu) { /* :590-625 */
+    const PopInfo& P0 = _pops[J.src];
+    const PopInfo& P1 = _pops[J.dest];
+    std::vector<int> a = hcu_coor(P0, src_mcu / P0.M), b = hcu_coor(P1, dest_hcu);
+    while (a.size() < b.size()) a.push_back(0);
+    while (b.size() < a.size()) b.push_back(0);
+    float d2 = 0;
+    for (size_t i = 0; i < a.size(); i++) d2 += (float)((a[i] - b[i]) * (a[i] - b[i]));
+    const float distance = (float)std::sqrt((double)d2);
+    const float mean = _d_norm * distance / _v_cond + 1;
+    /* normal(mean, 0.1 mean) by Box-Muller from two draws of the stream */
+    const double u1 = 1.0 - (double)uniform(), u2 = (double)uniform();
+    const double z = std::sqrt(-2.0 * bx_log_d(u1)) * bx_cos2pi_d(u2);
+    const float tij = (float)(mean + 0.1 * mean * z);
+    return (int)std::ceil(tij * 0.001 / _dt);
+  }
+
+  Database* _db = nullptr;
+  bcpnn_net* _net = nullptr;
+  float _dt = 0.001f, _d_norm = 0.75f, _v_cond = 0.2f, _wp = 0.5f, _wn = -0.5f;
+  int _t_th = 100, _period = 100, _pruning_period = 1000, _geometry = 0, _init_conn = 0;
+  uint32_t _seed = 0;
+  uint64_t _draws = 0;
+  std::vector<PopInfo> _pops;
+  std::vector<PrjInfo> _prjs;
+};
+REGISTERIMPL(ProcStructuralPlasticity)
 
 }  // namespace gsbn

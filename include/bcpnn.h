@@ -137,6 +137,17 @@ int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t
 int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* ticks, const int32_t* offsets,
                          const int32_t* idx);
 
+/* Structural-plasticity pruning of projection `proj`, on the device:
+   every connected slot row whose row tick ti is below threshold_t, or none of
+   whose weights reaches wp or wn (w >= wp or w <= wn), is disconnected
+   (ii = -1, di = 0, ti = 0, pi = 0, ei = 0, and pij, eij, zj2 of its cells set
+   to 0).  removed_src (cap >= H*C entries) receives the source MCUs of the
+   removed rows in row order, *n_removed their number.  Replaces
+   ProcStructuralPlasticity's Prj::prune / remove_conn
+   (ProcStructuralPlasticity/Prj.cpp:69-92, 130-165).  Synchronises. */
+int bcpnn_prune(bcpnn_net* net, int32_t proj, int32_t threshold_t, float wp, float wn, int32_t* removed_src,
+                size_t cap, int32_t* n_removed);
+
 /* Key of population `pop`'s random streams: Philox key (seed, key_pop*16 +
    stream) instead of (desc->seed, pop*16 + stream).  Lets a population of a
    batch (many independent networks built as one multi-population network)

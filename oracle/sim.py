@@ -345,6 +345,7 @@ class ExtGen:
         self.cycle_flag = 0
         self.wmask_idx = 0
         self.lginp_changed = False
+        self.plasticity = False
 
     def tick(self):
         self.simstep += 1
@@ -356,6 +357,7 @@ class ExtGen:
                 self.old_prn = self.prn
                 self.prn = m["prn"]
                 self.wmask_idx = m["wmask_id"]
+                self.plasticity = bool(m["plasticity"])
                 self.cycle_flag = 1
                 if self.old_lgidx_id != m["lgidx_id"]:
                     self.old_lgidx_id = m["lgidx_id"]
@@ -506,6 +508,145 @@ class SpkRec:
 
 
 # ---------------------------------------------------------------------------
+# ProcStructuralPlasticity (ProcStructuralPlasitcity.cpp:8-631,
+# ProcStructuralPlasticity/Prj.cpp:69-165, Pop.cpp:6-91), with gsbn's
+# random_device draws replaced by the seeded Philox stream the product uses:
+# draw i = philox((i, i >> 32, 0x53505241, 0), (seed, 0x5350))[0], uniform
+# (x >> 8) * 2^-24; Fisher-Yates from the back with j = floor(u * (i + 1)).
+# enable-geometry (random delays) is not restated here.
+# ---------------------------------------------------------------------------
+
+class StructuralPlasticity:
+    def __init__(self, sp, net, pops, projs, dt):
+        argi, argf, _ = proc_args(sp, "ProcStructuralPlasticity")
+        self.net, self.pops, self.projs, self.dt = net, pops, projs, f32(dt)
+        self.t_th = argi.get("t-th", 100) if argi.get("t-th", 100) > 0 else 100
+        self.period = argi.get("period", 100) if argi.get("period", 100) > 0 else 100
+        pp = argi.get("pruning-period", 1000)
+        self.pruning_period = pp if pp > 0 else 1000
+        if argi.get("enable-geometry", 0):
+            raise NotImplementedError("enable-geometry is not restated in the oracle")
+        self.wp, self.wn = f32(argf.get("wp", 0.5)), f32(argf.get("wn", -0.5))
+        self.seed = argi.get("seed", 0) & 0xFFFFFFFF
+        self.draws = 0
+        fan = [pp.fanout_num for pp in sp.net_param.pop_param for _ in range(pp.pop_num)]
+        self.fanout = [np.full(p["hcu_num"] * p["mcu_num"], fan[i], np.int64) for i, p in enumerate(pops)]
+        self.out = [[k for k, q in enumerate(projs) if q["src_pop"] == i] for i in range(len(pops))]
+        if argi.get("enable-init-conn", 0):
+            self.grow(-1, -1)
+
+    def uniform(self):
+        i = self.draws
+        self.draws += 1
+        x = philox([i & 0xFFFFFFFF, (i >> 32) & 0xFFFFFFFF, 0x53505241, 0], [self.seed, 0x5350])[0]
+        return f32(int(x) >> 8) * f32(2.0 ** -24)
+
+    def shuffle(self, a):
+        for i in range(len(a) - 1, 0, -1):
+            j = min(i, int(float(self.uniform()) * (i + 1)))
+            a[i], a[j] = a[j], a[i]
+
+    def update(self, cycle_flag, simstep, plasticity):
+        if cycle_flag != 1 or not plasticity:
+            return
+        if simstep % self.pruning_period == 0:
+            self.prune(simstep)
+        if simstep % self.period == 0:
+            self.grow(0, int(0.2 * self.period * 100 * float(self.dt)))
+
+    def prune(self, t):
+        """Prj::prune + remove_conn for every projection, fanout given back"""
+        for k, q in enumerate(self.projs):
+            ii, ti, wij = self.net.read(f"ii_{k}"), self.net.read(f"ti_{k}"), self.net.read(f"wij_{k}")
+            M = self.pops[q["dest_pop"]]["mcu_num"]
+            w = wij.reshape(-1, M)
+            strong = np.any((w >= self.wp) | (w <= self.wn), axis=1)
+            removed = (ii >= 0) & ((ti < t - self.t_th) | ~strong)
+            src = ii[removed].copy()
+            if removed.any():
+                for name, val in (("ii", -1), ("di", 0), ("ti", 0), ("pi", 0), ("ei", 0)):
+                    a = self.net.read(f"{name}_{k}")
+                    a[removed] = val
+                    self.net.write(f"{name}_{k}", a)
+                cells = np.repeat(removed, M)
+                for name in ("pij", "eij", "zj2"):
+                    a = self.net.read(f"{name}_{k}")
+                    a[cells] = 0
+                    self.net.write(f"{name}_{k}", a)
+            for c in src:
+                self.fanout[q["src_pop"]][c] += 1
+
+    def grow(self, hcu_threshold, mcu_threshold):
+        local, avail_hcu = [], []
+        for k, q in enumerate(self.projs):
+            dest, srcp = self.pops[q["dest_pop"]], self.pops[q["src_pop"]]
+            H, M = dest["hcu_num"], dest["mcu_num"]
+            C = min(srcp["hcu_num"] * srcp["mcu_num"], int(q["slot_num"]))
+            ii = self.net.read(f"ii_{k}").copy()
+            ej = self.net.read(f"ej_{k}").astype(np.float32)
+            free_slot = bool(np.any(ii[:C] < 0))  # gsbn looks at HCU 0's slots for every HCU
+            hcus = []
+            for i in range(H):
+                acc = f32(0)
+                for j in range(M):
+                    acc = f32(acc + ej[i * M + j])
+                if acc > f32(hcu_threshold) and free_slot:
+                    hcus.append(i)
+            local.append(ii)
+            avail_hcu.append((hcus, C))
+        for pi, p in enumerate(self.pops):
+            cnt = self.net.read(f".counter_{pi}")
+            active = [int(i) for i in np.nonzero(cnt > mcu_threshold)[0]]
+            self.net.write(f".counter_{pi}", np.zeros_like(cnt))
+            prjs = list(self.out[pi])
+            fan = self.fanout[pi]
+            while prjs and active:
+                u = self.uniform()
+                idx = min(int(f32(u) * f32(len(prjs))), len(prjs) - 1)
+                k = prjs[idx]
+                hcus, C = avail_hcu[k]
+                hcus = list(hcus)
+                if not hcus:
+                    break
+                self.shuffle(hcus)
+                for h in hcus:
+                    row = local[k][h * C:(h + 1) * C]
+                    taken = set(int(c) for c in row if c >= 0)
+                    cand = [m for m in active if m not in taken]
+                    if not cand:
+                        continue
+                    self.shuffle(cand)
+                    l = 0
+                    for s in range(C):
+                        if l >= len(cand):
+                            break
+                        if row[s] < 0:
+                            row[s] = cand[l]
+                            l += 1
+                    for m in cand[:l]:
+                        fan[m] -= 1
+                        if fan[m] <= 0:
+                            active = [x for x in active if x != m]
+                del prjs[idx]
+        for k, q in enumerate(self.projs):
+            hcus, C = avail_hcu[k]
+            ii = self.net.read(f"ii_{k}").copy()
+            di = self.net.read(f"di_{k}").copy()
+            H = self.pops[q["dest_pop"]]["hcu_num"]
+            for h in range(H):
+                for s in range(C):
+                    idx = h * C + s
+                    if ii[idx] >= 0 or local[k][idx] < 0:
+                        continue
+                    free = np.nonzero(ii[h * C:(h + 1) * C] < 0)[0]
+                    f = h * C + int(free[0])
+                    ii[f] = local[k][idx]
+                    di[f] = 1
+            self.net.write(f"ii_{k}", ii)
+            self.net.write(f"di_{k}", di)
+
+
+# ---------------------------------------------------------------------------
 # Solver loop (Solver.cpp:67-92, Upd.cpp:28-40)
 # ---------------------------------------------------------------------------
 
@@ -545,6 +686,9 @@ def simulate(sp, base_dir, real_bits=32, math=MATH_SHARED, max_ticks=None, stim=
     if "ProcSpkRec" in names:
         a = proc_args(sp, "ProcSpkRec")[0]
         rec = SpkRec(sp, pops, len(projs), a.get("offset", 0), a.get("period", 1))
+    spl = None
+    if "ProcStructuralPlasticity" in names:
+        spl = StructuralPlasticity(sp, net, pops, projs, float(f32(sp.gen_param.dt)))
     chk = None
     if "ProcCheck" in names:
         chk = Check(sp, gen.lgidx, pops, proc_args(sp, "ProcCheck")[0].get("threashold", 0))
@@ -571,6 +715,8 @@ def simulate(sp, base_dir, real_bits=32, math=MATH_SHARED, max_ticks=None, stim=
                         ssj = net.read(f".ssj_{k}")
                         flags.append((bool(np.any(ssi == 9)), bool(np.any(ssj == 9))))
                     rec.update(gen.cycle_flag, gen.simstep, sp_idx, flags)
+            elif name == "ProcStructuralPlasticity" and spl is not None:
+                spl.update(gen.cycle_flag, gen.simstep, gen.plasticity)
             elif name == "ProcCheck" and chk is not None:
                 spikes_i8 = [net.read(f"spike_{k}") for k in range(len(pops))] if gen.cycle_flag > 0 else None
                 chk.update(gen.cycle_flag, gen.simstep, spikes_i8)

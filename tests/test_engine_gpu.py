@@ -167,3 +167,32 @@ def test_gsbn_sim_command(tmp_path):
     assert rec_files(sp)["ProcSpkRec/spk_pop_0.csv"] == want["ProcSpkRec/spk_pop_0.csv"]
     bad = subprocess.run([GSBN_SIM, "-n", path, "-m", "CPU"], capture_output=True, text=True, timeout=300)
     assert bad.returncode == 1 and "no CPU path" in bad.stderr
+
+
+def test_structural_plasticity_matches_oracle(tmp_path):
+    """ProcStructuralPlasticity (device pruning + host growth, seeded stream)
+    against the oracle's restatement: same records, same final connectivity
+    and traces."""
+    def edit(text):
+        text = text.replace("prn: 1.0\n    plasticity: 0", "prn: 1.0\n    plasticity: 1")
+        sp_block = ('proc_param {\n  name: "ProcStructuralPlasticity"\n  argi { key: "period" val: 50 }\n'
+                    '  argi { key: "pruning-period" val: 100 }\n  argi { key: "t-th" val: 60 }\n'
+                    '  argi { key: "seed" val: 7 }\n  argf { key: "wp" val: 1.5 }\n  argf { key: "wn" val: -1.5 }\n}\n')
+        return text.replace('proc_param {\n  name: "ProcSpkRec"', sp_block + 'proc_param {\n  name: "ProcSpkRec"')
+
+    path, sp = write(workloads.config0(), tmp_path, edit)
+    assert [p.name for p in sp.proc_param].index("ProcStructuralPlasticity") == 4
+    s = engine.Solver(path)
+    s.run()
+    net = s.net(1, 1)
+    got = {n: net.read(n) for n in ("ii_0", "di_0", "pij_0", "eij_0", "zj2_0", "ti_0", "wij_0", ".counter_0")}
+    files = rec_files(sp)
+    s.close()
+    want_files, ref = oracle_files(sp, tmp_path)
+    for name in want_files:
+        assert files[name] == want_files[name], name
+    for n, a in got.items():
+        b = ref["net"].read(n)
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), n
+    # pruning and regrowth both happened
+    assert (got["ii_0"] < 0).any() or (got["ii_0"] != np.tile(np.arange(100), 10)).any()
