@@ -49,7 +49,8 @@ class NetDesc(ctypes.Structure):
     _fields_ = [("n_pops", ctypes.c_int32), ("pops", ctypes.POINTER(PopDesc)), ("n_projs", ctypes.c_int32),
                 ("projs", ctypes.POINTER(ProjDesc)), ("dt", ctypes.c_float), ("seed", ctypes.c_uint32),
                 ("poisson_noise_hz", ctypes.c_float), ("exchange_spikes", ctypes.c_int32),
-                ("device", ctypes.c_int32), ("max_ticks_per_run", ctypes.c_int32), ("tick_threads", ctypes.c_int32)]
+                ("device", ctypes.c_int32), ("max_ticks_per_run", ctypes.c_int32), ("tick_threads", ctypes.c_int32),
+                ("fp64_tables", ctypes.c_int32)]
 
 
 _lib = None
@@ -110,14 +111,14 @@ class Net:
     """One network on one GPU, driven through the C ABI."""
 
     def __init__(self, pops, projs, dt, seed=0, poisson_hz=0.0, exchange=True, device=0, max_ticks=1024,
-                 tick_threads=0):
+                 tick_threads=0, fp64_tables=0):
         self._lib = load()
         self._h = ctypes.c_void_p()
         self.n_pops, self.n_projs = len(pops), len(projs)
         self._pops = (PopDesc * max(1, len(pops)))(*[PopDesc(**p) for p in pops])
         self._projs = (ProjDesc * max(1, len(projs)))(*[ProjDesc(**p) for p in projs])
         desc = NetDesc(len(pops), self._pops, len(projs), self._projs, dt, seed, poisson_hz, 1 if exchange else 0,
-                       device, max_ticks, tick_threads)
+                       device, max_ticks, tick_threads, fp64_tables)
         rc = self._lib.bcpnn_net_create(ctypes.byref(desc), ctypes.byref(self._h))
         if rc != 0:
             msg = self._lib.bcpnn_last_error(self._h).decode() if self._h else ""

@@ -167,7 +167,10 @@ int fill_slot(bcpnn_net* net, int p, int s, float prn, int need) {
     CU(cudaMalloc((void**)&T.ptr, (size_t)cap * 4 * sizeof(float4)));
     T.cap = cap;
   }
-  build_table_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.cap, kp, D.ke, D.kzi, D.kzj);
+  if (D.fp64)
+    build_table_fp64_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.cap, kp, D.ke, D.kzi, D.kzj);
+  else
+    build_table_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.cap, kp, D.ke, D.kzi, D.kzj);
   CU(cudaGetLastError());
   net->launches++;
   T.kp_bits = bx_fbits(kp);
@@ -596,6 +599,7 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     D.bgain = d.bgain;
     D.wgain = d.wgain;
     D.kepsc = d.tauepsc > 0.0f ? dt / d.tauepsc : D.kzi;
+    D.fp64 = desc->fp64_tables ? 1 : 0;
     size_t R = (size_t)J.H * J.C, HM = (size_t)J.H * J.M, cells = R * J.M;
     if ((rc = dalloc(net, &D.ii, R))) return bail(rc);
     if ((rc = dalloc(net, &D.di, R))) return bail(rc);

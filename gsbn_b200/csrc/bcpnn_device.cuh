@@ -77,6 +77,7 @@ struct PopDev {
 
 struct ProjDev {
   int src, dest, H, M, C, Ns, proj_in_pop;
+  int fp64;                             /* decay tables: 0 gsbn's closed form, 1 FP64-built propagators */
   float taupdt, ke, kzi, kzj, kepsc, kfti, kftj, eps, eps2, wgain, bgain;
   int* ii; int* di; int* qi;            /* [H*C] */
   float* pi; float* ei; float* zi;      /* [H*C] */
@@ -134,10 +135,12 @@ struct TabRef {
 /* constants of the closed form for one kp */
 struct Coef {
   float kp, ke, kzi, kzj, kekp, Dekp, Dpzi, Dezi, D2, D3;
+  int fp64; /* tables hold FP64-built propagator coefficients (see fp64_entry) */
 };
 
-__device__ __forceinline__ Coef make_coef(float kp, float ke, float kzi, float kzj) {
+__device__ __forceinline__ Coef make_coef(float kp, float ke, float kzi, float kzj, int fp64 = 0) {
   Coef k;
+  k.fp64 = fp64;
   k.kp = kp; k.ke = ke; k.kzi = kzi; k.kzj = kzj;
   k.kekp = ke * kp;
   k.Dekp = ke - kp;
@@ -182,6 +185,77 @@ __device__ __forceinline__ void table_entry(float kp, float ke, float kzi, float
   o3 = make_float4(Ee, Eezi, Ee * Dezi, Emzi);
 }
 
+/* FP64-built propagator of the trace chain over d ticks.  Between events
+   the traces obey linear ODEs (rates per tick):
+     cells: p' = kp (e - p), e' = ke (s - e), s' = -(kzi + kzj) s, s = zi2 zj2
+     rows:  p' = kp (e - p), e' = ke (z - e), z' = -kzi z
+   so x(d) = expm(d A) x(0) with A upper bidiagonal.  gsbn's closed form
+   (Proj.cpp:435-443) is this solution written with divided differences
+   1/(ke - kzi), 1/((kzi - ke) + kzj), ..., which cancel catastrophically when
+   time constants nearly coincide.  expm(d A) by scaling and squaring with a
+   Taylor series (Moler & Van Loan, "Nineteen dubious ways...", 1978/2003,
+   method 3) uses products and sums only and does not care how close the
+   rates are; it runs in double and is rounded once to float.
+   entry[0] = (P<-p, P<-e, P<-s, E<-e)   entry[1] = (E<-s, e^{-kzi d}, e^{-kzj d}, 0)
+   entry[2] = (P<-p, P<-e, P<-z, E<-e)   entry[3] = (E<-z, e^{-kzi d}, 0, 0)       */
+__device__ __forceinline__ void expm3_upper(double a00, double a01, double a11, double a12, double a22, double d,
+                                            double E[6]) {
+  /* M = d A = [[m00, m01, 0], [0, m11, m12], [0, 0, m22]]; E = (E00, E01, E02, E11, E12, E22) */
+  double m00 = a00 * d, m01 = a01 * d, m11 = a11 * d, m12 = a12 * d, m22 = a22 * d;
+  double nrm = fmax(fabs(m00) + 0.0, fmax(fabs(m01) + fabs(m11), fabs(m12) + fabs(m22)));
+  int sq = 0;
+  while (nrm > 0.125) {
+    nrm *= 0.5;
+    sq++;
+  }
+  const double sc = ldexp(1.0, -sq);
+  m00 *= sc; m01 *= sc; m11 *= sc; m12 *= sc; m22 *= sc;
+  /* Taylor sum of exp(M): term T_k = T_{k-1} M / k, upper triangular */
+  double t00 = 1, t01 = 0, t02 = 0, t11 = 1, t12 = 0, t22 = 1;
+  double e00 = 1, e01 = 0, e02 = 0, e11 = 1, e12 = 0, e22 = 1;
+  for (int k = 1; k <= 16; k++) {
+    const double inv = 1.0 / (double)k;
+    const double n00 = t00 * m00 * inv;
+    const double n01 = (t00 * m01 + t01 * m11) * inv;
+    const double n02 = (t01 * m12 + t02 * m22) * inv;
+    const double n11 = t11 * m11 * inv;
+    const double n12 = (t11 * m12 + t12 * m22) * inv;
+    const double n22 = t22 * m22 * inv;
+    t00 = n00; t01 = n01; t02 = n02; t11 = n11; t12 = n12; t22 = n22;
+    e00 += t00; e01 += t01; e02 += t02; e11 += t11; e12 += t12; e22 += t22;
+  }
+  for (int i = 0; i < sq; i++) {
+    const double s00 = e00 * e00, s01 = e00 * e01 + e01 * e11, s02 = e00 * e02 + e01 * e12 + e02 * e22;
+    const double s11 = e11 * e11, s12 = e11 * e12 + e12 * e22, s22 = e22 * e22;
+    e00 = s00; e01 = s01; e02 = s02; e11 = s11; e12 = s12; e22 = s22;
+  }
+  E[0] = e00; E[1] = e01; E[2] = e02; E[3] = e11; E[4] = e12; E[5] = e22;
+}
+
+__device__ __forceinline__ void fp64_entry(float kp, float ke, float kzi, float kzj, int d, float4& o0, float4& o1,
+                                           float4& o2, float4& o3) {
+  const double p = kp, e = ke, zi = kzi, zj = kzj;
+  double C[6], R[6], J[6];
+  expm3_upper(-p, p, -e, e, -(zi + zj), (double)d, C);
+  expm3_upper(-p, p, -e, e, -zi, (double)d, R);
+  expm3_upper(0.0, 0.0, 0.0, 0.0, -zj, (double)d, J); /* J[5] = e^{-kzj d} */
+  o0 = make_float4((float)C[0], (float)C[1], (float)C[2], (float)C[3]);
+  o1 = make_float4((float)C[4], (float)R[5], (float)J[5], 0.0f);
+  o2 = make_float4((float)R[0], (float)R[1], (float)R[2], (float)R[3]);
+  o3 = make_float4((float)R[4], (float)R[5], 0.0f, 0.0f);
+}
+
+__global__ void build_table_fp64_kernel(float4* tab, int len, float kp, float ke, float kzi, float kzj) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < len; d += gridDim.x * blockDim.x) {
+    float4 t0, t1, t2, t3;
+    fp64_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+    tab[(size_t)d * 4 + 0] = t0;
+    tab[(size_t)d * 4 + 1] = t1;
+    tab[(size_t)d * 4 + 2] = t2;
+    tab[(size_t)d * 4 + 3] = t3;
+  }
+}
+
 /* the cell part (entry[0], entry[1]) of the decay factors for d elapsed
    ticks, computed with the same float expressions as table_entry */
 __device__ __forceinline__ void cell_factors(float kp, float ke, float kzi, float kzj, int d, float4& A, float4& B) {
@@ -206,9 +280,12 @@ struct F4x2 {
   float4 a, b;
 };
 
-__device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float kzj, int d, int part) {
+__device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float kzj, int d, int part, int fp64) {
   float4 t0, t1, t2, t3;
-  table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+  if (fp64)
+    fp64_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+  else
+    table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
   F4x2 r;
   if (part == 0) {
     r.a = t0;
@@ -221,8 +298,8 @@ __device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float 
 }
 
 __device__ __forceinline__ void table_pair(float kp, float ke, float kzi, float kzj, int d, int part, float4& A,
-                                           float4& B) {
-  F4x2 r = table_pair_nl(kp, ke, kzi, kzj, d, part);
+                                           float4& B, int fp64 = 0) {
+  F4x2 r = table_pair_nl(kp, ke, kzi, kzj, d, part, fp64);
   A = r.a;
   B = r.b;
 }
@@ -233,7 +310,7 @@ __device__ __forceinline__ void load_entry(const float4* tab, int len, const Coe
     A = tab[(size_t)d * 4 + part];
     B = tab[(size_t)d * 4 + part + 1];
   } else {
-    table_pair(k.kp, k.ke, k.kzi, k.kzj, d, part, A, B);
+    table_pair(k.kp, k.ke, k.kzi, k.kzj, d, part, A, B, k.fp64);
   }
 }
 
@@ -241,6 +318,16 @@ __device__ __forceinline__ void load_entry(const float4* tab, int len, const Coe
    :519-527 (column), :269-277 (all).  A = entry[0], B = entry[1]. */
 __device__ __forceinline__ void cell_decay(float& pij, float& eij, float& zi2, float& zj2, const Coef& k,
                                            float4 A, float4 B) {
+  if (k.fp64) { /* FP64-built propagator (fp64_entry) */
+    const float s = zi2 * zj2;
+    const float pn = (A.x * pij + A.y * eij) + A.z * s;
+    const float en = A.w * eij + B.x * s;
+    pij = pn;
+    eij = en;
+    zi2 = zi2 * B.y;
+    zj2 = zj2 * B.z;
+    return;
+  }
   float U = (((eij * k.kp) * k.kzi - (eij * k.ke) * k.kp) + (eij * k.kp) * k.kzj) + (k.kekp * zi2) * zj2;
   float V = (k.kekp * zi2) * zj2;
   float pn = (pij + (U / k.Dekp - V / k.D2) / k.D3) / A.x - ((A.y * U) / k.Dekp - (V * A.z) / k.D2) / A.w;
@@ -255,6 +342,14 @@ __device__ __forceinline__ void cell_decay(float& pij, float& eij, float& zi2, f
 /* Closed-form decay of the row traces, Proj.cpp:409-415 (row), :241-247
    (all).  A = entry[2], B = entry[3]. */
 __device__ __forceinline__ void row_decay(float& pi, float& ei, float& zi, const Coef& k, float4 A, float4 B) {
+  if (k.fp64) {
+    const float pn = (A.x * pi + A.y * ei) + A.z * zi;
+    const float en = A.w * ei + B.x * zi;
+    pi = pn;
+    ei = en;
+    zi = zi * B.y;
+    return;
+  }
   float X = ((ei * k.kp) * k.kzi - (ei * k.ke) * k.kp) + k.kekp * zi;
   float Y = k.kekp * zi;
   float pn = (pi - (X / k.Dekp + Y / k.Dpzi) / k.Dezi) / A.x + ((A.y * X) / k.Dekp + (Y * A.z) / k.Dpzi) / A.w;
@@ -284,7 +379,7 @@ __global__ void all_rows_kernel(const NetDev* __restrict__ net, const RunParams*
   const ProjDev& J = net->projs[p];
   int simstep = rp->simstep0 - 1;
   float kp = J.taupdt * rp->old_prn;
-  Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+  Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, J.fp64);
   const float4* tab = rp->tabs[p].tab_old;
   int len = rp->tabs[p].old_len;
   int R = J.H * J.C;
@@ -309,7 +404,7 @@ __global__ void all_cells_kernel(const NetDev* __restrict__ net, const RunParams
   const ProjDev& J = net->projs[p];
   int simstep = rp->simstep0 - 1;
   float kp = J.taupdt * rp->old_prn;
-  Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+  Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, J.fp64);
   const float4* tab = rp->tabs[p].tab_old;
   int len = rp->tabs[p].old_len;
   size_t ncell = (size_t)J.H * J.C * J.M;

@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         const int C = J.C;
         QView V = qview(sm, L, q, M, C);
         const float kp = J.taupdt * prn;
-        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, J.fp64);
         const float4* tab = rp->tabs[p].tab;
         const int tlen = rp->tabs[p].len;
         const size_t eoff = (size_t)J.proj_in_pop * n;
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           const int C = J.C;
           QView V = qview(sm, L, q, M, C);
           const float kp = J.taupdt * prn;
-          const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+          const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, J.fp64);
           const float4* tab = rp->tabs[p].tab;
           const int tlen = rp->tabs[p].len;
           const uint32_t* cbits = V.bits + cur * V.W;
@@ -749,7 +749,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                 c4.w += J.kftj;
               } else {
                 float4 A = tA[u], B = tB[u];
-                if (pdt >= tlen) cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+                if (pdt >= tlen) {
+                  if (k.fp64)
+                    table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, B, 1);
+                  else
+                    cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+                }
                 cell_decay(c4.x, c4.y, c4.z, c4.w, k, A, B);
                 c4.w = c4.w + J.kftj;
               }

@@ -89,6 +89,12 @@ typedef struct bcpnn_net_desc {
   int32_t max_ticks_per_run; /* capacity of the per-run spike log             */
   int32_t tick_threads;      /* CTA size of the tick kernel: 512 (0 = default)
                                 or 256 (two CTAs per SM, HCUs of <= 256 MCUs) */
+  int32_t fp64_tables;       /* 0: gsbn's closed-form trace decay in float (bit
+                                parity with the reference CPU path); 1: per
+                                elapsed-tick propagators expm(d A) built in FP64
+                                on the GPU and rounded once to float -- robust
+                                when time constants nearly coincide, not
+                                bit-identical to the reference */
 } bcpnn_net_desc;
 
 /* Build a network on the device with gsbn's initial values.  Limits: at most
