@@ -89,6 +89,7 @@ struct bcpnn_net {
   bool persistent = false;  /* one cooperative launch per run (else one launch per tick) */
   size_t tick_smem = 0;     /* dynamic shared memory of tick_kernel */
   int threads = 512;        /* CTA size of the tick kernel (512 or 256) */
+  bool fp64 = false;        /* FP64-built decay tables */
   const void* tick_fn = nullptr; /* the tick kernel variant of that size */
   unsigned int* bar = nullptr; /* grid barrier arrival counter of the persistent kernel */
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -285,10 +286,14 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
     cudaLaunchCooperativeKernel(net->tick_fn, dim3(net->total_hcu), dim3(net->threads), args, smem, net->stream);
   } else {
     for (int it = 0; it < n_ticks; ++it) {
-      if (net->threads == 256)
-        t256::tick_kernel<<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+      if (net->threads == 256 && net->fp64)
+        t256::tick_kernel<1><<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+      else if (net->threads == 256)
+        t256::tick_kernel<0><<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+      else if (net->fp64)
+        t512::tick_kernel<1><<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
       else
-        t512::tick_kernel<<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+        t512::tick_kernel<0><<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
     }
   }
 }
@@ -436,7 +441,11 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   net->max_ticks = desc->max_ticks_per_run;
   net->exchange = desc->exchange_spikes != 0;
   net->threads = desc->tick_threads == 256 ? 256 : 512;
-  net->tick_fn = net->threads == 256 ? (const void*)t256::tick_kernel : (const void*)t512::tick_kernel;
+  net->fp64 = desc->fp64_tables != 0;
+  if (net->threads == 256)
+    net->tick_fn = net->fp64 ? (const void*)t256::tick_kernel<1> : (const void*)t256::tick_kernel<0>;
+  else
+    net->tick_fn = net->fp64 ? (const void*)t512::tick_kernel<1> : (const void*)t512::tick_kernel<0>;
   {
     const char* e = std::getenv("GSBN_DIRECT_LAUNCH");
     net->direct = e && e[0] == '1';
@@ -684,9 +693,9 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
      with a smaller need does not lower it under an earlier one */
   {
     static std::mutex mu;
-    static size_t raised[2][kMaxDevices] = {{0}};
+    static size_t raised[4][kMaxDevices] = {{0}};
     std::lock_guard<std::mutex> lock(mu);
-    const int dev = net->device, v = net->threads == 256 ? 1 : 0;
+    const int dev = net->device, v = (net->threads == 256 ? 1 : 0) + (net->fp64 ? 2 : 0);
     if (dev < 0 || dev >= kMaxDevices) { net->err = "device ordinal out of range"; return bail(BCPNN_ERR_INVALID); }
     if (smem > raised[v][dev]) {
       if (cudaFuncSetAttribute(net->tick_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {

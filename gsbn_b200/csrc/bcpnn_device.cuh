@@ -280,12 +280,25 @@ struct F4x2 {
   float4 a, b;
 };
 
-__device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float kzj, int d, int part, int fp64) {
+__device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float kzj, int d, int part) {
   float4 t0, t1, t2, t3;
-  if (fp64)
-    fp64_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
-  else
-    table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+  table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
+  F4x2 r;
+  if (part == 0) {
+    r.a = t0;
+    r.b = t1;
+  } else {
+    r.a = t2;
+    r.b = t3;
+  }
+  return r;
+}
+
+/* the same for FP64-built propagators; a function of its own, so that the
+   closed-form path's call carries none of its double-precision registers */
+__device__ __noinline__ F4x2 table_pair_fp64_nl(float kp, float ke, float kzi, float kzj, int d, int part) {
+  float4 t0, t1, t2, t3;
+  fp64_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
   F4x2 r;
   if (part == 0) {
     r.a = t0;
@@ -299,7 +312,7 @@ __device__ __noinline__ F4x2 table_pair_nl(float kp, float ke, float kzi, float 
 
 __device__ __forceinline__ void table_pair(float kp, float ke, float kzi, float kzj, int d, int part, float4& A,
                                            float4& B, int fp64 = 0) {
-  F4x2 r = table_pair_nl(kp, ke, kzi, kzj, d, part, fp64);
+  F4x2 r = fp64 ? table_pair_fp64_nl(kp, ke, kzi, kzj, d, part) : table_pair_nl(kp, ke, kzi, kzj, d, part);
   A = r.a;
   B = r.b;
 }

@@ -295,6 +295,10 @@ __global__ void barrier_probe_kernel(unsigned int* bar, int* err, unsigned long 
 }
 
 /* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */
+/* kF64: the trace-decay form, fixed at compile time so the default
+   instance carries no trace of the other (0: gsbn's closed form in float,
+   1: FP64-built propagators, see fp64_entry) */
+template <int kF64>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* __restrict__ net,
                                                          const RunParams* __restrict__ rp, int it0, int n_ticks,
                                                          unsigned int* bar) {
@@ -522,7 +526,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         const int C = J.C;
         QView V = qview(sm, L, q, M, C);
         const float kp = J.taupdt * prn;
-        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, J.fp64);
+        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
         const float4* tab = rp->tabs[p].tab;
         const int tlen = rp->tabs[p].len;
         const size_t eoff = (size_t)J.proj_in_pop * n;
@@ -695,7 +699,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           const int C = J.C;
           QView V = qview(sm, L, q, M, C);
           const float kp = J.taupdt * prn;
-          const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, J.fp64);
+          const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
           const float4* tab = rp->tabs[p].tab;
           const int tlen = rp->tabs[p].len;
           const uint32_t* cbits = V.bits + cur * V.W;
