@@ -91,7 +91,9 @@ struct bcpnn_net {
   int threads = 512;        /* CTA size of the tick kernel (512 or 256) */
   bool fp64 = false;        /* FP64-built decay tables */
   const void* tick_fn = nullptr; /* the tick kernel variant of that size */
-  unsigned int* bar = nullptr; /* grid barrier arrival counter of the persistent kernel */
+  unsigned int* bar = nullptr; /* persistent kernel: [0] grid barrier arrivals, [1..2] column units by
+                                  tick parity, [4 + cta] column units done for each CTA */
+  int4* col_ring = nullptr;    /* deferred column units (NetDev::col_ring) */
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   uint64_t launches = 0;
   uint64_t all_cells = 0;   /* cells swept by all-cells catch-ups */
@@ -147,6 +149,7 @@ int check_device_error(bcpnn_net* net) {
     std::string why;
     if (e & kErrIndex) why += " a slot's source MCU index is outside the source population;";
     if (e & kErrBarrier) why += " a grid barrier of the persistent tick kernel timed out;";
+    if (e & kErrColumns) why += " a wait for the grid's column updates in the persistent tick kernel timed out;";
     return fail(net, BCPNN_ERR_DEVICE, "kernel reported error word " + std::to_string(e) + ":" + why);
   }
   return BCPNN_OK;
@@ -280,7 +283,7 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
   }
   size_t smem = net->tick_smem;
   if (net->persistent) {
-    cudaMemsetAsync(net->bar, 0, sizeof(unsigned int), net->stream);
+    cudaMemsetAsync(net->bar, 0, (4 + (size_t)net->total_hcu) * sizeof(unsigned int), net->stream);
     int it0 = 0, n = n_ticks;
     void* args[] = {(void*)&net->d_net, (void*)&net->d_rp, (void*)&it0, (void*)&n, (void*)&net->bar};
     cudaLaunchCooperativeKernel(net->tick_fn, dim3(net->total_hcu), dim3(net->threads), args, smem, net->stream);
@@ -714,7 +717,30 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     const char* e = std::getenv("GSBN_PER_TICK");
     bool forced = e && e[0] == '1';
     net->persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu;
-    if ((rc = dalloc(net, &net->bar, 1))) return bail(rc);
+    if ((rc = dalloc(net, &net->bar, 4 + (size_t)net->total_hcu))) return bail(rc);
+  }
+  /* deferred columns of the persistent launch: ring halves sized for every
+     MCU of every HCU spiking in one tick (units of kColUnit slots) */
+  if (net->persistent) {
+    long long cap = 0;
+    bool fits = true;
+    for (const PopHost& P : net->pops) {
+      long long parts = 0;
+      for (int q : P.in_proj) parts += (net->projs[q].C + kColUnit - 1) / kColUnit;
+      cap += (long long)P.H * P.M * parts;
+      if (P.M > 0xffff) fits = false;
+    }
+    /* unit counters are 32-bit within a launch */
+    fits = fits && cap > 0 && cap * (long long)net->max_ticks < (1ll << 31);
+    if (fits) {
+      if ((rc = dalloc(net, &net->col_ring, 2 * (size_t)cap))) return bail(rc);
+      H.col_ring = net->col_ring;
+      H.col_cap = (int)cap;
+      if (cudaMemcpy(net->d_net, &net->h, sizeof(NetDev), cudaMemcpyHostToDevice) != cudaSuccess) {
+        net->err = "copy of network descriptor failed";
+        return bail(BCPNN_ERR_CUDA);
+      }
+    }
   }
   if (cudaStreamSynchronize(net->stream) != cudaSuccess) {
     net->err = "initialisation failed";
@@ -946,6 +972,7 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   net->rp.old_prn = old_prn;
   net->rp.lginp = net->cur_lg;
   net->rp.wmask = net->cur_wm;
+  net->rp.defer = (net->persistent && net->col_ring) ? 1 : 0;
   CU(cudaMemcpyAsync(net->d_tabs, net->tabs.data(), net->tabs.size() * sizeof(TabRef), cudaMemcpyHostToDevice,
                      net->stream));
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));

@@ -47,11 +47,13 @@ constexpr int kMaxPops = 4096;      /* populations per network (batches of netwo
 constexpr int kMaxProj = 4096;      /* projections per network                 */
 constexpr int kRowChunkCells = kBlock; /* row cells staged per chunk (one per thread) */
 constexpr int kColU = 2;            /* column cells per thread per batch         */
+constexpr int kColUnit = 256;       /* slots of one column work unit (see NetDev::col_ring) */
 constexpr int kMaxIn = 8;           /* incoming projections per population       */
 
 /* error bits of NetDev::err */
 constexpr int kErrIndex = 1;        /* ii out of the source population range   */
 constexpr int kErrBarrier = 2;      /* a grid barrier wait ran out of time      */
+constexpr int kErrColumns = 4;      /* a wait for deferred column work ran out of time */
 
 struct PopDev {
   int H, M, n, hcu_start, mcu_start, dim_proj, id;
@@ -104,6 +106,13 @@ struct NetDev {
   uint32_t* ss_log;     /* [max_ticks][n_projs] debug flags of ProcSpkRec */
   unsigned long long* counters; /* row cells, col cells, all cells */
   int* err;
+  /* Deferred column work of the persistent launch.  The column updates of the
+     MCUs that spike in tick t are done in tick t+1 by every CTA of the grid
+     instead of by the spiking HCU's CTA alone.  A unit is up to kColUnit slots
+     of one spiking column: (owner CTA, projection, first row h*C + part*kColUnit,
+     MCU | rows << 16).  Two ring halves by tick parity, col_cap units each. */
+  int4* col_ring;
+  int col_cap;
 };
 
 /* Decay table entry for one elapsed-tick count d: four float4
@@ -123,6 +132,7 @@ struct RunParams {
   const float* lginp;   /* stimulus of the run: [total MCUs] */
   const float* wmask;   /* [total HCUs] */
   const struct TabRef* tabs;  /* [n_projs] decay tables of the run */
+  int defer;      /* column updates deferred and spread over the grid (persistent launch) */
 };
 
 /* decay tables of one projection for a run */

@@ -112,6 +112,7 @@ struct TickLayout {
   int stg_row, stg_ti;           /* [kBlock] int                                           */
   int stg_tv, stg_wv;            /* [kRowChunkCells] int / float                           */
   int w_dsup, w_act, w_spkl, w_pi, w_w;
+  int w_spkp;                    /* [2][M] int: spike lists by tick parity (deferred columns) */
   int w_spk, w_skip;             /* bytes                                                  */
   int st_dsup, st_act, st_cnt;
   int st_q[kMaxIn];              /* per incoming projection (QView) */
@@ -139,6 +140,7 @@ __host__ __device__ inline void tick_layout(int M, int n_in, const int* C, TickL
   L.w_spkl = o; o += M;
   L.w_pi = o; o += kBlock;
   L.w_w = o; o += kRowChunkCells;
+  L.w_spkp = o; o += 2 * M;
   L.w_spk = o; o += (M + 3) / 4;
   L.w_skip = o; o += (kRowChunkCells + 3) / 4;
   L.st_dsup = o; o += M;
@@ -222,8 +224,8 @@ __device__ __forceinline__ void stage_rows(const ProjDev& J, const int* list, in
     int rr = c / M;
     int j = c - rr * M;
     size_t index = (size_t)list[base + rr] * M + j;
-    int tv = J.tij[index];
-    float4 c4 = J.cell[index];
+    int tv = __ldcg(J.tij + index); /* cells and tij: other CTAs write them (deferred columns) */
+    float4 c4 = __ldcg(J.cell + index);
     float wv = J.wij[index];
     int pdt = simstep - tv;
     float4 A = make_float4(0, 0, 0, 0), B = A;
@@ -294,6 +296,86 @@ __global__ void barrier_probe_kernel(unsigned int* bar, int* err, unsigned long 
   grid_sync(bar, gridDim.x + 1u, err, &s_ok, limit_ns);
 }
 
+/* Deferred column updates, Proj.cpp:481-536, of the MCUs that spiked in the
+   tick at `simstep`.  Units [beg, end) of the ring half are split evenly over
+   the CTAs of the grid; the calling group (gsize kGroup, named barrier bar_id)
+   does this CTA's share, then signals each unit's owner CTA with a release add
+   on col_done[owner].  A unit's slots were published by their owner after its
+   row updates of that tick, so every cell sees the row update first, as in
+   gsbn (rows, then columns). */
+template <int kF64>
+__device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, const RunParams* __restrict__ rp,
+                                             const int4* __restrict__ ring, unsigned beg, unsigned end, int simstep,
+                                             unsigned int* col_done, int gtid, int bar_id) {
+  const unsigned n = end - beg, G = gridDim.x;
+  const unsigned per = (n + G - 1) / G;
+  const unsigned lo = min(n, blockIdx.x * per), hi = min(n, lo + per);
+  const unsigned cap = (unsigned)net->col_cap;
+  const float prn = rp->prn;
+  const int ncell = (int)(hi - lo) * kColUnit;
+  for (int b0 = 0; b0 < ncell; b0 += kColU * kGroup) {
+    size_t index[kColU];
+    int tv[kColU], pj[kColU];
+    float4 cv[kColU];
+    bool ok[kColU];
+#pragma unroll
+    for (int u = 0; u < kColU; ++u) {
+      const int k = b0 + u * kGroup + gtid;
+      ok[u] = false;
+      if (k < ncell) {
+        const int4 d = __ldcg(ring + (beg + lo + (unsigned)(k / kColUnit)) % cap);
+        const int r = k % kColUnit;
+        if (r < (d.w >> 16)) {
+          const ProjDev& J = net->projs[d.y];
+          const int row = d.z + r;
+          index[u] = (size_t)row * J.M + (d.w & 0xffff);
+          ok[u] = J.ii[row] >= 0;
+          pj[u] = d.y;
+          tv[u] = __ldcg(J.tij + index[u]);
+          cv[u] = __ldcg(J.cell + index[u]);
+        }
+      }
+    }
+    float4 tA[kColU], tB[kColU];
+#pragma unroll
+    for (int u = 0; u < kColU; ++u) {
+      if (!ok[u]) continue;
+      const TabRef& T = rp->tabs[pj[u]];
+      const int pdt = simstep - tv[u];
+      if (pdt > 0 && pdt < T.len) {
+        tA[u] = T.tab[(size_t)pdt * 4 + 0];
+        tB[u] = T.tab[(size_t)pdt * 4 + 1];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kColU; ++u) {
+      if (!ok[u]) continue;
+      const ProjDev& J = net->projs[pj[u]];
+      const int pdt = simstep - tv[u];
+      float4 c4 = cv[u];
+      if (pdt <= 0) {
+        c4.w += J.kftj;
+      } else {
+        const Coef k = make_coef(J.taupdt * prn, J.ke, J.kzi, J.kzj, kF64);
+        float4 A = tA[u], B = tB[u];
+        if (pdt >= rp->tabs[pj[u]].len) {
+          if (kF64)
+            table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, B, 1);
+          else
+            cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+        }
+        cell_decay(c4.x, c4.y, c4.z, c4.w, k, A, B);
+        c4.w = c4.w + J.kftj;
+      }
+      J.cell[index[u]] = c4;
+      J.tij[index[u]] = simstep;
+    }
+  }
+  group_sync(bar_id);
+  if (gtid == 0)
+    for (unsigned u = lo; u < hi; ++u) atomic_add_release(&col_done[__ldcg(ring + (beg + u) % cap).x], 1u);
+}
+
 /* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */
 /* kF64: the trace-decay form, fixed at compile time so the default
    instance carries no trace of the other (0: gsbn's closed form in float,
@@ -311,6 +393,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   __shared__ int s_flag9;
   __shared__ int s_nspk;
   __shared__ int s_ok;
+  __shared__ unsigned int s_hbeg, s_hend, s_upos, s_exp_total, s_last_end[2];
+  __shared__ int s_nspkp[2];
 
   const int P = net->cta_pop[blockIdx.x];
   const int h = net->cta_hcu[blockIdx.x];
@@ -321,6 +405,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   const bool groupA = tid < kGroup;
   const int gtid = groupA ? tid : tid - kGroup;
   const float prn = rp->prn;
+  /* deferred columns (persistent launch): bar[1..2] unit counters by tick
+     parity, bar[4 + cta] units done for each CTA */
+  const int defer = rp->defer;
+  unsigned int* const col_tail = bar + 1;
+  unsigned int* const col_done = bar + 4;
 
   int Cq[kMaxIn];
 #pragma unroll
@@ -334,6 +423,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   float* w_pi = sm + L.w_pi;
   float* w_w = sm + L.w_w;
   int8_t* w_spk = (int8_t*)(sm + L.w_spk);
+  int* w_spkp = (int*)(sm + L.w_spkp);
   int8_t* w_skip = (int8_t*)(sm + L.w_skip);
   float* st_dsup = sm + L.st_dsup;
   float* st_act = sm + L.st_act;
@@ -372,6 +462,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       for (int w = tid; w < V.W; w += kBlock) V.bits[cur0 * V.W + w] = 0u;
       if (tid == 0) V.nlist[cur0] = J.list_cnt[h];
     }
+    if (tid == 0) {
+      s_exp_total = 0;
+      s_last_end[0] = s_last_end[1] = 0;
+      s_nspkp[0] = s_nspkp[1] = 0;
+    }
   }
   __syncthreads();
   for (int q = 0; q < n_in; ++q) {
@@ -403,6 +498,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
 
     if (groupA) {
       /* ================= group A: population, j-traces, rows ============= */
+      /* column units this CTA published up to the previous tick (group B adds
+         this tick's only after the spike hand-over below) */
+      const unsigned int exp_done = s_exp_total;
       /* population update, Pop.cpp:229-323 */
       const float* lginp = rp->lginp + pop.mcu_start;
       const float* wmask = rp->wmask + pop.hcu_start;
@@ -551,6 +649,49 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           if (h == 0) pop.bj[cur][eoff] = V.bj[0];
         }
         group_sync(kBarA);
+        if (defer && q == 0 && it > it0) {
+          /* the previous tick's columns of this HCU, done by the grid, must be
+             in place before its rows; then refresh the staged cells they hit */
+          if (gtid == 0) {
+            const unsigned long long t0 = globaltimer_ns();
+            while (load_acquire(col_done + blockIdx.x) < exp_done) {
+              if (*(volatile int*)net->err) break;
+              if (globaltimer_ns() - t0 > kBarrierNs) {
+                atomicOr(net->err, kErrColumns);
+                break;
+              }
+              __nanosleep(20);
+            }
+          }
+          group_sync(kBarA);
+          const int np = s_nspkp[prev];
+          const int nr0 = V.nlist[cur] < row_chunk_rows(M) ? V.nlist[cur] : row_chunk_rows(M);
+          if (np > 0 && nr0 > 0) {
+            float4* fcv = (float4*)(sm + L.stg_cv);
+            float4* fcA = (float4*)(sm + L.stg_cA);
+            float4* fcB = (float4*)(sm + L.stg_cB);
+            int* ftv = (int*)(sm + L.stg_tv);
+            const int* frow = (const int*)(sm + L.stg_row);
+            for (int c = gtid; c < nr0 * np; c += kGroup) {
+              const int rr = c / np;
+              const int j = w_spkp[prev * M + (c - rr * np)];
+              const size_t index = (size_t)frow[rr] * M + j;
+              const int tv = __ldcg(J.tij + index);
+              const float4 c4 = __ldcg(J.cell + index);
+              const int pdt = simstep - tv;
+              float4 A = make_float4(0, 0, 0, 0), B = A;
+              if (pdt > 0 && pdt < tlen) {
+                A = tab[(size_t)pdt * 4 + 0];
+                B = tab[(size_t)pdt * 4 + 1];
+              }
+              ftv[rr * M + j] = tv;
+              fcv[rr * M + j] = c4;
+              fcA[rr * M + j] = A;
+              fcB[rr * M + j] = B;
+            }
+            group_sync(kBarA);
+          }
+        }
 
         /* row updates of this HCU's active rows, ascending, Proj.cpp:365-479 */
         const int nrow = V.nlist[cur];
@@ -644,9 +785,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         }
       }
       /* rows done: group B may now update column cells of active rows */
-      asm volatile("bar.arrive %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
+      if (!defer) asm volatile("bar.arrive %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
     } else {
       /* ================= group B: delay queue, columns =================== */
+      if (defer) {
+        /* the grid's column units of the previous tick, this CTA's share */
+        if (gtid == 0) {
+          const unsigned int e = __ldcg(col_tail + prev);
+          s_hbeg = s_last_end[prev];
+          s_hend = e;
+          s_last_end[prev] = e;
+        }
+        group_sync(kBarB);
+        help_columns<kF64>(net, rp, net->col_ring + (size_t)prev * net->col_cap, s_hbeg, s_hend, simstep - 1, col_done,
+                           gtid, kBarB);
+      }
       for (int q = 0; q < n_in; ++q) {
         const ProjDev& J = net->projs[pop.in_proj[q]];
         const int C = J.C;
@@ -686,6 +839,42 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       /* wait for group A's spike list */
       asm volatile("bar.sync %0, %1;" ::"r"(kBarSpikes), "r"(kBlock) : "memory");
       const int nspk = s_nspk;
+      if (defer) {
+        /* publish this tick's column units; the grid does them next tick */
+        for (int i = gtid; i < nspk; i += kGroup) w_spkp[cur * M + i] = w_spkl[i];
+        int parts[kMaxIn];
+        int nunits = 0;
+#pragma unroll
+        for (int q = 0; q < kMaxIn; ++q) {
+          parts[q] = q < n_in ? (Cq[q] + kColUnit - 1) / kColUnit : 0;
+          nunits += nspk * parts[q];
+        }
+        if (gtid == 0) {
+          s_nspkp[cur] = nspk;
+          if (nunits > 0) {
+            s_upos = atomicAdd(col_tail + cur, (unsigned int)nunits);
+            s_exp_total += (unsigned int)nunits;
+            for (int q = 0; q < n_in; ++q) atomicAdd(&net->counters[1], (unsigned long long)nspk * Cq[q]);
+          }
+        }
+        group_sync(kBarB);
+        if (nunits > 0) {
+          const unsigned int pos = s_upos, cap = (unsigned int)net->col_cap;
+          int4* ring = net->col_ring + (size_t)cur * net->col_cap;
+          for (int u = gtid; u < nunits; u += kGroup) {
+            int q = 0, uu = u;
+            while (uu >= nspk * parts[q]) {
+              uu -= nspk * parts[q];
+              ++q;
+            }
+            const int i = uu / parts[q], part = uu - i * parts[q];
+            const int C = Cq[q];
+            const int rows = min(kColUnit, C - part * kColUnit);
+            ring[(pos + (unsigned int)u) % cap] =
+                make_int4((int)blockIdx.x, pop.in_proj[q], h * C + part * kColUnit, w_spkl[i] | (rows << 16));
+          }
+        }
+      } else
       /* column updates of this HCU's spiking MCUs, Proj.cpp:481-536.  Pass
          0: slots whose row is not active this tick; pass 1, after group A's
          row updates: the cells of active rows.  One code site for both, loads
@@ -779,6 +968,22 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       QView V = qview(sm, L, 0, M, J.C);
       int nr = V.nlist[nxt] < row_chunk_rows(M) ? V.nlist[nxt] : row_chunk_rows(M);
       stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, rp->tabs[p0].tab, rp->tabs[p0].len, sm, L, tid, kBlock);
+    }
+  }
+
+  /* ---- the last tick's deferred columns -------------------------------- */
+  if (defer) {
+    if (!grid_sync(bar, (unsigned int)n_ticks * gridDim.x, net->err, &s_ok)) return;
+    if (!groupA) {
+      const int lastp = (rp->k0 + it0 + n_ticks - 1) & 1;
+      if (gtid == 0) {
+        const unsigned int e = __ldcg(col_tail + lastp);
+        s_hbeg = s_last_end[lastp];
+        s_hend = e;
+      }
+      group_sync(kBarB);
+      help_columns<kF64>(net, rp, net->col_ring + (size_t)lastp * net->col_cap, s_hbeg, s_hend,
+                         rp->simstep0 + it0 + n_ticks - 1, col_done, gtid, kBarB);
     }
   }
 
