@@ -21,7 +21,7 @@ EXPORTS = (
     "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
     "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_ss_flags",
     "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_read_state_noalloc", "bcpnn_counters", "bcpnn_kernel_launches",
-    "bcpnn_selftest_barrier_timeout", "bcpnn_set_pop_rng", "bcpnn_prune", "bcpnn_last_error",
+    "bcpnn_selftest_barrier_timeout", "bcpnn_selftest_division", "bcpnn_set_pop_rng", "bcpnn_prune", "bcpnn_last_error",
     "bcpnn_status_string",
 )
 
@@ -90,6 +90,8 @@ def load():
         "bcpnn_counters": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_kernel_launches": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_selftest_barrier_timeout": (ctypes.c_int, [vp, ctypes.c_int64]),
+        "bcpnn_selftest_division": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                                   ctypes.POINTER(ctypes.c_uint64)]),
         "bcpnn_set_pop_rng": (ctypes.c_int, [vp, i32, ctypes.c_uint32, ctypes.c_uint32]),
         "bcpnn_prune": (ctypes.c_int, [vp, i32, i32, ctypes.c_float, ctypes.c_float, vp, sz, P(i32)]),
         "bcpnn_last_error": (ctypes.c_char_p, [vp]),
@@ -248,6 +250,13 @@ class Net:
 
     def set_pop_rng(self, pop, seed, key_pop):
         self._check(self._lib.bcpnn_set_pop_rng(self._h, pop, seed, key_pop))
+
+    def selftest_division(self, n_pairs, seed=1):
+        """(pairs compared, quotients that differ) of the exact warp-uniform
+        division against `/` on this network's device"""
+        t, b = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        self._check(self._lib.bcpnn_selftest_division(self._h, int(n_pairs), int(seed), ctypes.byref(t), ctypes.byref(b)))
+        return t.value, b.value
 
     def selftest_barrier_timeout(self, limit_ns):
         """status of the barrier self-test (BCPNN_ERR_DEVICE = -6 expected)"""

@@ -1178,6 +1178,63 @@ int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out) {
   return BCPNN_OK;
 }
 
+/* pairs for the division self-test: a 64-bit mix of (seed, index), with one
+   draw in two forced into a hard class */
+__device__ __forceinline__ uint32_t selftest_mix(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return (uint32_t)(x ^ (x >> 31));
+}
+
+__global__ void division_check_kernel(uint64_t n, uint64_t seed, unsigned long long* tested,
+                                      unsigned long long* bad) {
+  unsigned long long t = 0, b = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t ua = selftest_mix(seed * 0x100000001b3ull + 3 * i), ub = selftest_mix(seed * 0x100000001b3ull + 3 * i + 1);
+    switch (selftest_mix(seed + 3 * i + 2) % 20) {
+      case 0: ua &= 0x807fffffu; break;                                   /* subnormal numerator  */
+      case 1: ub &= 0x807fffffu; break;                                   /* subnormal divisor    */
+      case 2: ua &= 0x80000000u; break;                                   /* zero numerator       */
+      case 3: ub = (ub & 0x80000000u) | 0x7f800000u; break;               /* infinite divisor     */
+      case 4: ua = (ua & 0x80000000u) | 0x7f800000u; break;               /* infinite numerator   */
+      case 5: ub &= 0x80000000u; break;                                   /* zero divisor         */
+      case 6: ub = (ub & 0x80ffffffu) | 0x7e000000u; break;               /* huge divisor         */
+      case 7: ua = (ua & 0x80ffffffu) | 0x7e000000u; ub = (ub & 0x80ffffffu) | 0x01000000u; break; /* overflow */
+      case 8: ub = (ub & 0x807fffffu) | (((ua >> 23) & 0xffu) + 100u > 254u ? 0x3f800000u : (((ua >> 23) & 0xffu) + 100u) << 23); break;
+      case 9: ua = (ua & 0x807fffffu) | 0x3f800000u; ub = (ub & 0x807fffffu) | 0x3f800000u; break; /* [1, 2) */
+      default: break;
+    }
+    const float a = __uint_as_float(ua), d = __uint_as_float(ub);
+    if (a != a || d != d) continue;
+    const float q0 = a / d, q1 = div_rn(a, d);
+    ++t;
+    if (__float_as_uint(q0) != __float_as_uint(q1) && !(q0 != q0 && q1 != q1)) ++b;
+  }
+  atomicAdd(tested, t);
+  atomicAdd(bad, b);
+}
+
+int bcpnn_selftest_division(bcpnn_net* net, uint64_t n_pairs, uint64_t seed, uint64_t* tested, uint64_t* mismatches) {
+  if (!net || !tested || !mismatches) return BCPNN_ERR_INVALID;
+  cudaSetDevice(net->device);
+  unsigned long long* c = nullptr;
+  CU(cudaMalloc((void**)&c, 2 * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(c, 0, 2 * sizeof(unsigned long long), net->stream);
+  if (e == cudaSuccess) {
+    division_check_kernel<<<148 * 4, 256, 0, net->stream>>>(n_pairs, seed, c, c + 1);
+    e = cudaGetLastError();
+  }
+  unsigned long long h[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, c, sizeof(h), cudaMemcpyDeviceToHost, net->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+  cudaFree(c);
+  if (e != cudaSuccess) return fail(net, BCPNN_ERR_CUDA, std::string("division self-test: ") + cudaGetErrorString(e));
+  *tested = h[0];
+  *mismatches = h[1];
+  return BCPNN_OK;
+}
+
 int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns) {
   if (!net) return BCPNN_ERR_INVALID;
   if (limit_ns < 100000 || limit_ns > 2000000000) return fail(net, BCPNN_ERR_INVALID, "bcpnn_selftest_barrier_timeout: limit outside [1e5, 2e9] ns");

@@ -337,6 +337,40 @@ __device__ __forceinline__ void load_entry(const float4* tab, int len, const Coe
   }
 }
 
+/* IEEE quotient a / b, rounded to nearest even: bit-identical to `a / b`.
+   CUDA's float division leaves its quick path for a zero numerator, an
+   infinite divisor, subnormal operands and quotients near the ends of the
+   exponent range, and a warp waits for any lane on that path; in the decay
+   closed forms most divisions meet one of these (traces that decayed to zero,
+   exp() table entries that overflowed or underflowed).  So:
+   - a zero numerator over a finite nonzero divisor, and a finite numerator
+     over an infinite divisor, give their exact signed zero by selection;
+   - a warp whose other lanes all have normal operands with exponents less
+     than 100 apart divides in float (the quick path of `/`);
+   - otherwise the warp divides in double and rounds once to float.  For
+     p-bit operands a quotient rounded to p' >= 2p + 2 bits and then to p bits
+     is the correctly rounded p-bit quotient (Figueroa, "When is double
+     rounding innocuous?", SIGNUM Newsletter 30(3), 1995); 53 >= 2*24 + 2, and
+     float operands are far from double's range limits;
+   - an infinite or NaN operand, or a zero divisor, goes through `/` itself. */
+__device__ __forceinline__ float div_rn(float a, float b) {
+  const uint32_t ua = __float_as_uint(a), ub = __float_as_uint(b);
+  const uint32_t aa = ua << 1, bb = ub << 1; /* magnitude bits */
+  const bool zsel = (aa == 0u && bb - 1u < 0xff000000u) || (bb == 0xff000000u && aa < 0xff000000u);
+  const uint32_t ea = aa >> 24, eb = bb >> 24; /* biased exponents */
+  const bool quick = (ea - 1u < 254u) && (eb - 1u < 254u) && (ea - eb + 100u < 200u);
+  const float za = zsel ? 1.0f : a, zb = zsel ? 1.0f : b;
+  float q;
+  if (__all_sync(__activemask(), zsel || quick)) {
+    q = za / zb;
+  } else if (!zsel && (ea == 255u || eb == 255u || bb == 0u)) {
+    q = a / b;
+  } else {
+    q = __double2float_rn(__ddiv_rn((double)za, (double)zb));
+  }
+  return zsel ? __uint_as_float((ua ^ ub) & 0x80000000u) : q;
+}
+
 /* Closed-form decay of one cell over pdt ticks, Proj.cpp:435-443 (row),
    :519-527 (column), :269-277 (all).  A = entry[0], B = entry[1]. */
 __device__ __forceinline__ void cell_decay(float& pij, float& eij, float& zi2, float& zj2, const Coef& k,
@@ -353,9 +387,10 @@ __device__ __forceinline__ void cell_decay(float& pij, float& eij, float& zi2, f
   }
   float U = (((eij * k.kp) * k.kzi - (eij * k.ke) * k.kp) + (eij * k.kp) * k.kzj) + (k.kekp * zi2) * zj2;
   float V = (k.kekp * zi2) * zj2;
-  float pn = (pij + (U / k.Dekp - V / k.D2) / k.D3) / A.x - ((A.y * U) / k.Dekp - (V * A.z) / k.D2) / A.w;
+  float pn = div_rn(pij + div_rn(div_rn(U, k.Dekp) - div_rn(V, k.D2), k.D3), A.x) -
+             div_rn(div_rn(A.y * U, k.Dekp) - div_rn(V * A.z, k.D2), A.w);
   float W = (k.ke * zi2) * zj2;
-  float en = (eij + W / k.D3) / B.x - W / B.y;
+  float en = div_rn(eij + div_rn(W, k.D3), B.x) - div_rn(W, B.y);
   pij = pn;
   eij = en;
   zi2 = zi2 * B.z;
@@ -375,9 +410,10 @@ __device__ __forceinline__ void row_decay(float& pi, float& ei, float& zi, const
   }
   float X = ((ei * k.kp) * k.kzi - (ei * k.ke) * k.kp) + k.kekp * zi;
   float Y = k.kekp * zi;
-  float pn = (pi - (X / k.Dekp + Y / k.Dpzi) / k.Dezi) / A.x + ((A.y * X) / k.Dekp + (Y * A.z) / k.Dpzi) / A.w;
+  float pn = div_rn(pi - div_rn(div_rn(X, k.Dekp) + div_rn(Y, k.Dpzi), k.Dezi), A.x) +
+             div_rn(div_rn(A.y * X, k.Dekp) + div_rn(Y * A.z, k.Dpzi), A.w);
   float KZ = k.ke * zi;
-  float en = (ei - KZ / k.Dezi) / B.x + (KZ * B.y) / B.z;
+  float en = div_rn(ei - div_rn(KZ, k.Dezi), B.x) + div_rn(KZ * B.y, B.z);
   pi = pn;
   ei = en;
   zi = zi * B.w;

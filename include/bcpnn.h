@@ -244,6 +244,16 @@ int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out);
    without bound. */
 int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns);
 
+/* Numerics self-test (no counterpart in the reference): the decay closed
+   forms divide with a warp-uniform exact division instead of `/` (zero and
+   infinite operands by their exact results, a double-precision quotient
+   rounded once for subnormal or extreme operands).  This runs n_pairs float
+   pairs drawn from `seed` (with biased draws of zero, infinite, subnormal and
+   extreme-exponent operands) through both on the network's device and
+   reports how many pairs were compared (NaN operands skipped) and how many
+   quotients differed in any bit (NaN results compare equal). */
+int bcpnn_selftest_division(bcpnn_net* net, uint64_t n_pairs, uint64_t seed, uint64_t* tested, uint64_t* mismatches);
+
 /* Message of the last failing call on this handle ("" if none). */
 const char* bcpnn_last_error(const bcpnn_net* net);
 
