@@ -396,9 +396,32 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   __shared__ unsigned int s_hbeg, s_hend, s_upos, s_exp_total, s_last_end[2];
   __shared__ int s_nspkp[2];
 
+  /* this CTA's population and incoming projections, their decay tables and
+     the spike buffers it feeds, copied to shared memory once per launch: every
+     tick reads them many times, in chains of dependent loads */
+  __shared__ PopDev s_pop;
+  __shared__ ProjDev s_proj[kMaxIn];
+  __shared__ TabRef s_tab[kMaxIn];
+  __shared__ int s_inp[kMaxIn];
+  __shared__ int8_t* s_siout[kMaxIn][2];
+
   const int P = net->cta_pop[blockIdx.x];
   const int h = net->cta_hcu[blockIdx.x];
-  const PopDev& pop = net->pops[P];
+  if (threadIdx.x == 0) s_pop = net->pops[P];
+  __syncthreads();
+  if (threadIdx.x < kMaxIn && threadIdx.x < s_pop.n_in) {
+    const int p = s_pop.in_proj[threadIdx.x];
+    s_inp[threadIdx.x] = p;
+    s_proj[threadIdx.x] = net->projs[p];
+    s_tab[threadIdx.x] = rp->tabs[p];
+  }
+  if (threadIdx.x < kMaxIn && threadIdx.x < s_pop.n_out) {
+    const ProjDev& O = net->projs[s_pop.out_proj[threadIdx.x]];
+    s_siout[threadIdx.x][0] = O.si[0];
+    s_siout[threadIdx.x][1] = O.si[1];
+  }
+  __syncthreads();
+  const PopDev& pop = s_pop;
   const int M = pop.M, n = pop.n;
   const int n_in = pop.n_in;
   const int tid = threadIdx.x;
@@ -413,7 +436,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
 
   int Cq[kMaxIn];
 #pragma unroll
-  for (int q = 0; q < kMaxIn; ++q) Cq[q] = q < n_in ? net->projs[pop.in_proj[q]].C : 0;
+  for (int q = 0; q < kMaxIn; ++q) Cq[q] = q < n_in ? s_proj[q].C : 0;
   TickLayout L;
   tick_layout(M, n_in, Cq, L);
 
@@ -441,7 +464,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       w_spk[j] = pop.spike[idx];
     }
     for (int q = 0; q < n_in; ++q) {
-      const ProjDev& J = net->projs[pop.in_proj[q]];
+      const ProjDev& J = s_proj[q];
       QView V = qview(sm, L, q, M, J.C);
       const size_t eoff = (size_t)J.proj_in_pop * n;
       for (int j = tid; j < M; j += kBlock) {
@@ -470,7 +493,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   }
   __syncthreads();
   for (int q = 0; q < n_in; ++q) {
-    const ProjDev& J = net->projs[pop.in_proj[q]];
+    const ProjDev& J = s_proj[q];
     QView V = qview(sm, L, q, M, J.C);
     for (int e = tid; e < V.nlist[cur0]; e += kBlock) {
       int s = V.list[cur0 * J.C + e] - h * J.C;
@@ -478,11 +501,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
     }
   }
   if (n_in > 0) {
-    const ProjDev& J = net->projs[pop.in_proj[0]];
+    const ProjDev& J = s_proj[0];
     QView V = qview(sm, L, 0, M, J.C);
     int nr = V.nlist[cur0] < row_chunk_rows(M) ? V.nlist[cur0] : row_chunk_rows(M);
-    const int p0 = pop.in_proj[0];
-    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, rp->tabs[p0].tab, rp->tabs[p0].len, sm, L, tid,
+    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, s_tab[0].tab, s_tab[0].len, sm, L, tid,
                kBlock);
   }
 
@@ -612,21 +634,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           int idx = h * M + j;
           int8_t sv = w_spk[j];
           if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
-          for (int q = 0; q < pop.n_out; ++q) net->projs[pop.out_proj[q]].si[cur][idx] = sv;
+          for (int q = 0; q < pop.n_out; ++q) {
+            int8_t* si = q < kMaxIn ? s_siout[q][cur] : net->projs[pop.out_proj[q]].si[cur];
+            si[idx] = sv;
+          }
         }
       }
       /* hand the spike list to group B */
       asm volatile("bar.arrive %0, %1;" ::"r"(kBarSpikes), "r"(kBlock) : "memory");
 
       for (int q = 0; q < n_in; ++q) {
-        const int p = pop.in_proj[q];
-        const ProjDev& J = net->projs[p];
+        const int p = s_inp[q];
+        const ProjDev& J = s_proj[q];
         const int C = J.C;
         QView V = qview(sm, L, q, M, C);
         const float kp = J.taupdt * prn;
         const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
-        const float4* tab = rp->tabs[p].tab;
-        const int tlen = rp->tabs[p].len;
+        const float4* tab = s_tab[q].tab;
+        const int tlen = s_tab[q].len;
         const size_t eoff = (size_t)J.proj_in_pop * n;
 
         /* j-traces and bias, Proj.cpp:310-363 */
@@ -713,7 +738,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
             stage_rows(J, list, base, nr, M, simstep, tab, tlen, sm, L, gtid, kGroup);
             group_sync(kBarA);
           }
-          for (int t = gtid; t < nr; t += kGroup) {
+          /* row traces (threads from the top of the group) beside the cell
+             decays (from the bottom): a cell's decay does not need its row's
+             new traces, only its weight does */
+          for (int t = kGroup - 1 - gtid; t < nr; t += kGroup) {
             int r = stg_row[t];
             if (r == 9) s_flag9 = 1;
             float4 tr = stg_rtr[t];
@@ -735,7 +763,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
               w_pi[t] = pi;
             }
           }
-          group_sync(kBarA);
           for (int c = gtid; c < nr * M; c += kGroup) {
             int rr = c / M;
             int j = c - rr * M;
@@ -754,16 +781,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
               cv.z = cv.z + J.kfti;
               J.cell[index] = cv;
               J.tij[index] = simstep;
-              float w;
-              if (kp != 0.0f) {
-                w = J.wgain * bx_logf((cv.x + J.eps2) / ((w_pi[rr] + J.eps) * (V.pj[j] + J.eps)));
-                J.wij[index] = w;
-              } else {
-                w = stg_wv[c];
-              }
-              w_w[c] = w;
+              w_w[c] = cv.x; /* the new pij, for the weight below */
               w_skip[c] = 0;
             }
+          }
+          group_sync(kBarA);
+          /* weights of the decayed cells, Proj.cpp:458-462 */
+          for (int c = gtid; c < nr * M; c += kGroup) {
+            if (w_skip[c]) continue;
+            int rr = c / M;
+            int j = c - rr * M;
+            float w;
+            if (kp != 0.0f) {
+              w = J.wgain * bx_logf((w_w[c] + J.eps2) / ((w_pi[rr] + J.eps) * (V.pj[j] + J.eps)));
+              J.wij[(size_t)stg_row[rr] * M + j] = w;
+            } else {
+              w = stg_wv[c];
+            }
+            w_w[c] = w;
           }
           group_sync(kBarA);
           for (int j = gtid; j < M; j += kGroup) {
@@ -801,7 +836,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                            gtid, kBarB);
       }
       for (int q = 0; q < n_in; ++q) {
-        const ProjDev& J = net->projs[pop.in_proj[q]];
+        const ProjDev& J = s_proj[q];
         const int C = J.C;
         QView V = qview(sm, L, q, M, C);
         /* delay queue of this HCU's slots and ordered compaction of the next
@@ -871,7 +906,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
             const int C = Cq[q];
             const int rows = min(kColUnit, C - part * kColUnit);
             ring[(pos + (unsigned int)u) % cap] =
-                make_int4((int)blockIdx.x, pop.in_proj[q], h * C + part * kColUnit, w_spkl[i] | (rows << 16));
+                make_int4((int)blockIdx.x, s_inp[q], h * C + part * kColUnit, w_spkl[i] | (rows << 16));
           }
         }
       } else
@@ -883,14 +918,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         if (pass == 1) asm volatile("bar.sync %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
         if (nspk == 0) continue;
         for (int q = 0; q < n_in; ++q) {
-          const int p = pop.in_proj[q];
-          const ProjDev& J = net->projs[p];
+          const ProjDev& J = s_proj[q];
           const int C = J.C;
           QView V = qview(sm, L, q, M, C);
           const float kp = J.taupdt * prn;
           const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
-          const float4* tab = rp->tabs[p].tab;
-          const int tlen = rp->tabs[p].len;
+          const float4* tab = s_tab[q].tab;
+          const int tlen = s_tab[q].len;
           const uint32_t* cbits = V.bits + cur * V.W;
           const int* clist = V.list + cur * C;
           const int ncol = (pass == 0) ? nspk * C : V.nlist[cur] * nspk;
@@ -963,11 +997,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
 
     /* stage the next tick's first row chunk before the barrier */
     if (it + 1 < it0 + n_ticks && n_in > 0) {
-      const int p0 = pop.in_proj[0];
-      const ProjDev& J = net->projs[p0];
+      const ProjDev& J = s_proj[0];
       QView V = qview(sm, L, 0, M, J.C);
       int nr = V.nlist[nxt] < row_chunk_rows(M) ? V.nlist[nxt] : row_chunk_rows(M);
-      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, rp->tabs[p0].tab, rp->tabs[p0].len, sm, L, tid, kBlock);
+      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, s_tab[0].tab, s_tab[0].len, sm, L, tid, kBlock);
     }
   }
 
@@ -1000,7 +1033,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       pop.spike[idx] = w_spk[j];
     }
     for (int q = 0; q < n_in; ++q) {
-      const ProjDev& J = net->projs[pop.in_proj[q]];
+      const ProjDev& J = s_proj[q];
       QView V = qview(sm, L, q, M, J.C);
       const size_t eoff = (size_t)J.proj_in_pop * n;
       for (int j = tid; j < M; j += kBlock) {
