@@ -56,6 +56,7 @@ constexpr int kMinBlocks = kBlock <= 256 ? 2 : 1;
 constexpr int kGroup = kBlock / 2;
 constexpr int kGroupWarps = kGroup / 32;
 constexpr int kBarA = 1, kBarB = 2, kBarSpikes = 3, kBarRows = 4;
+constexpr int kDQ = 4; /* delay-queue chunks of kGroup slots compacted together */
 
 __device__ __forceinline__ void group_sync(int id) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kGroup) : "memory");
@@ -385,9 +386,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                                                          const RunParams* __restrict__ rp, int it0, int n_ticks,
                                                          unsigned int* bar) {
   extern __shared__ __align__(16) float sm[];
-  __shared__ int s_warpA[kGroupWarps], s_warpB[kGroupWarps];
+  __shared__ int s_warpA[kGroupWarps];
   __shared__ float s_red[kGroupWarps];
-  __shared__ int s_totalA, s_totalB;
+  __shared__ int s_totalA;
   __shared__ float s_dsup0;
   __shared__ float s_vsum;
   __shared__ int s_flag9;
@@ -395,6 +396,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   __shared__ int s_ok;
   __shared__ unsigned int s_hbeg, s_hend, s_upos, s_exp_total, s_last_end[2];
   __shared__ int s_nspkp[2];
+  __shared__ int s_dq[kDQ * kGroupWarps];
 
   /* this CTA's population and incoming projections, their decay tables and
      the spike buffers it feeds, copied to shared memory once per launch: every
@@ -574,12 +576,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         /* serial, in MCU order (Pop.cpp:281-293) */
         float vsum = 0.0f;
         int m = 0;
-        for (; m + 4 <= M; m += 4) {
-          float a0 = w_act[m], a1 = w_act[m + 1], a2 = w_act[m + 2], a3 = w_act[m + 3];
-          vsum += a0;
-          vsum += a1;
-          vsum += a2;
-          vsum += a3;
+        if (M >= 8) {
+          float a[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) a[u] = w_act[u];
+          for (m = 8; m + 8 <= M; m += 8) {
+            float b[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) b[u] = w_act[m + u];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) vsum += a[u];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] = b[u];
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) vsum += a[u];
         }
         for (; m < M; m++) vsum += w_act[m];
         s_vsum = vsum;
@@ -844,30 +855,63 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         const int8_t* si = J.si[prev];
         int* nlist = V.list + nxt * C;
         uint32_t* nbits = V.bits + nxt * V.W;
+        /* kDQ chunks of kGroup slots at a time: their spike flags are
+           loaded together, then compacted with one shared-memory scan */
+        const int lane = gtid & 31, warp = gtid >> 5;
         int cnt = 0;
-        for (int s0 = 0; s0 < C; s0 += kGroup) {
-          int s = s0 + gtid;
-          bool act = false;
-          if (s < C) {
-            int src = V.ii[s];
-            if (src >= 0) {
-              if (src >= J.Ns) {
-                atomicOr(net->err, kErrIndex);
-              } else {
-                int qv = V.qi[s];
-                act = (qv & 0x01) != 0;
-                qv >>= 1;
-                if (__ldcg(si + src) > 0) qv |= (0x01 << (V.di[s] - 1));
-                V.qi[s] = qv;
-              }
+        for (int s0 = 0; s0 < C; s0 += kDQ * kGroup) {
+          int8_t sv[kDQ];
+#pragma unroll
+          for (int u = 0; u < kDQ; ++u) {
+            const int s = s0 + u * kGroup + gtid;
+            sv[u] = 0;
+            if (s < C) {
+              const int src = V.ii[s];
+              if (src >= 0 && src < J.Ns) sv[u] = __ldcg(si + src);
             }
           }
-          unsigned m = __ballot_sync(0xffffffffu, act);
-          if ((gtid & 31) == 0 && s < C) nbits[s >> 5] = m;
-          int tot;
-          int pos = group_prefix(act, gtid, kBarB, s_warpB, &s_totalB, &tot);
-          if (act) nlist[cnt + pos] = h * C + s;
-          cnt += tot;
+          unsigned mb[kDQ];
+#pragma unroll
+          for (int u = 0; u < kDQ; ++u) {
+            const int s = s0 + u * kGroup + gtid;
+            bool act = false;
+            if (s < C) {
+              const int src = V.ii[s];
+              if (src >= 0) {
+                if (src >= J.Ns) {
+                  atomicOr(net->err, kErrIndex);
+                } else {
+                  int qv = V.qi[s];
+                  act = (qv & 0x01) != 0;
+                  qv >>= 1;
+                  if (sv[u] > 0) qv |= (0x01 << (V.di[s] - 1));
+                  V.qi[s] = qv;
+                }
+              }
+            }
+            mb[u] = __ballot_sync(0xffffffffu, act);
+            if (lane == 0) {
+              s_dq[u * kGroupWarps + warp] = __popc(mb[u]);
+              if (s < C) nbits[s >> 5] = mb[u];
+            }
+          }
+          group_sync(kBarB);
+          /* slots in ascending order: chunk by chunk, warp by warp, lane by lane */
+          int run = 0;
+#pragma unroll
+          for (int u = 0; u < kDQ; ++u) {
+            int before = 0, tot = 0;
+            for (int w = 0; w < kGroupWarps; ++w) {
+              const int c = s_dq[u * kGroupWarps + w];
+              tot += c;
+              before += (w < warp) ? c : 0;
+            }
+            if ((mb[u] >> lane) & 1u)
+              nlist[cnt + run + before + __popc(mb[u] & ((1u << lane) - 1u))] = h * C + s0 + u * kGroup + gtid;
+            run += tot;
+          }
+          cnt += run;
+          group_sync(kBarB);
         }
         if (gtid == 0) V.nlist[nxt] = cnt;
       }
