@@ -13,9 +13,10 @@ bcpnn_reset, then one bcpnn_run per segment.  `value` is synaptic updates/s
 (row + column + all-cells cell updates, counted by the kernels) over K steps,
 timed with CUDA events on the library's stream, stimulus rows already
 resident in HBM.  `e2e` is the same metric through the C ABI with host
-buffers: per segment the stimulus is copied from pinned host memory and the
-segment's spike log is read back, and ProcCheck's recall evaluation runs on
-the host.  The network state (~0.25 GB) is larger than L2, so no flush is
+buffers: per segment the stimulus row is copied from pinned host memory, the
+segment's spike log is read back, and ProcCheck's recall counters run on the
+device with their per-HCU results read back; all of it is queued behind the
+runs, with one synchronisation per step.  The network state (~0.25 GB) is larger than L2, so no flush is
 needed between steps.
 
 --impl reference times the CPU oracle (a restatement of gsbn's
@@ -221,7 +222,10 @@ def run_ours(args, rank, world, local_rank):
     ticks_per_launch = tk_ticks / max(1, tk_launches)
     ms, cells = combine_over_ranks(ms, cells, f"cuda:{dev}")
 
-    # e2e: host buffers through the C ABI, spike logs read back, recall on host
+    # e2e: host buffers through the C ABI, every segment's spike log read back
+    # (ProcSpkRec's input) and ProcCheck's recall counted on the device.  Each
+    # segment's stimulus row, spike-log copy and recall result are queued on
+    # the library stream behind its run; one sync per step.
     pin_lg = [torch.empty(lgidx.shape[1], dtype=torch.int32, pin_memory=True).numpy() for r in runs]
     pin_wm = [torch.empty(wmask.shape[1], dtype=torch.float32, pin_memory=True).numpy() for r in runs]
     for i, r in enumerate(runs):
@@ -233,15 +237,21 @@ def run_ours(args, rank, world, local_rank):
     d2h = sum(a.nbytes for a in pin_log)
     lib = capi.load()
 
+    check = extgen.DeviceCheck(sp, lgidx, net, [(p["hcu_num"], p["mcu_num"]) for p in pops],
+                               alloc=lambda k: torch.zeros(k, dtype=torch.int32, pin_memory=True).numpy())
+    d2h += sum(a.nbytes + b.nbytes for c in check.bufs for a, b in c)
+
     def e2e_step():
         net.reset()
+        check.reset()
         for i, r in enumerate(runs):
             net._check(lib.bcpnn_set_stimulus_idx(net._h, capi._ptr(pin_lg[i]), pin_lg[i].size, eps,
                                                   capi._ptr(pin_wm[i]), pin_wm[i].size))
             net.run(r.first, r.n, r.prn, r.old_prn)
-            net._check(lib.bcpnn_get_spike_log(net._h, 0, capi._ptr(pin_log[i]), pin_log[i].size))
-        return extgen.recall(sp, lgidx, [(p["hcu_num"], p["mcu_num"]) for p in pops], runs,
-                             [[lg] for lg in pin_log])
+            net._check(lib.bcpnn_get_spike_log_async(net._h, 0, capi._ptr(pin_log[i]), pin_log[i].size))
+            check.after_run(r)
+        net.sync()
+        return check.result()
 
     recall = e2e_step()
     net.sync()

@@ -19,7 +19,8 @@ _NP = {F32: np.float32, I32: np.int32, I8: np.int8}
 EXPORTS = (
     "bcpnn_net_create", "bcpnn_net_destroy", "bcpnn_set_conn", "bcpnn_set_stimulus", "bcpnn_upload_stimuli",
     "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
-    "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_ss_flags",
+    "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_spike_log_async", "bcpnn_check_count",
+    "bcpnn_check_result_async", "bcpnn_get_ss_flags",
     "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_read_state_noalloc", "bcpnn_counters", "bcpnn_kernel_launches",
     "bcpnn_selftest_barrier_timeout", "bcpnn_selftest_division", "bcpnn_set_pop_rng", "bcpnn_prune", "bcpnn_last_error",
     "bcpnn_status_string",
@@ -82,6 +83,9 @@ def load():
         "bcpnn_sync": (ctypes.c_int, [vp]),
         "bcpnn_spike_log_words": (ctypes.c_int, [vp, i32, P(i32)]),
         "bcpnn_get_spike_log": (ctypes.c_int, [vp, i32, vp, sz]),
+        "bcpnn_get_spike_log_async": (ctypes.c_int, [vp, i32, vp, sz]),
+        "bcpnn_check_count": (ctypes.c_int, [vp, i32, i32, i32]),
+        "bcpnn_check_result_async": (ctypes.c_int, [vp, i32, vp, vp, sz]),
         "bcpnn_get_ss_flags": (ctypes.c_int, [vp, vp, sz]),
         "bcpnn_state_info": (ctypes.c_int, [vp, ctypes.c_char_p, P(i32), P(sz)]),
         "bcpnn_read_state": (ctypes.c_int, [vp, ctypes.c_char_p, vp, sz]),
@@ -206,6 +210,21 @@ class Net:
         out = np.zeros((self.last_ticks, w.value), dtype=np.uint32)
         self._check(self._lib.bcpnn_get_spike_log(self._h, pop, _ptr(out), out.size))
         return out
+
+    def spike_log_async(self, pop, out):
+        """Queue the copy of the last run's spike log of `pop` into `out`
+        (uint32 [ticks, words], page-locked for an asynchronous copy); `out`
+        is complete after the next sync()."""
+        self._check(self._lib.bcpnn_get_spike_log_async(self._h, pop, _ptr(out), out.size))
+
+    def check_count(self, pop, k0, k1):
+        """add the spikes of ticks k0..k1-1 of the last run to `pop`'s recall counters"""
+        self._check(self._lib.bcpnn_check_count(self._h, pop, int(k0), int(k1)))
+
+    def check_result_async(self, pop, idx, cnt):
+        """queue per-HCU (first most-spiking MCU or -1, its count) of `pop`
+        into int32 idx/cnt and clear the counters; complete after sync()"""
+        self._check(self._lib.bcpnn_check_result_async(self._h, pop, _ptr(idx), _ptr(cnt), idx.size))
 
     def ss_flags(self):
         out = np.zeros((self.last_ticks, self.n_projs), dtype=np.uint8)

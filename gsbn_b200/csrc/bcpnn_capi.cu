@@ -99,6 +99,9 @@ struct bcpnn_net {
   uint64_t all_cells = 0;   /* cells swept by all-cells catch-ups */
   uint64_t stamp = 0;
   float* stim_lg = nullptr; /* device stimulus tables (bcpnn_upload_stimuli) */
+  int32_t* d_lgidx = nullptr; /* one pattern-index row (bcpnn_set_stimulus_idx) */
+  std::vector<int32_t*> check_cnt; /* per population: ProcCheck counters [H*M] (bcpnn_check_count) */
+  std::vector<int32_t*> check_out; /* per population: [2][H] idx, count of the last check */
   float* stim_wm = nullptr;
   int stim_lg_rows = 0, stim_wm_rows = 0;
   const float* cur_lg = nullptr; /* stimulus of the next run */
@@ -265,6 +268,9 @@ int reset_state(bcpnn_net* net) {
     if ((rc = dzero(net, D.si[1], (size_t)J.Ns))) return rc;
     if ((rc = dzero(net, D.list_cnt, (size_t)J.H * sizeof(int)))) return rc;
   }
+  for (size_t q = 0; q < net->check_cnt.size(); ++q)
+    if (net->check_cnt[q] && (rc = dzero(net, net->check_cnt[q], (size_t)net->pops[q].H * net->pops[q].M * sizeof(int32_t))))
+      return rc;
   net->k_total = 0;
   return BCPNN_OK;
 }
@@ -842,15 +848,37 @@ static void lginp_from_idx(const bcpnn_net* net, const int32_t* lgidx_row, float
       for (int j = 0; j < P.M; ++j) out[k++] = (lgidx_row[h] == j) ? hit : miss;
 }
 
+/* lginp of one pattern-index row on the device (the same two float values
+   as lginp_from_idx), one CTA per HCU: no host buffer to stage, so with
+   page-locked rows the whole upload is queued without a wait */
+__global__ void lginp_idx_kernel(const NetDev* __restrict__ net, const int32_t* __restrict__ lgidx, float hit,
+                                 float miss, float* __restrict__ out) {
+  const PopDev& P = net->pops[net->cta_pop[blockIdx.x]];
+  const int h = net->cta_hcu[blockIdx.x];
+  const int want = lgidx[P.hcu_start + h];
+  for (int j = threadIdx.x; j < P.M; j += blockDim.x) out[P.mcu_start + h * P.M + j] = (want == j) ? hit : miss;
+}
+
 int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hcu, float eps, const float* wmask_row,
                            size_t n_wmask) {
   if (!net) return BCPNN_ERR_INVALID;
   if (!lgidx_row || !wmask_row) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_stimulus_idx: null buffer");
   if (n_hcu != (size_t)net->total_hcu || n_wmask != (size_t)net->total_hcu)
     return fail(net, BCPNN_ERR_SIZE, "bcpnn_set_stimulus_idx: sizes must be total HCUs");
-  std::vector<float> lg(net->total_mcu);
-  lginp_from_idx(net, lgidx_row, eps, lg.data());
-  return bcpnn_set_stimulus(net, lg.data(), lg.size(), wmask_row, n_wmask);
+  CU(cudaSetDevice(net->device));
+  if (!net->d_lgidx) {
+    int rc = dalloc(net, &net->d_lgidx, (size_t)net->total_hcu);
+    if (rc) return rc;
+  }
+  CU(cudaMemcpyAsync(net->d_lgidx, lgidx_row, n_hcu * sizeof(int32_t), cudaMemcpyHostToDevice, net->stream));
+  lginp_idx_kernel<<<net->total_hcu, 128, 0, net->stream>>>(net->d_net, net->d_lgidx, bx_logf(1 + eps),
+                                                            bx_logf(0 + eps), net->h.lginp);
+  CU(cudaGetLastError());
+  net->launches += 1;
+  CU(cudaMemcpyAsync(net->h.wmask, wmask_row, n_wmask * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  net->cur_lg = net->h.lginp;
+  net->cur_wm = net->h.wmask;
+  return BCPNN_OK;
 }
 
 int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
@@ -1023,6 +1051,96 @@ int bcpnn_get_spike_log(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_wor
   if (need) CU(cudaMemcpyAsync(out, net->log_buf + P.log_offset, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, net->stream));
   CU(cudaStreamSynchronize(net->stream));
   return check_device_error(net);
+}
+
+int bcpnn_get_spike_log_async(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (pop < 0 || pop >= (int)net->pops.size() || !out)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_get_spike_log_async: bad arguments");
+  const PopHost& P = net->pops[pop];
+  size_t need = (size_t)net->last_run_ticks * P.log_words;
+  if (n_words != need) return fail(net, BCPNN_ERR_SIZE, "bcpnn_get_spike_log_async: n_words != last run ticks * words");
+  CU(cudaSetDevice(net->device));
+  if (need) CU(cudaMemcpyAsync(out, net->log_buf + P.log_offset, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, net->stream));
+  return BCPNN_OK;
+}
+
+/* ProcCheck/Pop.cpp:36-44: count the spikes of ticks k0..k1-1 of a spike log */
+__global__ void check_count_kernel(const uint32_t* __restrict__ log, int words, int k0, int k1, int n,
+                                   int32_t* __restrict__ counts) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int c = 0;
+    for (int t = k0; t < k1; ++t) c += (int)((log[(size_t)t * words + (i >> 5)] >> (i & 31)) & 1u);
+    counts[i] += c;
+  }
+}
+
+/* ProcCheck/Pop.cpp:46-60: per HCU the first MCU with the largest count (-1
+   when none counted) and that count; counters cleared */
+__global__ void check_result_kernel(int32_t* __restrict__ counts, int H, int M, int32_t* __restrict__ out) {
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
+    int best = -1, most = 0;
+    for (int j = 0; j < M; ++j) {
+      const int c = counts[(size_t)h * M + j];
+      if (c > most) {
+        best = j;
+        most = c;
+      }
+      counts[(size_t)h * M + j] = 0;
+    }
+    out[h] = best;
+    out[H + h] = most;
+  }
+}
+
+static int check_buffers(bcpnn_net* net, int pop) {
+  if (net->check_cnt.empty()) {
+    net->check_cnt.assign(net->pops.size(), nullptr);
+    net->check_out.assign(net->pops.size(), nullptr);
+  }
+  if (!net->check_cnt[pop]) {
+    const PopHost& P = net->pops[pop];
+    int rc = dalloc(net, &net->check_cnt[pop], (size_t)P.H * P.M);
+    if (rc) return rc;
+    if ((rc = dalloc(net, &net->check_out[pop], 2 * (size_t)P.H))) return rc;
+    CU(cudaMemsetAsync(net->check_cnt[pop], 0, (size_t)P.H * P.M * sizeof(int32_t), net->stream));
+  }
+  return BCPNN_OK;
+}
+
+int bcpnn_check_count(bcpnn_net* net, int32_t pop, int32_t k0, int32_t k1) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (pop < 0 || pop >= (int)net->pops.size()) return fail(net, BCPNN_ERR_INVALID, "bcpnn_check_count: bad population");
+  if (k0 < 0 || k1 < k0 || k1 > net->last_run_ticks)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_check_count: ticks outside the last run");
+  CU(cudaSetDevice(net->device));
+  int rc = check_buffers(net, pop);
+  if (rc) return rc;
+  if (k1 == k0) return BCPNN_OK;
+  const PopHost& P = net->pops[pop];
+  const int n = P.H * P.M;
+  check_count_kernel<<<(n + 255) / 256, 256, 0, net->stream>>>(net->log_buf + P.log_offset, P.log_words, k0, k1, n,
+                                                               net->check_cnt[pop]);
+  CU(cudaGetLastError());
+  net->launches += 1;
+  return BCPNN_OK;
+}
+
+int bcpnn_check_result_async(bcpnn_net* net, int32_t pop, int32_t* idx, int32_t* cnt, size_t n_hcu) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (pop < 0 || pop >= (int)net->pops.size() || !idx || !cnt)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_check_result_async: bad arguments");
+  const PopHost& P = net->pops[pop];
+  if (n_hcu != (size_t)P.H) return fail(net, BCPNN_ERR_SIZE, "bcpnn_check_result_async: n_hcu != HCUs of the population");
+  CU(cudaSetDevice(net->device));
+  int rc = check_buffers(net, pop);
+  if (rc) return rc;
+  check_result_kernel<<<(P.H + 127) / 128, 128, 0, net->stream>>>(net->check_cnt[pop], P.H, P.M, net->check_out[pop]);
+  CU(cudaGetLastError());
+  net->launches += 1;
+  CU(cudaMemcpyAsync(idx, net->check_out[pop], n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaMemcpyAsync(cnt, net->check_out[pop] + P.H, n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost, net->stream));
+  return BCPNN_OK;
 }
 
 int bcpnn_get_ss_flags(bcpnn_net* net, uint8_t* out, size_t n_bytes) {

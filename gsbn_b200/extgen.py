@@ -70,29 +70,36 @@ def stim_tables(stim):
 
 def recall(sp, lgidx, pop_shapes, runs, logs, threshold=0):
     """Correct / evaluated recall patterns from per-run spike logs of every
-    population (logs[run][pop] = uint32 [ticks, words])."""
+    population (logs[run][pop] = uint32 [ticks, words]).  Tick by tick this is
+    ProcCheck's cursor walk; the ticks strictly inside a check window are
+    summed as one span per run."""
     checks = _modes(sp.gen_param, only_prn0=True, clamp=False)
     counters = [np.zeros((h, m), np.int64) for h, m in pop_shapes]
     total_hcu = sum(h for h, _ in pop_shapes)
     cursor, correct, evaluated, updated = 0, 0, 0, False
     for r, plog in zip(runs, logs):
-        bits = [np.unpackbits(l.view(np.uint8), axis=1, bitorder="little")[:, :h * m]
-                for l, (h, m) in zip(plog, pop_shapes)]
-        for k in range(r.n):
+        bits = None
+        k = 0
+        while k < r.n and cursor < len(checks):
             t = r.first + k
-            if cursor >= len(checks):
-                break
             c = checks[cursor]
             if t <= c["begin"]:
+                k += min(c["begin"] + 1 - t, r.n - k)  # ticks up to begin are skipped
                 continue
             if t < c["end"]:
+                k1 = min(c["end"] - r.first, r.n)  # ticks t .. end-1 of this run
+                if bits is None:
+                    bits = [np.unpackbits(l.view(np.uint8), axis=1, bitorder="little")[:, :h * m]
+                            for l, (h, m) in zip(plog, pop_shapes)]
                 for cnt, b, (h, m) in zip(counters, bits, pop_shapes):
-                    cnt += b[k].reshape(h, m)
+                    cnt += b[k:k1].sum(axis=0, dtype=np.int64).reshape(h, m)
                 updated = True
+                k = k1
                 continue
             if not updated:
                 while cursor < len(checks) and t >= checks[cursor]["end"]:
                     cursor += 1
+                k += 1
                 continue
             idx, num = [], []
             for cnt in counters:
@@ -109,4 +116,70 @@ def recall(sp, lgidx, pop_shapes, runs, logs, threshold=0):
             correct += int(ok)
             evaluated += 1
             cursor += 1
+            k += 1
     return correct, evaluated
+
+
+class DeviceCheck:
+    """ProcCheck's evaluation (ProcCheck.cpp:149-237) with its counters on the
+    device (bcpnn_check_count / bcpnn_check_result_async): call after_run(r)
+    right after each net.run(r), then result() after net.sync().  The tick
+    cursor is walked here exactly as recall() walks it; no spike log has to
+    reach the host.  `alloc(n)` gives an int32 host buffer of n elements
+    (page-locked, for copies that do not wait)."""
+
+    def __init__(self, sp, lgidx, net, pop_shapes, threshold=0, alloc=None):
+        self.checks = _modes(sp.gen_param, only_prn0=True, clamp=False)
+        self.lgidx, self.net, self.shapes, self.threshold = lgidx, net, pop_shapes, threshold
+        self.total_hcu = sum(h for h, _ in pop_shapes)
+        alloc = alloc or (lambda n: np.zeros(n, np.int32))
+        self.bufs = [[(alloc(h), alloc(h)) for h, _ in pop_shapes] for _ in self.checks]
+        self.reset()
+
+    def reset(self):
+        self.cursor, self.updated, self.pending = 0, False, []
+
+    def after_run(self, r):
+        k = 0
+        while k < r.n and self.cursor < len(self.checks):
+            t = r.first + k
+            c = self.checks[self.cursor]
+            if t <= c["begin"]:
+                k += min(c["begin"] + 1 - t, r.n - k)
+                continue
+            if t < c["end"]:
+                k1 = min(c["end"] - r.first, r.n)
+                for p in range(len(self.shapes)):
+                    self.net.check_count(p, k, k1)
+                self.updated = True
+                k = k1
+                continue
+            if not self.updated:
+                while self.cursor < len(self.checks) and t >= self.checks[self.cursor]["end"]:
+                    self.cursor += 1
+                k += 1
+                continue
+            for p, (idx, cnt) in enumerate(self.bufs[self.cursor]):
+                self.net.check_result_async(p, idx, cnt)
+            self.pending.append(self.cursor)
+            self.cursor += 1
+            k += 1
+
+    def details(self):
+        """[(check index, idx over all HCUs, count over all HCUs)] of the evaluated checks (after sync)"""
+        return [(c, np.concatenate([b[0] for b in self.bufs[c]]), np.concatenate([b[1] for b in self.bufs[c]]))
+                for c in self.pending]
+
+    def result(self):
+        """(correct, evaluated) after net.sync()"""
+        correct = 0
+        th = self.threshold
+        for c, idx, num in self.details():
+            exp = self.lgidx[self.checks[c]["lgexp"]][:self.total_hcu]
+            ok = True
+            for i in range(self.total_hcu):
+                if ((num[i] < th or idx[i] != exp[i]) and exp[i] >= 0) or (num[i] > th and exp[i] < 0):
+                    ok = False
+                    break
+            correct += int(ok)
+        return correct, len(self.pending)

@@ -130,7 +130,10 @@ int bcpnn_use_stimulus(bcpnn_net* net, int32_t lginp_row, int32_t wmask_row);
 /* The same from ProcExtGen's pattern-index rows (.lgidx, one MCU index per
    HCU; any other value means no input to that HCU): the library computes
    lginp = log(1+eps) on the indexed MCU and log(0+eps) elsewhere
-   (ProcExtGen.cpp:130-144) with its own float log. */
+   (ProcExtGen.cpp:130-144) with its own float log, on the device.  Both
+   rows are copied on the network's stream: a page-locked row is read when
+   the stream reaches the copy, so keep it unchanged until the next
+   bcpnn_sync; a pageable row is staged before the call returns. */
 int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hcu, float eps, const float* wmask_row,
                            size_t n_wmask);
 int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
@@ -191,6 +194,29 @@ int bcpnn_spike_log_words(const bcpnn_net* net, int32_t pop, int32_t* words);
    population (index h*M + m, as ProcSpkRec writes it, ProcSpkRec/Pop.cpp:30-52).
    Synchronises the stream. */
 int bcpnn_get_spike_log(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words);
+
+/* The same copy queued on the network's stream without waiting for it: the
+   host can queue the next segment's stimulus and run behind it, and the
+   device runs the segments back to back.  `out` must stay valid, and is only
+   complete, after the next bcpnn_sync (which also reports a device error of
+   the runs); with page-locked `out` the copy is asynchronous, with pageable
+   memory the driver may complete it before returning.  A later bcpnn_run
+   does not disturb a queued copy (stream order). */
+int bcpnn_get_spike_log_async(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words);
+
+/* ProcCheck's recall counters on the device (ProcCheck/Pop.cpp:36-44
+   update_counter, :46-60 check_result), so a recall segment's evaluation
+   needs no spike log on the host.  bcpnn_check_count adds, for every MCU of
+   population `pop`, its spikes in ticks k0 .. k1-1 of the last run (0-based
+   within the run) to the population's counters (zero at creation).
+   bcpnn_check_result_async queues, per HCU, the MCU with the most counted
+   spikes (the first on ties, -1 when none spiked) and that count into
+   idx/cnt (n_hcu = the population's HCUs) and clears the counters; like the
+   asynchronous spike log, idx/cnt are complete after the next bcpnn_sync.
+   The caller walks ProcCheck's tick cursor (which ticks count, when a
+   segment is evaluated) and compares idx/cnt with the expected pattern. */
+int bcpnn_check_count(bcpnn_net* net, int32_t pop, int32_t k0, int32_t k1);
+int bcpnn_check_result_async(bcpnn_net* net, int32_t pop, int32_t* idx, int32_t* cnt, size_t n_hcu);
 
 /* Per tick of the last run, one byte per projection: bit 0 set if row 9 was in
    .ssi_<proj>, bit 1 if MCU 9 was in .ssj_<proj> (the debug flags ProcSpkRec
