@@ -36,7 +36,8 @@ class BcpnnError(RuntimeError):
 class PopDesc(ctypes.Structure):
     _fields_ = [("hcu_num", ctypes.c_int32), ("mcu_num", ctypes.c_int32), ("taum", ctypes.c_float),
                 ("wtagain", ctypes.c_float), ("maxfq", ctypes.c_float), ("igain", ctypes.c_float),
-                ("wgain", ctypes.c_float), ("lgbias", ctypes.c_float), ("snoise", ctypes.c_float)]
+                ("wgain", ctypes.c_float), ("lgbias", ctypes.c_float), ("snoise", ctypes.c_float),
+                ("taua", ctypes.c_float), ("adgain", ctypes.c_float)]
 
 
 class ProjDesc(ctypes.Structure):
@@ -51,7 +52,8 @@ class NetDesc(ctypes.Structure):
                 ("projs", ctypes.POINTER(ProjDesc)), ("dt", ctypes.c_float), ("seed", ctypes.c_uint32),
                 ("poisson_noise_hz", ctypes.c_float), ("exchange_spikes", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("max_ticks_per_run", ctypes.c_int32), ("tick_threads", ctypes.c_int32),
-                ("fp64_tables", ctypes.c_int32)]
+                ("fp64_tables", ctypes.c_int32), ("update_variant", ctypes.c_int32),
+                ("spike_buffer_size", ctypes.c_int32)]
 
 
 _lib = None
@@ -117,14 +119,16 @@ class Net:
     """One network on one GPU, driven through the C ABI."""
 
     def __init__(self, pops, projs, dt, seed=0, poisson_hz=0.0, exchange=True, device=0, max_ticks=1024,
-                 tick_threads=0, fp64_tables=0):
+                 tick_threads=0, fp64_tables=0, variant=0, spike_buffer=1):
+        """variant 0: ProcUpdLazy; 1: ProcUpdMulti with a ring of `spike_buffer`
+        ticks (populations then need taua and adgain)"""
         self._lib = load()
         self._h = ctypes.c_void_p()
         self.n_pops, self.n_projs = len(pops), len(projs)
         self._pops = (PopDesc * max(1, len(pops)))(*[PopDesc(**p) for p in pops])
         self._projs = (ProjDesc * max(1, len(projs)))(*[ProjDesc(**p) for p in projs])
         desc = NetDesc(len(pops), self._pops, len(projs), self._projs, dt, seed, poisson_hz, 1 if exchange else 0,
-                       device, max_ticks, tick_threads, fp64_tables)
+                       device, max_ticks, tick_threads, fp64_tables, variant, spike_buffer)
         rc = self._lib.bcpnn_net_create(ctypes.byref(desc), ctypes.byref(self._h))
         if rc != 0:
             msg = self._lib.bcpnn_last_error(self._h).decode() if self._h else ""

@@ -30,6 +30,7 @@
 #include "bcpnn_tick.cuh"
 #undef BCPNN_TICK_THREADS
 #undef BCPNN_TICK_NS
+#include "bcpnn_multi.cuh"
 #include "bcpnn_numerics.h"
 
 using namespace bcpnn;
@@ -90,6 +91,8 @@ struct bcpnn_net {
   size_t tick_smem = 0;     /* dynamic shared memory of tick_kernel */
   int threads = 512;        /* CTA size of the tick kernel (512 or 256) */
   bool fp64 = false;        /* FP64-built decay tables */
+  bool multi = false;       /* ProcUpdMulti variant (bcpnn_multi.cuh), per-tick launches */
+  int ring_len = 1;         /* its spike buffer size */
   const void* tick_fn = nullptr; /* the tick kernel variant of that size */
   unsigned int* bar = nullptr; /* persistent kernel: [0] grid barrier arrivals, [1..2] column units by
                                   tick parity, [4 + cta] column units done for each CTA */
@@ -247,6 +250,8 @@ int reset_state(bcpnn_net* net) {
     if ((rc = dset(net, D.act, n, (float)(1.0 / P.M)))) return rc;                 /* Pop.cpp:60 */
     if ((rc = dzero(net, D.spike, n))) return rc;
     if ((rc = dzero(net, D.counter, n * sizeof(int)))) return rc;
+    if (D.ada && (rc = dzero(net, D.ada, n * sizeof(float)))) return rc;
+    if (D.ring && (rc = dzero(net, D.ring, n * (size_t)D.ring_len))) return rc;
   }
   for (size_t q = 0; q < net->projs.size(); ++q) {
     const ProjHost& J = net->projs[q];
@@ -280,7 +285,7 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
   for (const PopHost& P : net->pops)
     cudaMemsetAsync(net->log_buf + P.log_offset, 0, (size_t)n_ticks * P.log_words * sizeof(uint32_t), net->stream);
   cudaMemsetAsync(net->h.ss_log, 0, (size_t)n_ticks * net->h.n_projs * sizeof(uint32_t), net->stream);
-  if (with_all) {
+  if (with_all && !net->multi) {
     for (int p = 0; p < net->h.n_projs; ++p) {
       const ProjHost& J = net->projs[p];
       all_rows_kernel<<<grid_for((size_t)J.H * J.C, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
@@ -288,6 +293,25 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
     }
   }
   size_t smem = net->tick_smem;
+  if (net->multi) {
+    /* ProcUpdMulti: catch-up at a change of prn, then per tick the
+       populations and one launch per projection */
+    if (with_all)
+      for (int p = 0; p < net->h.n_projs; ++p) {
+        const ProjHost& J = net->projs[p];
+        multi::all_kernel<<<grid_for((size_t)J.H * J.C * 32, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
+      }
+    const size_t pop_smem = (size_t)(2 * net->max_m + net->max_m) * sizeof(float);
+    for (int it = 0; it < n_ticks; ++it) {
+      multi::pop_kernel<<<net->total_hcu, multi::kPopThreads, pop_smem, net->stream>>>(net->d_net, net->d_rp, it);
+      for (int p = 0; p < net->h.n_projs; ++p) {
+        const ProjHost& J = net->projs[p];
+        multi::proj_kernel<<<J.H, multi::kProjThreads, multi::proj_smem_bytes(J.M, J.C), net->stream>>>(
+            net->d_net, net->d_rp, it, p);
+      }
+    }
+    return;
+  }
   if (net->persistent) {
     cudaMemsetAsync(net->bar, 0, (4 + (size_t)net->total_hcu) * sizeof(unsigned int), net->stream);
     int it0 = 0, n = n_ticks;
@@ -360,6 +384,7 @@ bool resolve(const bcpnn_net* net, const char* cname, Resolved* r) {
     if (base == "act") return plain(D.act, BCPNN_F32, n);
     if (base == "spike") return plain(D.spike, BCPNN_I8, n);
     if (base == ".counter") return plain(D.counter, BCPNN_I32, n);
+    if (base == "ada" && D.ada) return plain(D.ada, BCPNN_F32, n);
   }
   if (id < (int)net->projs.size()) {
     const ProjHost& J = net->projs[id];
@@ -426,11 +451,14 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   *out = nullptr;
   if (!desc || desc->n_pops <= 0 || desc->n_pops > kMaxPops || desc->n_projs < 0 || desc->n_projs > kMaxProj ||
       (desc->n_pops && !desc->pops) || (desc->n_projs && !desc->projs) || !(desc->dt > 0.0f) ||
-      desc->max_ticks_per_run <= 0 || (desc->tick_threads != 0 && desc->tick_threads != 256 && desc->tick_threads != 512))
+      desc->max_ticks_per_run <= 0 || (desc->tick_threads != 0 && desc->tick_threads != 256 && desc->tick_threads != 512) ||
+      desc->update_variant < 0 || desc->update_variant > 1 || desc->spike_buffer_size < 0 ||
+      desc->spike_buffer_size > 1024 || (desc->update_variant == 1 && desc->fp64_tables))
     return BCPNN_ERR_INVALID;
   for (int p = 0; p < desc->n_pops; ++p)
     if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 ||
-        desc->pops[p].mcu_num > (desc->tick_threads == 256 ? 256 : 512))
+        desc->pops[p].mcu_num > (desc->tick_threads == 256 ? 256 : 512) ||
+        (desc->update_variant == 1 && !(desc->pops[p].taua > 0.0f)))
       return BCPNN_ERR_INVALID;
   {
     std::vector<int> n_in(desc->n_pops, 0);
@@ -451,6 +479,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   net->exchange = desc->exchange_spikes != 0;
   net->threads = desc->tick_threads == 256 ? 256 : 512;
   net->fp64 = desc->fp64_tables != 0;
+  net->multi = desc->update_variant == 1;
+  net->ring_len = desc->spike_buffer_size > 0 ? desc->spike_buffer_size : 1;
   if (net->threads == 256)
     net->tick_fn = net->fp64 ? (const void*)t256::tick_kernel<1> : (const void*)t256::tick_kernel<0>;
   else
@@ -572,6 +602,13 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     if ((rc = dalloc(net, &D.act, n))) return bail(rc);
     if ((rc = dalloc(net, &D.spike, n))) return bail(rc);
     if ((rc = dalloc(net, &D.counter, n))) return bail(rc);
+    if (net->multi) {
+      if ((rc = dalloc(net, &D.ada, n))) return bail(rc);
+      if ((rc = dalloc(net, &D.ring, n * (size_t)net->ring_len))) return bail(rc);
+      D.ring_len = net->ring_len;
+      D.tauadt = dt / P.d.taua;                /* ProcUpdMulti/Pop.cpp:46 */
+      D.adgain = P.d.adgain;
+    }
     D.spk_log = net->log_buf + P.log_offset;
     D.log_words = P.log_words;
     D.n_in = (int)P.in_proj.size();
@@ -722,8 +759,31 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, net->tick_fn, net->threads, smem);
     const char* e = std::getenv("GSBN_PER_TICK");
     bool forced = e && e[0] == '1';
-    net->persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu;
+    net->persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu && !net->multi;
     if ((rc = dalloc(net, &net->bar, 4 + (size_t)net->total_hcu))) return bail(rc);
+  }
+  /* ProcUpdMulti: shared memory of its projection kernel (largest M, C) */
+  if (net->multi) {
+    size_t ms = 0;
+    for (const ProjHost& J : net->projs) ms = std::max(ms, multi::proj_smem_bytes(J.M, J.C));
+    int smem_max = 0;
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, net->device);
+    if (ms + 1024 > (size_t)smem_max) {
+      net->err = "network too large for the ProcUpdMulti projection kernel: " + std::to_string(ms) +
+                 " bytes of shared memory per HCU";
+      return bail(BCPNN_ERR_INVALID);
+    }
+    static std::mutex mu;
+    static size_t raised[kMaxDevices] = {0};
+    std::lock_guard<std::mutex> lock(mu);
+    if (ms > raised[net->device]) {
+      if (cudaFuncSetAttribute(multi::proj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms) !=
+          cudaSuccess) {
+        net->err = "cannot raise the shared memory limit of the ProcUpdMulti projection kernel";
+        return bail(BCPNN_ERR_CUDA);
+      }
+      raised[net->device] = ms;
+    }
   }
   /* deferred columns of the persistent launch: ring halves sized for every
      MCU of every HCU spiking in one tick (units of kColUnit slots) */
@@ -1020,7 +1080,10 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     }
     CU(cudaGraphLaunch(ge, net->stream));
   }
-  net->launches += (uint64_t)(net->persistent ? 1 : n_ticks) + (with_all ? 2u * net->projs.size() : 0u);
+  if (net->multi)
+    net->launches += (uint64_t)n_ticks * (1 + net->projs.size()) + (with_all ? net->projs.size() : 0u);
+  else
+    net->launches += (uint64_t)(net->persistent ? 1 : n_ticks) + (with_all ? 2u * net->projs.size() : 0u);
   if (with_all)
     for (const ProjHost& J : net->projs) net->all_cells += (uint64_t)J.H * J.C * J.M;
   net->k_total += n_ticks;

@@ -75,6 +75,11 @@ struct PopDev {
   const int* ext_off; /* [ext_t1 - ext_t0 + 1] offsets by simstep - ext_t0 */
   const int* ext_idx;
   int ext_t0, ext_t1;
+  /* ProcUpdMulti only */
+  float* ada;        /* [n] adaptation current                                */
+  int8_t* ring;      /* [ring_len][n] spikes by simstep % ring_len          */
+  int ring_len;      /* "spike buffer size"                                  */
+  float tauadt, adgain;
 };
 
 struct ProjDev {

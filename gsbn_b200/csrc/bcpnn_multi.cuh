@@ -1,0 +1,377 @@
+/*
+ * bcpnn_multi.cuh -- the ProcUpdMulti variant of the update
+ * (src/gsbn/procedures/ProcUpdMulti.cpp:94-125, ProcUpdMulti/Pop.cpp,
+ * ProcUpdMulti/Proj.cpp).  What differs from ProcUpdLazy:
+ *   - population: adaptation current `ada` subtracted from the support and
+ *     relaxed towards adgain*act (Pop.cpp:222-311), a constant 6.9*wmask in
+ *     double (Pop.cpp:246), the soft-WTA maximum seeded with the HCU's own
+ *     first MCU (Pop.cpp:263), spikes kept in a ring of `spike buffer size`
+ *     ticks (Pop.cpp:320-329);
+ *   - projections: no column updates.  A cell has no zi2/tij of its own; it
+ *     starts from its row's zi and ti and, when its row is active, replays
+ *     the postsynaptic spikes still in the ring since then (each one: decay
+ *     to that tick, zj2 += kftj), decays to now and adds kftj for a spike
+ *     now (Proj.cpp:364-488); the row's zi gains kfti only when time passed
+ *     (Proj.cpp:685-693); every active cell adds its weight to epsc.
+ * The closed forms are gsbn's (same expressions as ProcUpdLazy), evaluated
+ * with the shared decay tables and the exact division of bcpnn_device.cuh.
+ *
+ * One launch of pop_kernel per tick over every (population, HCU), then one
+ * launch of proj_kernel per projection over its destination HCUs (512
+ * threads); all_kernel does the catch-up at a change of prn.  Per-tick
+ * buffers follow the ProcUpdLazy path's tick parity (dsup, epsc, bj, si), so
+ * state reads and the spike log work unchanged.
+ */
+#ifndef BCPNN_MULTI_CUH
+#define BCPNN_MULTI_CUH
+
+#include "bcpnn_device.cuh"
+
+namespace bcpnn {
+namespace multi {
+
+constexpr int kPopThreads = 128;
+constexpr int kProjThreads = kBlock; /* 512: block_prefix works over kBlock threads */
+constexpr int kRowCells = 1024;      /* cells of one row chunk in shared memory */
+
+__host__ __device__ inline int row_chunk(int M) { return M >= kRowCells ? 1 : kRowCells / M; }
+
+/* dynamic shared memory of proj_kernel, in bytes */
+__host__ __device__ inline size_t proj_smem_bytes(int M, int C) {
+  return (size_t)(M + C + kRowCells + 3 * row_chunk(M)) * 4;
+}
+
+/* the decay-table pair of `part` for d elapsed ticks (d < len from the table,
+   else computed) */
+__device__ __forceinline__ void entry(const float4* tab, int len, const Coef& k, int d, int part, float4& A,
+                                      float4& B) {
+  load_entry(tab, len, k, d, part, A, B);
+}
+
+/* Population update, ProcUpdMulti/Pop.cpp:222-311 and fill_spike 403-421.
+   dynamic shared memory: 2*M floats. */
+__global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ float s_vsum;
+  const int P = net->cta_pop[blockIdx.x];
+  const int h = net->cta_hcu[blockIdx.x];
+  const PopDev& pop = net->pops[P];
+  const int M = pop.M, n = pop.n;
+  const int simstep = rp->simstep0 + it, kk = rp->k0 + it;
+  const int cur = kk & 1, prev = cur ^ 1;
+  float* s_dsup = sm;
+  float* s_act = sm + M;
+  int8_t* s_spk = (int8_t*)(sm + 2 * M);
+  const float wm = rp->wmask[pop.hcu_start + h];
+  const float* lginp = rp->lginp + pop.mcu_start;
+
+  /* update_sup_kernel_1_cpu, Pop.cpp:222-253 */
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    const int idx = h * M + j;
+    float wsup = 0.0f;
+    int offset = 0;
+    for (int m = 0; m < pop.dim_proj; ++m) {
+      wsup += pop.bj[prev][offset + idx] + pop.epsc[prev][offset + idx];
+      offset += n;
+    }
+    float noise = 0.0f;
+    if (pop.snoise != 0.0f)
+      noise = pop.snoise * dev_normal01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+    float sup = pop.lgbias + pop.igain * lginp[idx] + noise;
+    sup += (pop.wgain * wm) * wsup;
+    sup -= wm * pop.ada[idx];
+    sup = (float)((double)sup + 6.9 * (double)wm); /* a double constant in gsbn */
+    const float d = pop.dsup[prev][idx];
+    const float nd = d + (sup - d) * pop.taumdt;
+    pop.dsup[cur][idx] = nd;
+    s_dsup[j] = nd;
+  }
+  __syncthreads();
+  /* update_sup_kernel_2_cpu, Pop.cpp:255-286: serial in MCU order */
+  if (threadIdx.x == 0) {
+    float mx = s_dsup[0];
+    for (int m = 0; m < M; ++m)
+      if (s_dsup[m] > mx) mx = s_dsup[m];
+    const float maxact = bx_expf(pop.wtagain * mx);
+    float vsum = 0.0f;
+    for (int m = 0; m < M; ++m) {
+      float a = bx_expf(pop.wtagain * (s_dsup[m] - mx));
+      if (maxact < 1.0f) a *= maxact;
+      vsum += a;
+      s_act[m] = a;
+    }
+    s_vsum = vsum;
+  }
+  __syncthreads();
+  /* update_sup_kernel_3_cpu, Pop.cpp:288-311 */
+  const float vsum = s_vsum;
+  const float pr = net->poisson_hz * net->dt;
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    const int idx = h * M + j;
+    float a = s_act[j];
+    if (vsum > 1.0f) a /= vsum;
+    pop.act[idx] = a;
+    const float u = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+    int8_t spk = (int8_t)(u < a * pop.maxfqdt);
+    if (net->poisson_hz > 0.0f) {
+      const float up = bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+      if (up < pr) spk = 1;
+    }
+    pop.counter[idx] += spk;
+    pop.ada[idx] += (pop.adgain * a - pop.ada[idx]) * pop.tauadt;
+    s_spk[j] = spk;
+  }
+  /* fill_spike, Pop.cpp:403-421: replayed spikes replace the sampled ones */
+  if (pop.ext) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < M; j += blockDim.x) s_spk[j] = 0;
+    __syncthreads();
+    if (simstep >= pop.ext_t0 && simstep < pop.ext_t1) {
+      const int b0 = pop.ext_off[simstep - pop.ext_t0], b1 = pop.ext_off[simstep - pop.ext_t0 + 1];
+      for (int e = b0 + threadIdx.x; e < b1; e += blockDim.x) {
+        const int v = pop.ext_idx[e];
+        if (v >= h * M && v < h * M + M) s_spk[v - h * M] = 1;
+      }
+    }
+  }
+  __syncthreads();
+  int8_t* ring = pop.ring + (size_t)(simstep % pop.ring_len) * n;
+  uint32_t* log = pop.spk_log + (size_t)it * pop.log_words;
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    const int idx = h * M + j;
+    const int8_t sv = s_spk[j];
+    ring[idx] = sv;
+    pop.spike[idx] = sv;
+    if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
+    for (int q = 0; q < pop.n_out; ++q) net->projs[pop.out_proj[q]].si[cur][idx] = sv;
+  }
+}
+
+/* One cell of an active row (update_row_kernel_cpu, Proj.cpp:409-488, after
+   the row traces): replay of the postsynaptic spikes in the ring, decay to
+   simstep, kftj for a spike now.  tij/zi2 start from the row's ti/zi. */
+__device__ __forceinline__ void replay_cell(float4& c4, int tij, float zi2, int simstep, int last_exclusive,
+                                            const int8_t* __restrict__ ring, int B, int n, int mcu, const Coef& k,
+                                            const float4* tab, int tlen, float kftj, bool final_decay_always) {
+  float pij = c4.x, eij = c4.y, zj2 = c4.w;
+  int now = tij;
+  if (simstep - now >= B) now = simstep - B + 1;
+  while (now < simstep) {
+    ++now;
+    if ((!last_exclusive || now < simstep) && ring[(size_t)(now % B) * n + mcu] > 0) {
+      const int pdt = now - tij;
+      if (pdt > 0) {
+        float4 A, Bv;
+        entry(tab, tlen, k, pdt, 0, A, Bv);
+        cell_decay(pij, eij, zi2, zj2, k, A, Bv);
+        zj2 = zj2 + kftj;
+        tij = now;
+      }
+    }
+  }
+  const int pdt = simstep - tij;
+  if (final_decay_always || pdt > 0) {
+    float4 A, Bv;
+    entry(tab, tlen, k, pdt, 0, A, Bv);
+    float zi2_unused = zi2;
+    cell_decay(pij, eij, zi2_unused, zj2, k, A, Bv);
+  }
+  c4 = make_float4(pij, eij, zi2, zj2);
+}
+
+/* One tick of projection p for one destination HCU: update_jxx_cpu,
+   update_ssi_cpu, update_row_cpu and update_que_cpu (Proj.cpp:557-706). */
+__global__ void __launch_bounds__(kProjThreads, 1) proj_kernel(const NetDev* __restrict__ net,
+                                                              const RunParams* __restrict__ rp, int it, int p) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ int s_warp[kWarps], s_total, s_flag9;
+  const ProjDev& J = net->projs[p];
+  const PopDev& pop = net->pops[J.dest];
+  const int h = blockIdx.x;
+  const int M = J.M, C = J.C, n = pop.n, B = pop.ring_len;
+  const int simstep = rp->simstep0 + it, kk = rp->k0 + it;
+  const int cur = kk & 1, prev = cur ^ 1;
+  const float kp = J.taupdt * rp->prn;
+  const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+  const float4* tab = rp->tabs[p].tab;
+  const int tlen = rp->tabs[p].len;
+  const size_t eoff = (size_t)J.proj_in_pop * n;
+  const int8_t* sj = pop.ring + (size_t)(simstep % B) * n;
+  const int rch = row_chunk(M);
+  float* s_epsc = sm;
+  int* s_list = (int*)(sm + M);
+  float* s_w = sm + M + C;
+  float* s_pi = s_w + kRowCells;
+  int* s_ti = (int*)(s_pi + rch);
+  float* s_zi = (float*)(s_ti + rch);
+  const int tid = threadIdx.x;
+
+  /* update_jxx_kernel_cpu, Proj.cpp:321-362 */
+  for (int j = tid; j < M; j += blockDim.x) {
+    const int idx = h * M + j;
+    float pj = J.pj[idx], ej = J.ej[idx], zj = J.zj[idx];
+    float e = pop.epsc[prev][eoff + idx];
+    e *= (1 - J.kepsc);
+    pj += (ej - pj) * kp;
+    ej += (zj - ej) * k.ke;
+    zj *= (1 - J.kzj);
+    if (sj[idx] > 0) zj += J.kftj;
+    pop.bj[cur][eoff + idx] = (kp != 0.0f) ? J.bgain * bx_logf(pj + J.eps) : pop.bj[prev][eoff + idx];
+    J.pj[idx] = pj;
+    J.ej[idx] = ej;
+    J.zj[idx] = zj;
+    s_epsc[j] = e;
+  }
+  /* the active rows of this tick (the previous tick's delay queue), ascending */
+  const int nrow = J.list_cnt[h];
+  for (int i = tid; i < nrow; i += blockDim.x) s_list[i] = J.list[h * C + i];
+  if (tid == 0) s_flag9 = 0;
+  __syncthreads();
+
+  /* update_row_cpu, Proj.cpp:638-706 */
+  for (int base = 0; base < nrow; base += rch) {
+    const int nr = (nrow - base) < rch ? (nrow - base) : rch;
+    for (int t = tid; t < nr; t += blockDim.x) {
+      const int r = s_list[base + t];
+      s_ti[t] = J.ti[r];
+      s_zi[t] = J.zi[r];
+      if (r == 9) s_flag9 = 1;
+    }
+    __syncthreads();
+    /* row traces (from the top thread down) beside the cells (from thread 0 up) */
+    for (int t = blockDim.x - 1 - tid; t < nr; t += blockDim.x) {
+      const int r = s_list[base + t];
+      const int pdt = simstep - s_ti[t];
+      float pi = J.pi[r];
+      if (pdt > 0) {
+        float ei = J.ei[r], zi = s_zi[t];
+        float4 A, Bv;
+        entry(tab, tlen, k, pdt, 2, A, Bv);
+        row_decay(pi, ei, zi, k, A, Bv); /* zi becomes zi*exp(-kzi*pdt) */
+        J.pi[r] = pi;
+        J.ei[r] = ei;
+        J.zi[r] = zi + J.kfti;
+      }
+      J.ti[r] = simstep;
+      s_pi[t] = pi;
+    }
+    for (int c = tid; c < nr * M; c += blockDim.x) {
+      const int rr = c / M, j = c - rr * M;
+      const size_t index = (size_t)s_list[base + rr] * M + j;
+      float4 c4 = J.cell[index];
+      replay_cell(c4, s_ti[rr], s_zi[rr], simstep, 1, pop.ring, B, n, h * M + j, k, tab, tlen, J.kftj, true);
+      if (sj[h * M + j] > 0) c4.w += J.kftj;
+      J.cell[index] = c4;
+      s_w[c] = c4.x;
+    }
+    __syncthreads();
+    for (int c = tid; c < nr * M; c += blockDim.x) {
+      const int rr = c / M, j = c - rr * M;
+      const size_t index = (size_t)s_list[base + rr] * M + j;
+      float w;
+      if (kp != 0.0f) {
+        w = J.wgain * bx_logf((s_w[c] + J.eps2) / ((s_pi[rr] + J.eps) * (J.pj[h * M + j] + J.eps)));
+        J.wij[index] = w;
+      } else {
+        w = J.wij[index];
+      }
+      s_w[c] = w;
+    }
+    __syncthreads();
+    for (int j = tid; j < M; j += blockDim.x) {
+      float e = s_epsc[j];
+      for (int rr = 0; rr < nr; ++rr) e += s_w[rr * M + j];
+      s_epsc[j] = e;
+    }
+    __syncthreads();
+  }
+  for (int j = tid; j < M; j += blockDim.x) pop.epsc[cur][eoff + h * M + j] = s_epsc[j];
+
+  /* update_que_cpu, Proj.cpp:620-636, and the next tick's active rows
+     (update_ssi_cpu, :580-588), ascending */
+  const int8_t* si = J.si[prev];
+  int cnt = 0;
+  for (int s0 = 0; s0 < C; s0 += blockDim.x) {
+    const int s = s0 + tid;
+    bool act = false;
+    if (s < C) {
+      const int r = h * C + s;
+      const int src = J.ii[r];
+      if (src >= 0) {
+        if (src >= J.Ns) {
+          atomicOr(net->err, kErrIndex);
+        } else {
+          int qv = J.qi[r];
+          act = (qv & 0x01) != 0;
+          qv >>= 1;
+          if (si[src] > 0) qv |= (0x01 << (J.di[r] - 1));
+          J.qi[r] = qv;
+        }
+      }
+    }
+    int tot;
+    const int pos = block_prefix(act, s_warp, &s_total, &tot);
+    if (act) J.list[h * C + cnt + pos] = h * C + s;
+    cnt += tot;
+  }
+  if (tid == 0) {
+    J.list_cnt[h] = cnt;
+    uint32_t f = 0;
+    if (s_flag9) f |= 1;
+    if (h == 9 / M && 9 < n && sj[9] > 0) f |= 2;
+    if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + p], f);
+    atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
+  }
+}
+
+/* update_all_cpu (Proj.cpp:490-555) for projection p at a change of prn:
+   every row and its cells caught up to simstep0-1 with kp = taupdt*old_prn,
+   replaying the ring up to and including that tick.  One warp per row. */
+__global__ void all_kernel(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int p) {
+  const ProjDev& J = net->projs[p];
+  const PopDev& pop = net->pops[J.dest];
+  const int M = J.M, C = J.C, n = pop.n, B = pop.ring_len;
+  const int simstep = rp->simstep0 - 1;
+  const float kp = J.taupdt * rp->old_prn;
+  const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+  const float4* tab = rp->tabs[p].tab_old;
+  const int tlen = rp->tabs[p].old_len;
+  const int lane = threadIdx.x & 31;
+  const int R = J.H * C;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&net->counters[2], (unsigned long long)R * M);
+  for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < R; r += (gridDim.x * blockDim.x) >> 5) {
+    const int ti = J.ti[r];
+    const float zi = J.zi[r];
+    const int h = r / C;
+    const int pdt = simstep - ti;
+    float4 rA = make_float4(0, 0, 0, 0), rB = rA;
+    if (pdt > 0) entry(tab, tlen, k, pdt, 2, rA, rB);
+    if (lane == 0 && pdt > 0) {
+      float pi = J.pi[r], ei = J.ei[r], z = zi;
+      row_decay(pi, ei, z, k, rA, rB);
+      J.pi[r] = pi;
+      J.ei[r] = ei;
+    }
+    __syncwarp();
+    const float pi_new = J.pi[r];
+    for (int j = lane; j < M; j += 32) {
+      const size_t index = (size_t)r * M + j;
+      float4 c4 = J.cell[index];
+      replay_cell(c4, ti, zi, simstep, 0, pop.ring, B, n, h * M + j, k, tab, tlen, J.kftj, false);
+      J.cell[index] = c4;
+      if (kp != 0.0f)
+        J.wij[index] = J.wgain * bx_logf((c4.x + J.eps2) / ((pi_new + J.eps) * (J.pj[h * M + j] + J.eps)));
+    }
+    __syncwarp();
+    if (lane == 0) {
+      if (pdt > 0) J.zi[r] = zi * rB.w;
+      J.ti[r] = simstep;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace multi
+}  // namespace bcpnn
+
+#endif /* BCPNN_MULTI_CUH */

@@ -58,6 +58,8 @@ typedef struct bcpnn_pop_desc {
   float wgain;
   float lgbias;
   float snoise;
+  float taua;        /* ProcUpdMulti only: adaptation time constant (gsbn.proto:52, default 0.05) */
+  float adgain;      /* ProcUpdMulti only: adaptation gain (gsbn.proto:51, default 1)           */
 } bcpnn_pop_desc;
 
 /* One projection: gsbn ProjParam (gsbn.proto:61-74) fields used by
@@ -95,6 +97,11 @@ typedef struct bcpnn_net_desc {
                                 on the GPU and rounded once to float -- robust
                                 when time constants nearly coincide, not
                                 bit-identical to the reference */
+  int32_t update_variant;    /* 0: ProcUpdLazy; 1: ProcUpdMulti (row-only updates
+                                that replay a ring of postsynaptic spikes,
+                                adaptation in the population; per-tick launches) */
+  int32_t spike_buffer_size; /* ProcUpdMulti argi "spike buffer size" (1 .. 1024;
+                                0 means 1) */
 } bcpnn_net_desc;
 
 /* Build a network on the device with gsbn's initial values.  Limits: at most
