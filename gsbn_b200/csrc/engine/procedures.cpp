@@ -265,8 +265,8 @@ class ProcUpdLazy : public ProcedureBase {
  public:
   ~ProcUpdLazy() override {}
 
-  void init_new(SolverParam sp, Database& db) override { build(sp, db, false); }
-  void init_copy(SolverParam sp, Database& db) override { build(sp, db, true); }
+  void init_new(SolverParam sp, Database& db) override { build(sp, db, false, get_proc_param(sp), 0); }
+  void init_copy(SolverParam sp, Database& db) override { build(sp, db, true, get_proc_param(sp), 0); }
 
   void update_cpu() override {
     fatal("ProcUpdLazy has no CPU path in this build: run with mode GPU");
@@ -320,10 +320,10 @@ class ProcUpdLazy : public ProcedureBase {
     }
   }
 
- private:
-  void build(const SolverParam& sp, Database& db, bool copy) {
+ protected:
+  /* variant 0: ProcUpdLazy; 1: ProcUpdMulti (its ProcParam, its spike ring) */
+  void build(const SolverParam& sp, Database& db, bool copy, const ProcParam& pp, int variant) {
     _db = &db;
-    ProcParam pp = get_proc_param(sp);
     Parser par(pp);
     const NetParam& net = sp.net_param;
     for (const PopParam& p : net.pop_param)
@@ -339,6 +339,8 @@ class ProcUpdLazy : public ProcedureBase {
         d.wgain = p.wgain;
         d.lgbias = p.lgbias;
         d.snoise = p.snoise;
+        d.taua = p.taua;
+        d.adgain = p.adgain;
         db.pops.push_back(d);
       }
     for (const ProjParam* q : live_projs(net, (int)db.pops.size())) {
@@ -377,6 +379,12 @@ class ProcUpdLazy : public ProcedureBase {
     desc.exchange_spikes = has_proc(sp, "ProcExchangeSpike") ? 1 : 0;
     desc.device = device;
     desc.max_ticks_per_run = _max_ticks;
+    desc.update_variant = variant;
+    if (variant == 1) {
+      int ring = 1; /* ProcUpdMulti/Pop.cpp:31-36 */
+      if (par.argi("spike buffer size", ring) && ring <= 0) fatal("ProcUpdMulti: spike buffer size must be > 0");
+      desc.spike_buffer_size = ring;
+    }
     bcpnn_net* n = nullptr;
     int st = bcpnn_net_create(&desc, &n);
     if (st != BCPNN_OK) fatal(std::string("ProcUpdLazy: bcpnn_net_create: ") + bcpnn_status_string(st));
@@ -490,6 +498,22 @@ class ProcUpdLazy : public ProcedureBase {
 REGISTERIMPL(ProcUpdLazy)
 
 /* =================================================================
+ * ProcUpdMulti (src/gsbn/procedures/ProcUpdMulti.cpp:8-180): the row-only
+ * update with a ring of postsynaptic spikes and an adaptation current, on
+ * the same device network (bcpnn_net_desc.update_variant = 1, per-tick
+ * launches).  Keys: argi "spike buffer size" (default 1) and ProcUpdLazy's
+ * "seed", "device", "max-ticks-per-run", "external spike".
+ * ================================================================= */
+class ProcUpdMulti : public ProcUpdLazy {
+  REGISTER(ProcUpdMulti)
+ public:
+  void init_new(SolverParam sp, Database& db) override { build(sp, db, false, get_proc_param(sp), 1); }
+  void init_copy(SolverParam sp, Database& db) override { build(sp, db, true, get_proc_param(sp), 1); }
+  void update_cpu() override { fatal("ProcUpdMulti has no CPU path in this build: run with mode GPU"); }
+};
+REGISTERIMPL(ProcUpdMulti)
+
+/* =================================================================
  * ProcExchangeSpike (src/gsbn/procedures/ProcExchangeSpike.cpp:94-139):
  * si_<proj> <- spike_<src_pop> after every tick.  Fused into the tick kernel
  * (the network is built with exchange_spikes when this procedure is listed),
@@ -500,7 +524,8 @@ class ProcExchangeSpike : public ProcedureBase {
  public:
   void init_new(SolverParam sp, Database&) override {
     get_proc_param(sp);
-    if (!has_proc(sp, "ProcUpdLazy")) fatal("ProcExchangeSpike needs ProcUpdLazy");
+    if (!has_proc(sp, "ProcUpdLazy") && !has_proc(sp, "ProcUpdMulti"))
+      fatal("ProcExchangeSpike needs ProcUpdLazy or ProcUpdMulti");
   }
   void init_copy(SolverParam sp, Database& db) override { init_new(sp, db); }
   void update_cpu() override {}

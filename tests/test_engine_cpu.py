@@ -14,7 +14,7 @@ from gsbn_b200 import engine, schema, workloads
 REF_DATA = "/root/reference/data"
 
 PROCEDURES = {"ProcExtGen", "ProcUpdLazy", "ProcExchangeSpike", "ProcInitConn", "ProcSpkRec", "ProcCheck",
-              "ProcSnapshot", "ProcStructuralPlasticity"}
+              "ProcSnapshot", "ProcStructuralPlasticity", "ProcUpdMulti"}
 
 
 def g_float(v):

@@ -59,3 +59,54 @@ def test_multi_matches_oracle(tmp_path, ring):
         assert spikes > 20
     finally:
         gpu.close()
+
+
+def test_engine_runs_procupdmulti(tmp_path):
+    """A prototxt naming ProcUpdMulti (with gsbn's "spike buffer size" 25)
+    through the host engine's registry records the same spike trains as the
+    same network driven directly through the C ABI."""
+    from gsbn_b200 import engine
+    w = workloads.config0()
+    path = w.write(str(tmp_path))
+    with open(path) as f:
+        text = f.read()
+    assert 'name: "ProcUpdLazy"' in text
+    text = text.replace('name: "ProcUpdLazy"', 'name: "ProcUpdMulti"\n  argi { key: "spike buffer size" val: 25 }')
+    with open(path, "w") as f:
+        f.write(text)
+    with open(path) as f:
+        sp = schema.parse_prototxt(f.read())
+    s = engine.Solver(path)
+    s.run(True)
+    s.close()
+    import os
+    rec = {}
+    with open(os.path.join(sp.rec_param.directory, "ProcSpkRec", "spk_pop_0.csv")) as f:
+        for line in f.read().splitlines()[1:]:
+            v = [int(x) for x in line.split(",")]
+            rec[v[0]] = v[1:]
+    pops, projs = workloads.net_from_solver_param(sp)
+    for p in pops:
+        p.update(taua=0.05, adgain=1.0)
+    conn = workloads.read_conn_map(w.conn, pops, projs)
+    lgidx, wmask = extgen.stim_tables(schema.read_stim(sp.gen_param.stim_file))
+    eps = float(np.float32(sp.gen_param.eps))
+    net = capi.Net(pops, projs, float(np.float32(sp.gen_param.dt)), seed=w.meta["seed"], max_ticks=256, variant=1,
+                   spike_buffer=25)
+    try:
+        for k, (ii, di) in enumerate(conn):
+            net.set_conn(k, ii, di)
+        net.upload_stimuli_idx(lgidx, eps, wmask)
+        want = {}
+        for r in extgen.segments(sp):
+            net.use_stimulus(r.lgidx, r.wmask)
+            net.run(r.first, r.n, r.prn, r.old_prn)
+            bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")
+            for k in range(r.n):
+                idx = np.nonzero(bits[k])[0].tolist()
+                if idx:
+                    want[r.first + k] = idx
+    finally:
+        net.close()
+    assert rec == want
+    assert len(want) > 100
