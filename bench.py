@@ -451,6 +451,54 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     }
 
 
+def run_multi_extension(dev, steps, warmup, ring=25):
+    """ProcUpdMulti (row-only updates replaying a ring of postsynaptic spikes,
+    adaptation) on the 100x100 density-0.1 workload with gsbn's spike buffer
+    size 25: the same 200-segment step as the headline, one population launch
+    and one projection launch per tick (CUDA graph per run)."""
+    import torch
+    from gsbn_b200 import capi, extgen
+    work = tempfile.mkdtemp(prefix="gsbn_multi_")
+    w, sp, pops, projs, stim, conn, runs = build_schedule(work)
+    pops = [dict(p, taua=0.05, adgain=1.0) for p in pops]
+    net = capi.Net(pops, projs, float(np.float32(sp.gen_param.dt)), seed=w.meta["seed"], device=dev, max_ticks=128,
+                   variant=1, spike_buffer=ring)
+    try:
+        for k, (ii, di) in enumerate(conn):
+            net.set_conn(k, ii, di)
+        lgidx, wmask = extgen.stim_tables(stim)
+        net.upload_stimuli_idx(lgidx, float(np.float32(sp.gen_param.eps)), wmask)
+        stream = torch.cuda.ExternalStream(net.stream(), device=dev)
+
+        def step():
+            net.reset()
+            for r in runs:
+                net.use_stimulus(r.lgidx, r.wmask)
+                net.run(r.first, r.n, r.prn, r.old_prn)
+
+        for _ in range(max(1, warmup)):
+            step()
+        net.sync()
+        c0, l0 = sum(net.counters()), net.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        net.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        cells = (sum(net.counters()) - c0) / steps
+        ticks = sum(r.n for r in runs)
+        return {"workload": "100x100 HCU/MCU, recurrent density 0.1, ProcUpdMulti with spike buffer size 25 "
+                            "(adaptation taua 0.05, adgain 1): 1e4 training + 1e4 recall ticks per step",
+                "metric": "synaptic updates/s", "value": cells / (ms * 1e-3), "unit": "cell updates/s",
+                "ticks_per_s": ticks / (ms * 1e-3), "us_per_tick": ms * 1e3 / ticks, "ms_per_step": ms,
+                "steps": steps, "gpu_launches_per_step": (net.kernel_launches() - l0) / steps, "dtype": "f32"}
+    finally:
+        net.close()
+
+
 def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
     """The batching extension: 256 independent networks of uneven size (HCUs
     8-64, MCUs 5-50, full recurrent), 20 patterns each, advanced together under
@@ -630,14 +678,16 @@ def main():
     if args.only_extensions:
         if rank == 0:
             ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates),
-                   "batched": run_batch_extension(local_rank, max(1, args.steps // 2))}
+                   "batched": run_batch_extension(local_rank, max(1, args.steps // 2)),
+                   "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1)}
             print(json.dumps({"extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank)
     if rank == 0 and not args.no_extensions:
         out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
                                                                  args.recall_replicates),
-                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2))}
+                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2)),
+                             "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1)}
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, sample, secs = cpu_sample(args.cpu_ticks)
