@@ -33,6 +33,20 @@
 #include "bcpnn_multi.cuh"
 #include "bcpnn_numerics.h"
 
+namespace bcpnn {
+namespace multi {
+/* ProcUpdMulti's persistent launch: the tick loop of bcpnn_multi.cuh with the
+   bounded grid barrier of the tick kernel */
+__global__ void __launch_bounds__(kProjThreads, 1) tick_kernel(const NetDev* __restrict__ net,
+                                                              const RunParams* __restrict__ rp, int it0, int n_ticks,
+                                                              unsigned int* bar) {
+  __shared__ int s_ok;
+  tick_loop(net, rp, it0, n_ticks,
+            [&](int k) { return t512::grid_sync(bar, (unsigned int)k * gridDim.x, net->err, &s_ok); });
+}
+}  // namespace multi
+}  // namespace bcpnn
+
 using namespace bcpnn;
 
 namespace {
@@ -91,7 +105,9 @@ struct bcpnn_net {
   size_t tick_smem = 0;     /* dynamic shared memory of tick_kernel */
   int threads = 512;        /* CTA size of the tick kernel (512 or 256) */
   bool fp64 = false;        /* FP64-built decay tables */
-  bool multi = false;       /* ProcUpdMulti variant (bcpnn_multi.cuh), per-tick launches */
+  bool multi = false;       /* ProcUpdMulti variant (bcpnn_multi.cuh) */
+  bool multi_persistent = false; /* its one-launch-per-run form */
+  size_t multi_smem = 0;
   int ring_len = 1;         /* its spike buffer size */
   const void* tick_fn = nullptr; /* the tick kernel variant of that size */
   unsigned int* bar = nullptr; /* persistent kernel: [0] grid barrier arrivals, [1..2] column units by
@@ -301,6 +317,14 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
         const ProjHost& J = net->projs[p];
         multi::all_kernel<<<grid_for((size_t)J.H * J.C * 32, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
       }
+    if (net->multi_persistent) {
+      cudaMemsetAsync(net->bar, 0, sizeof(unsigned int), net->stream);
+      int it0 = 0, n = n_ticks;
+      void* args[] = {(void*)&net->d_net, (void*)&net->d_rp, (void*)&it0, (void*)&n, (void*)&net->bar};
+      cudaLaunchCooperativeKernel((const void*)multi::tick_kernel, dim3(net->total_hcu), dim3(multi::kProjThreads), args,
+                                  net->multi_smem, net->stream);
+      return;
+    }
     const size_t pop_smem = (size_t)(2 * net->max_m + net->max_m) * sizeof(float);
     for (int it = 0; it < n_ticks; ++it) {
       multi::pop_kernel<<<net->total_hcu, multi::kPopThreads, pop_smem, net->stream>>>(net->d_net, net->d_rp, it);
@@ -773,17 +797,28 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
                  " bytes of shared memory per HCU";
       return bail(BCPNN_ERR_INVALID);
     }
+    ms = std::max(ms, (size_t)(3 * net->max_m) * sizeof(float)); /* the population update's share */
+    net->multi_smem = ms;
     static std::mutex mu;
     static size_t raised[kMaxDevices] = {0};
     std::lock_guard<std::mutex> lock(mu);
     if (ms > raised[net->device]) {
       if (cudaFuncSetAttribute(multi::proj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms) !=
-          cudaSuccess) {
-        net->err = "cannot raise the shared memory limit of the ProcUpdMulti projection kernel";
+              cudaSuccess ||
+          cudaFuncSetAttribute(multi::tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms) !=
+              cudaSuccess) {
+        net->err = "cannot raise the shared memory limit of the ProcUpdMulti kernels";
         return bail(BCPNN_ERR_CUDA);
       }
       raised[net->device] = ms;
     }
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, net->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi::tick_kernel, multi::kProjThreads, ms);
+    const char* e = std::getenv("GSBN_PER_TICK");
+    const bool forced = e && e[0] == '1';
+    net->multi_persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu;
   }
   /* deferred columns of the persistent launch: ring halves sized for every
      MCU of every HCU spiking in one tick (units of kColUnit slots) */
@@ -1064,7 +1099,7 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   CU(cudaMemcpyAsync(net->d_tabs, net->tabs.data(), net->tabs.size() * sizeof(TabRef), cudaMemcpyHostToDevice,
                      net->stream));
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));
-  if (net->direct || net->persistent) {
+  if (net->direct || net->persistent || net->multi_persistent) {
     enqueue_run(net, n_ticks, with_all);
     CU(cudaGetLastError());
   } else {
@@ -1081,7 +1116,8 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     CU(cudaGraphLaunch(ge, net->stream));
   }
   if (net->multi)
-    net->launches += (uint64_t)n_ticks * (1 + net->projs.size()) + (with_all ? net->projs.size() : 0u);
+    net->launches += (net->multi_persistent ? 1u : (uint64_t)n_ticks * (1 + net->projs.size())) +
+                     (with_all ? net->projs.size() : 0u);
   else
     net->launches += (uint64_t)(net->persistent ? 1 : n_ticks) + (with_all ? 2u * net->projs.size() : 0u);
   if (with_all)

@@ -50,11 +50,10 @@ __device__ __forceinline__ void entry(const float4* tab, int len, const Coef& k,
 
 /* Population update, ProcUpdMulti/Pop.cpp:222-311 and fill_spike 403-421.
    dynamic shared memory: 2*M floats. */
-__global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it) {
-  extern __shared__ __align__(16) float sm[];
-  __shared__ float s_vsum;
-  const int P = net->cta_pop[blockIdx.x];
-  const int h = net->cta_hcu[blockIdx.x];
+__device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it, int P,
+                                        int h, float* sm, float* s_vsum_p) {
+  float& s_vsum = *s_vsum_p;
+  __shared__ float s_red[32];
   const PopDev& pop = net->pops[P];
   const int M = pop.M, n = pop.n;
   const int simstep = rp->simstep0 + it, kk = rp->k0 + it;
@@ -87,22 +86,34 @@ __global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __re
     s_dsup[j] = nd;
   }
   __syncthreads();
-  /* update_sup_kernel_2_cpu, Pop.cpp:255-286: serial in MCU order */
-  if (threadIdx.x == 0) {
+  /* update_sup_kernel_2_cpu, Pop.cpp:255-286: the maximum (order does not
+     matter) and the exponentials in parallel, the sum serial in MCU order */
+  {
     float mx = s_dsup[0];
-    for (int m = 0; m < M; ++m)
-      if (s_dsup[m] > mx) mx = s_dsup[m];
+    for (int m = threadIdx.x; m < M; m += blockDim.x) mx = s_dsup[m] > mx ? s_dsup[m] : mx;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float w = __shfl_xor_sync(0xffffffffu, mx, o);
+      mx = w > mx ? w : mx;
+    }
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    mx = s_red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = s_red[w] > mx ? s_red[w] : mx;
     const float maxact = bx_expf(pop.wtagain * mx);
-    float vsum = 0.0f;
-    for (int m = 0; m < M; ++m) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
       float a = bx_expf(pop.wtagain * (s_dsup[m] - mx));
       if (maxact < 1.0f) a *= maxact;
-      vsum += a;
       s_act[m] = a;
     }
-    s_vsum = vsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float vsum = 0.0f;
+      for (int m = 0; m < M; ++m) vsum += s_act[m];
+      s_vsum = vsum;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   /* update_sup_kernel_3_cpu, Pop.cpp:288-311 */
   const float vsum = s_vsum;
   const float pr = net->poisson_hz * net->dt;
@@ -147,6 +158,12 @@ __global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __re
   }
 }
 
+__global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ float s_vsum;
+  pop_hcu(net, rp, it, net->cta_pop[blockIdx.x], net->cta_hcu[blockIdx.x], sm, &s_vsum);
+}
+
 /* One cell of an active row (update_row_kernel_cpu, Proj.cpp:409-488, after
    the row traces): replay of the postsynaptic spikes in the ring, decay to
    simstep, kftj for a spike now.  tij/zi2 start from the row's ti/zi. */
@@ -181,13 +198,17 @@ __device__ __forceinline__ void replay_cell(float4& c4, int tij, float zi2, int 
 
 /* One tick of projection p for one destination HCU: update_jxx_cpu,
    update_ssi_cpu, update_row_cpu and update_que_cpu (Proj.cpp:557-706). */
-__global__ void __launch_bounds__(kProjThreads, 1) proj_kernel(const NetDev* __restrict__ net,
-                                                              const RunParams* __restrict__ rp, int it, int p) {
-  extern __shared__ __align__(16) float sm[];
-  __shared__ int s_warp[kWarps], s_total, s_flag9;
+struct ProjShared {
+  int warp[kWarps], total, flag9;
+};
+
+__device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it,
+                                         int p, int h, float* sm, ProjShared* ps) {
+  int* s_warp = ps->warp;
+  int& s_total = ps->total;
+  int& s_flag9 = ps->flag9;
   const ProjDev& J = net->projs[p];
   const PopDev& pop = net->pops[J.dest];
-  const int h = blockIdx.x;
   const int M = J.M, C = J.C, n = pop.n, B = pop.ring_len;
   const int simstep = rp->simstep0 + it, kk = rp->k0 + it;
   const int cur = kk & 1, prev = cur ^ 1;
@@ -321,6 +342,39 @@ __global__ void __launch_bounds__(kProjThreads, 1) proj_kernel(const NetDev* __r
     if (h == 9 / M && 9 < n && sj[9] > 0) f |= 2;
     if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + p], f);
     atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
+  }
+}
+
+__global__ void __launch_bounds__(kProjThreads, 1) proj_kernel(const NetDev* __restrict__ net,
+                                                              const RunParams* __restrict__ rp, int it, int p) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ ProjShared ps;
+  proj_hcu(net, rp, it, p, blockIdx.x, sm, &ps);
+}
+
+/* Persistent form: one cooperative launch per run, one CTA per (population,
+   HCU).  A tick of ProcUpdMulti needs from other HCUs only the source spikes
+   of the previous tick (si, the exchange), so one CTA does its HCU's
+   population update and then its rows of every incoming projection, and one
+   grid barrier separates the ticks.  The bodies are those of pop_kernel and
+   proj_kernel.  bar: the grid-barrier arrival counter, zero at launch. */
+template <typename GridSync>
+__device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it0,
+                                          int n_ticks, GridSync sync) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ float s_vsum;
+  __shared__ ProjShared ps;
+  const int P = net->cta_pop[blockIdx.x];
+  const int h = net->cta_hcu[blockIdx.x];
+  const PopDev& pop = net->pops[P];
+  for (int it = it0; it < it0 + n_ticks; ++it) {
+    if (it > it0 && !sync(it - it0)) return;
+    pop_hcu(net, rp, it, P, h, sm, &s_vsum);
+    __syncthreads();
+    for (int q = 0; q < pop.n_in; ++q) {
+      proj_hcu(net, rp, it, pop.in_proj[q], h, sm, &ps);
+      __syncthreads();
+    }
   }
 }
 

@@ -23,8 +23,9 @@ def lginp_row(row, pops, eps):
     return np.array([hit if row[h] == m else miss for h in range(H) for m in range(M)], np.float32)
 
 
-@pytest.mark.parametrize("ring", [25, 1])
-def test_multi_matches_oracle(tmp_path, ring):
+@pytest.mark.parametrize("ring,per_tick", [(25, False), (25, True), (1, False)])
+def test_multi_matches_oracle(tmp_path, ring, per_tick):
+    """persistent launch (one per run) and one launch per tick"""
     w = workloads.config0()
     sp, _ = w.solver_param(str(tmp_path))
     pops, projs = workloads.net_from_solver_param(sp)
@@ -37,7 +38,8 @@ def test_multi_matches_oracle(tmp_path, ring):
     assert any(r.prn != r.old_prn for r in runs[1:])
     dt = float(np.float32(sp.gen_param.dt))
     orc = multi.MultiNet(pops, projs, dt, seed=w.meta["seed"], spike_buffer=ring)
-    gpu = capi.Net(pops, projs, dt, seed=w.meta["seed"], max_ticks=256, variant=1, spike_buffer=ring)
+    from tests.test_gpu_parity import gpu_net
+    gpu = gpu_net(pops, projs, dt, seed=w.meta["seed"], max_ticks=256, variant=1, spike_buffer=ring, per_tick=per_tick)
     try:
         for k, (ii, di) in enumerate(conn):
             orc.set_conn(k, ii, di)
