@@ -402,6 +402,14 @@ __device__ __forceinline__ void cell_decay(float& pij, float& eij, float& zi2, f
   zj2 = zj2 * B.w;
 }
 
+/* Out-of-line copies for the tick kernel: one body of the closed forms
+   shared by its call sites keeps the kernel's instruction footprint small
+   (each phase runs once per tick, so its code is fetched again every tick). */
+__device__ __noinline__ float4 cell_decay_nl(float4 c, const Coef k, float4 A, float4 B) {
+  cell_decay(c.x, c.y, c.z, c.w, k, A, B);
+  return c;
+}
+
 /* Closed-form decay of the row traces, Proj.cpp:409-415 (row), :241-247
    (all).  A = entry[2], B = entry[3]. */
 __device__ __forceinline__ void row_decay(float& pi, float& ei, float& zi, const Coef& k, float4 A, float4 B) {
@@ -422,6 +430,11 @@ __device__ __forceinline__ void row_decay(float& pi, float& ei, float& zi, const
   pi = pn;
   ei = en;
   zi = zi * B.w;
+}
+
+__device__ __noinline__ float4 row_decay_nl(float4 r, const Coef k, float4 A, float4 B) {
+  row_decay(r.x, r.y, r.z, k, A, B);
+  return r;
 }
 
 /* ------------------------------------------------------------------------ */

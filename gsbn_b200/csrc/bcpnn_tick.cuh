@@ -365,7 +365,7 @@ __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, con
           else
             cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
         }
-        cell_decay(c4.x, c4.y, c4.z, c4.w, k, A, B);
+        c4 = cell_decay_nl(c4, k, A, B);
         c4.w = c4.w + J.kftj;
       }
       J.cell[index[u]] = c4;
@@ -765,7 +765,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
               float pi = tr.x, ei = tr.y, zi = tr.z;
               float4 A = stg_rA[t], B = stg_rB[t];
               if (pdt >= tlen) load_entry(tab, tlen, k, pdt, 2, A, B);
-              row_decay(pi, ei, zi, k, A, B);
+              {
+                const float4 rt = row_decay_nl(make_float4(pi, ei, zi, 0.0f), k, A, B);
+                pi = rt.x;
+                ei = rt.y;
+                zi = rt.z;
+              }
               zi = zi + J.kfti;
               J.pi[r] = pi;
               J.ei[r] = ei;
@@ -788,7 +793,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
             } else {
               float4 A = stg_cA[c], B = stg_cB[c];
               if (pdt >= tlen) load_entry(tab, tlen, k, pdt, 0, A, B);
-              cell_decay(cv.x, cv.y, cv.z, cv.w, k, A, B);
+              cv = cell_decay_nl(cv, k, A, B);
               cv.z = cv.z + J.kfti;
               J.cell[index] = cv;
               J.tij[index] = simstep;
@@ -1026,7 +1031,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                   else
                     cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
                 }
-                cell_decay(c4.x, c4.y, c4.z, c4.w, k, A, B);
+                c4 = cell_decay_nl(c4, k, A, B);
                 c4.w = c4.w + J.kftj;
               }
               J.cell[index[u]] = c4;
