@@ -109,7 +109,8 @@ struct bcpnn_net {
   bool multi_persistent = false; /* its one-launch-per-run form */
   size_t multi_smem = 0;
   int ring_len = 1;         /* its spike buffer size */
-  const void* tick_fn = nullptr; /* the tick kernel variant of that size */
+  const void* tick_fn = nullptr;  /* the tick kernel variant of the persistent launch */
+  const void* tick_fn0 = nullptr; /* the same size and decay form with in-CTA columns */
   unsigned int* bar = nullptr; /* persistent kernel: [0] grid barrier arrivals, [1..2] column units by
                                   tick parity, [4 + cta] column units done for each CTA */
   int4* col_ring = nullptr;    /* deferred column units (NetDev::col_ring) */
@@ -344,13 +345,13 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
   } else {
     for (int it = 0; it < n_ticks; ++it) {
       if (net->threads == 256 && net->fp64)
-        t256::tick_kernel<1><<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+        t256::tick_kernel<1, 0><<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
       else if (net->threads == 256)
-        t256::tick_kernel<0><<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+        t256::tick_kernel<0, 0><<<net->total_hcu, 256, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
       else if (net->fp64)
-        t512::tick_kernel<1><<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+        t512::tick_kernel<1, 0><<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
       else
-        t512::tick_kernel<0><<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
+        t512::tick_kernel<0, 0><<<net->total_hcu, 512, smem, net->stream>>>(net->d_net, net->d_rp, it, 1, net->bar);
     }
   }
 }
@@ -505,10 +506,13 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   net->fp64 = desc->fp64_tables != 0;
   net->multi = desc->update_variant == 1;
   net->ring_len = desc->spike_buffer_size > 0 ? desc->spike_buffer_size : 1;
-  if (net->threads == 256)
-    net->tick_fn = net->fp64 ? (const void*)t256::tick_kernel<1> : (const void*)t256::tick_kernel<0>;
-  else
-    net->tick_fn = net->fp64 ? (const void*)t512::tick_kernel<1> : (const void*)t512::tick_kernel<0>;
+  if (net->threads == 256) {
+    net->tick_fn = net->fp64 ? (const void*)t256::tick_kernel<1, 1> : (const void*)t256::tick_kernel<0, 1>;
+    net->tick_fn0 = net->fp64 ? (const void*)t256::tick_kernel<1, 0> : (const void*)t256::tick_kernel<0, 0>;
+  } else {
+    net->tick_fn = net->fp64 ? (const void*)t512::tick_kernel<1, 1> : (const void*)t512::tick_kernel<0, 1>;
+    net->tick_fn0 = net->fp64 ? (const void*)t512::tick_kernel<1, 0> : (const void*)t512::tick_kernel<0, 0>;
+  }
   {
     const char* e = std::getenv("GSBN_DIRECT_LAUNCH");
     net->direct = e && e[0] == '1';
@@ -768,7 +772,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     const int dev = net->device, v = (net->threads == 256 ? 1 : 0) + (net->fp64 ? 2 : 0);
     if (dev < 0 || dev >= kMaxDevices) { net->err = "device ordinal out of range"; return bail(BCPNN_ERR_INVALID); }
     if (smem > raised[v][dev]) {
-      if (cudaFuncSetAttribute(net->tick_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      if (cudaFuncSetAttribute(net->tick_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+          cudaFuncSetAttribute(net->tick_fn0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         net->err = "cannot raise the shared memory limit of tick_kernel";
         return bail(BCPNN_ERR_CUDA);
       }
@@ -833,6 +838,7 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     }
     /* unit counters are 32-bit within a launch */
     fits = fits && cap > 0 && cap * (long long)net->max_ticks < (1ll << 31);
+    if (!fits) net->tick_fn = net->tick_fn0; /* persistent, with in-CTA columns */
     if (fits) {
       if ((rc = dalloc(net, &net->col_ring, 2 * (size_t)cap))) return bail(rc);
       H.col_ring = net->col_ring;

@@ -380,8 +380,11 @@ __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, con
 /* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */
 /* kF64: the trace-decay form, fixed at compile time so the default
    instance carries no trace of the other (0: gsbn's closed form in float,
-   1: FP64-built propagators, see fp64_entry) */
-template <int kF64>
+   1: FP64-built propagators, see fp64_entry).  kDefer: column updates
+   deferred and spread over the grid (the persistent launch with its unit
+   ring) or done by the CTA itself in the tick (one launch per tick); each
+   instance holds only its own form. */
+template <int kF64, int kDefer>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* __restrict__ net,
                                                          const RunParams* __restrict__ rp, int it0, int n_ticks,
                                                          unsigned int* bar) {
@@ -432,7 +435,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   const float prn = rp->prn;
   /* deferred columns (persistent launch): bar[1..2] unit counters by tick
      parity, bar[4 + cta] units done for each CTA */
-  const int defer = rp->defer;
+  constexpr int defer = kDefer;
   unsigned int* const col_tail = bar + 1;
   unsigned int* const col_done = bar + 4;
 
