@@ -1101,7 +1101,6 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   net->rp.old_prn = old_prn;
   net->rp.lginp = net->cur_lg;
   net->rp.wmask = net->cur_wm;
-  net->rp.defer = (net->persistent && net->col_ring) ? 1 : 0;
   CU(cudaMemcpyAsync(net->d_tabs, net->tabs.data(), net->tabs.size() * sizeof(TabRef), cudaMemcpyHostToDevice,
                      net->stream));
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));

@@ -137,7 +137,6 @@ struct RunParams {
   const float* lginp;   /* stimulus of the run: [total MCUs] */
   const float* wmask;   /* [total HCUs] */
   const struct TabRef* tabs;  /* [n_projs] decay tables of the run */
-  int defer;      /* column updates deferred and spread over the grid (persistent launch) */
 };
 
 /* decay tables of one projection for a run */
