@@ -318,7 +318,7 @@ def profile_value(name, key):
     return None
 
 
-def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_sample=8):
+def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_sample=8, cpu=True):
     """The precision extension: recall of a trained 64x64 network (4096 x 4096
     weights) by 4096 noise replicates (25% cue, 20 Hz Poisson noise, 200
     ticks) with the support as a BF16 tcgen05 contraction, against the plain
@@ -418,6 +418,16 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
         plain_q_acc.append(float(recall.hcu_accuracy(counts, tr.H, tr.M, expected[r:r + 1])[0]))
         net.close()
     fp64 = profile_value("recall_precision_64x64.md", "fp64_error")
+    if cpu:
+        try:
+            v, sample = cpu_recall_sample(tr.pops, tr.projs, tr.dt, tr.poisson_hz, trained, lg[0], wm[0], tr.eps,
+                                          tr.t0, tr.old_prn, T, seed_base)
+            cpu_base = {"value": v, "unit": "replicate-ticks/s", "cores": 1, "kind": "port", "sample": sample,
+                        "cpu": cpu_model()}
+        except Exception as e:  # an auxiliary figure: the GPU numbers stand without it
+            cpu_base = {"unavailable": f"{type(e).__name__}: {e}"}
+    else:
+        cpu_base = None
     return {
         "workload": f"64x64 HCU/MCU full recurrent (4096 x 4096 weights), {work.meta['patterns']} trained patterns, "
                     f"{R} noise replicates, 25% cue, 20 Hz Poisson noise, {T} recall ticks",
@@ -448,6 +458,7 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
                                      "hcu_accuracy_bf16_sample": float(acc_q[:plain_sample].mean()),
                                      "hcu_accuracy_plain_fp32_sample": float(np.mean(plain_q_acc))}},
         "fp64_error": fp64,
+        "cpu_baseline": cpu_base,
     }
 
 
@@ -499,7 +510,7 @@ def run_multi_extension(dev, steps, warmup, ring=25):
         net.close()
 
 
-def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
+def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
     """The batching extension: 256 independent networks of uneven size (HCUs
     8-64, MCUs 5-50, full recurrent), 20 patterns each, advanced together under
     the schedule the tuner picks, against the plain path (one network per
@@ -555,7 +566,7 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
     plain_cells = plain.counters() - c1
     plain.close()
     sec = statistics.mean(secs)
-    return {
+    out = {
         "workload": f"{n_nets} independent networks, HCUs 8-64 x MCUs 5-50 (uniform), full recurrent, "
                     f"{sum(m.cells for m in members) / 1e6:.0f}M cells, 20 patterns each: "
                     f"{ticks} ticks (20 x 100 training + 20 x 50 recall)",
@@ -568,6 +579,14 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500):
         "batched_same_ticks": {"network_ticks_per_s": n_nets * n_head / t_head_best},
         "speedup_vs_plain_same_ticks": t_head_plain / t_head_best,
     }
+    if cpu:
+        try:
+            v, cores, sample = cpu_batch_sample(members, runs)
+            out["cpu_baseline"] = {"value": v, "unit": "network-ticks/s", "cores": cores, "kind": "port",
+                                   "sample": sample, "cpu": cpu_model()}
+        except Exception as e:  # an auxiliary figure: the GPU numbers above stand without it
+            out["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def cpu_sample(sample_ticks=600):
@@ -612,6 +631,99 @@ def cpu_sample(sample_ticks=600):
     sample = (f"{n_tr} training ticks + {n_rc} recall ticks of the 100x100 workload, including both all-cells "
               f"catch-ups, {s_tr + s_rc:.1f} s of CPU; per-tick rates scaled to the 2e4-tick step")
     return (c_tr + c_rc) / (t_tr + t_rc), sample, s_tr + s_rc
+
+
+def _lginp_row(row, hcu, mcu, hit, miss):
+    """ProcExtGen's lginp for one stimulus row (ProcExtGen.cpp:130-144): per
+    HCU log(1+eps) on the indexed MCU, log(eps) elsewhere and on HCUs without
+    input."""
+    out = np.full(hcu * mcu, miss, np.float32)
+    row = np.asarray(row[:hcu], np.int64)
+    h = np.nonzero((row >= 0) & (row < mcu))[0]
+    out[h * mcu + row[h]] = hit
+    return out
+
+
+def _batch_member_cpu(item):
+    """One batch member on the oracle, in a spawned worker: its first training
+    tick (with the start-of-run all-cells pass) and k_tr more training ticks,
+    then its first recall tick (with the training->recall all-cells catch-up)
+    and k_rc more recall ticks, each part timed alone.  Returns the member's
+    CPU seconds for its whole schedule, scaled per phase, and the seconds
+    actually spent."""
+    (pop, proj, seed, ii, di, lg_tr, wm_tr, lg_rc, wm_rc, tr_run, rc_run, dt, eps, k_tr, k_rc) = item
+    from oracle import sim
+    orc = sim.OracleNet([pop], [proj], dt, seed=seed)
+    orc.set_conn(0, ii, di)
+    H, M = pop["hcu_num"], pop["mcu_num"]
+    hit, miss = orc.logf(np.float32(1) + np.float32(eps)), orc.logf(np.float32(eps))
+    total, spent = 0.0, 0.0
+    for (first, n_phase, prn, old_prn), lg, wm, k in ((tr_run, lg_tr, wm_tr, k_tr), (rc_run, lg_rc, wm_rc, k_rc)):
+        orc.set_stimulus(_lginp_row(lg, H, M, hit, miss), wm[:H])
+        t0 = time.perf_counter()
+        orc.run(first, 1, prn, old_prn, spikes=False)
+        t1 = time.perf_counter()
+        orc.run(first + 1, k, prn, prn, spikes=False)
+        t2 = time.perf_counter()
+        total += (t1 - t0) + (t2 - t1) / k * (n_phase - 1)
+        spent += t2 - t0
+    return total, spent
+
+
+def cpu_batch_sample(members, runs, k_tr=20, k_rc=10):
+    """The oracle on the batched workload: B independent networks over the
+    host's cores (one spawned worker per core, largest networks first).  Every
+    member runs a bounded sample of its schedule (_batch_member_cpu); the
+    members' scaled CPU seconds, summed and divided by the cores, give the
+    wall time of the whole batch.  Returns (network ticks/s, cores, sample
+    description)."""
+    import multiprocessing as mp
+    train = [r for r in runs if r[2] != 0.0]
+    recall = [r for r in runs if r[2] == 0.0]
+    tr_run = (train[0][0], sum(r[1] for r in train), train[0][2], train[0][3])
+    rc_run = (recall[0][0], sum(r[1] for r in recall), recall[0][2], recall[0][3])
+    ticks = sum(r[1] for r in runs)
+    items = [(m.pop, m.proj, m.seed, m.ii, m.di, m.lgidx[train[0][4]], m.wmask[train[0][5]],
+              m.lgidx[recall[0][4]], m.wmask[recall[0][5]], tr_run, rc_run, 0.001, 1e-4, k_tr, k_rc)
+             for m in sorted(members, key=lambda m: -m.cells)]
+    from concurrent.futures import ProcessPoolExecutor
+    cores = max(1, min(len(os.sched_getaffinity(0)), 64, len(items)))
+    t0 = time.perf_counter()
+    # spawned workers (no fork of a process that holds a CUDA context); a worker
+    # that dies raises BrokenProcessPool here instead of leaving a wait behind
+    with ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as pool:
+        res = list(pool.map(_batch_member_cpu, items, chunksize=1))
+    wall = time.perf_counter() - t0
+    cpu_total = sum(r[0] for r in res)
+    value = len(members) * ticks / (cpu_total / cores)
+    sample = (f"all {len(members)} networks, each 1+{k_tr} training and 1+{k_rc} recall ticks (both all-cells "
+              f"passes included) on {cores} worker processes, {wall:.1f} s wall; per-phase tick rates scaled to "
+              f"the {ticks}-tick schedule, summed CPU time divided by the cores")
+    return value, cores, sample
+
+
+def cpu_recall_sample(pops, projs, dt, poisson_hz, state, lg_row, wm_row, eps, t0, old_prn, ticks, seed, k=40):
+    """The oracle on one recall replicate of the trained network, one core:
+    the end-of-training state written in, the first recall tick (with its
+    all-cells catch-up) and k more ticks timed, scaled to `ticks` ticks.
+    gsbn has no recall-only path, so this is the full ProcUpdLazy per tick.
+    Returns (replicate ticks/s, sample description)."""
+    from oracle import sim
+    orc = sim.OracleNet(pops, projs, dt, seed=seed, poisson_hz=poisson_hz)
+    for name, a in state.items():
+        orc.write(name, a)
+    H, M = pops[0]["hcu_num"], pops[0]["mcu_num"]
+    hit, miss = orc.logf(np.float32(1) + np.float32(eps)), orc.logf(np.float32(eps))
+    orc.set_stimulus(_lginp_row(lg_row, H, M, hit, miss), wm_row[:H])
+    s0 = time.perf_counter()
+    orc.run(t0, 1, 0.0, old_prn, spikes=False)
+    s1 = time.perf_counter()
+    orc.run(t0 + 1, k, 0.0, 0.0, spikes=False)
+    s2 = time.perf_counter()
+    per_rep = (s1 - s0) + (s2 - s1) / k * (ticks - 1)
+    sample = (f"one replicate, 1+{k} recall ticks on 1 core ({s2 - s0:.1f} s; the first tick carries the "
+              f"all-cells catch-up), scaled to {ticks} ticks")
+    return ticks / per_rep, sample
 
 
 def run_reference(args):
@@ -665,6 +777,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    cpu = world == 1 and not args.no_cpu_baseline
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
@@ -677,16 +790,17 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.only_extensions:
         if rank == 0:
-            ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates),
-                   "batched": run_batch_extension(local_rank, max(1, args.steps // 2)),
+            ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates,
+                                                       cpu=cpu),
+                   "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
                    "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1)}
             print(json.dumps({"extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank)
     if rank == 0 and not args.no_extensions:
         out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
-                                                                 args.recall_replicates),
-                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2)),
+                                                                 args.recall_replicates, cpu=cpu),
+                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
                              "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1)}
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
