@@ -462,7 +462,7 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     }
 
 
-def run_multi_extension(dev, steps, warmup, ring=25):
+def run_multi_extension(dev, steps, warmup, ring=25, cpu=True):
     """ProcUpdMulti (row-only updates replaying a ring of postsynaptic spikes,
     adaptation) on the 100x100 density-0.1 workload with gsbn's spike buffer
     size 25: the same 200-segment step as the headline, one population launch
@@ -501,13 +501,21 @@ def run_multi_extension(dev, steps, warmup, ring=25):
         ms = e0.elapsed_time(e1) / steps
         cells = (sum(net.counters()) - c0) / steps
         ticks = sum(r.n for r in runs)
-        return {"workload": "100x100 HCU/MCU, recurrent density 0.1, ProcUpdMulti with spike buffer size 25 "
-                            "(adaptation taua 0.05, adgain 1): 1e4 training + 1e4 recall ticks per step",
-                "metric": "synaptic updates/s", "value": cells / (ms * 1e-3), "unit": "cell updates/s",
-                "ticks_per_s": ticks / (ms * 1e-3), "us_per_tick": ms * 1e3 / ticks, "ms_per_step": ms,
-                "steps": steps, "gpu_launches_per_step": (net.kernel_launches() - l0) / steps, "dtype": "f32"}
+        out = {"workload": "100x100 HCU/MCU, recurrent density 0.1, ProcUpdMulti with spike buffer size 25 "
+                           "(adaptation taua 0.05, adgain 1): 1e4 training + 1e4 recall ticks per step",
+               "metric": "synaptic updates/s", "value": cells / (ms * 1e-3), "unit": "cell updates/s",
+               "ticks_per_s": ticks / (ms * 1e-3), "us_per_tick": ms * 1e3 / ticks, "ms_per_step": ms,
+               "steps": steps, "gpu_launches_per_step": (net.kernel_launches() - l0) / steps, "dtype": "f32"}
     finally:
         net.close()
+    if cpu:
+        try:
+            v, sample = cpu_multi_sample(ring)
+            out["cpu_baseline"] = {"value": v, "unit": "cell updates/s", "cores": 1, "kind": "port",
+                                   "sample": sample, "cpu": cpu_model()}
+        except Exception as e:  # an auxiliary figure: the GPU numbers above stand without it
+            out["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
@@ -589,20 +597,13 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
     return out
 
 
-def cpu_sample(sample_ticks=600):
-    """The oracle on a bounded sample of the workload: the first
-    `sample_ticks` training ticks (with the start-of-run all-cells pass), then
-    the training->recall all-cells catch-up and `sample_ticks // 2` recall
-    ticks.  Returns cells/s scaled to the full step by the phase rates."""
-    from gsbn_b200 import workloads
-    from oracle import sim
-    from tests.harness import load_workload, schedule
-    work = tempfile.mkdtemp(prefix="gsbn_cpu_")
-    sp, pops, projs, stim, conn, seed, phz = load_workload(workloads.config1(), work)
-    orc = sim.OracleNet(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed)
-    for k, (ii, di) in enumerate(conn):
-        orc.set_conn(k, ii, di)
-    runs = schedule(sp, stim, pops, orc.logf)
+def _phase_sample(orc, runs, sample_ticks):
+    """Time an oracle network (OracleNet or MultiNetC) on a bounded sample of
+    a schedule: the first `sample_ticks` training ticks, then
+    `sample_ticks // 2` recall ticks, each phase's first tick (which carries
+    its all-cells pass) timed alone.  Returns (cells/s scaled to the whole
+    schedule by the phase rates, training ticks run, recall ticks run,
+    seconds spent)."""
     train = [r for r in runs if r.prn != 0.0]
     recall = [r for r in runs if r.prn == 0.0]
 
@@ -628,9 +629,48 @@ def cpu_sample(sample_ticks=600):
 
     t_tr, c_tr, s_tr, n_tr = phase(train, sample_ticks)
     t_rc, c_rc, s_rc, n_rc = phase(recall, sample_ticks // 2)
+    return (c_tr + c_rc) / (t_tr + t_rc), n_tr, n_rc, s_tr + s_rc
+
+
+def cpu_sample(sample_ticks=600):
+    """The oracle on a bounded sample of the workload: the first
+    `sample_ticks` training ticks (with the start-of-run all-cells pass), then
+    the training->recall all-cells catch-up and `sample_ticks // 2` recall
+    ticks.  Returns cells/s scaled to the full step by the phase rates."""
+    from gsbn_b200 import workloads
+    from oracle import sim
+    from tests.harness import load_workload, schedule
+    work = tempfile.mkdtemp(prefix="gsbn_cpu_")
+    sp, pops, projs, stim, conn, seed, phz = load_workload(workloads.config1(), work)
+    orc = sim.OracleNet(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed)
+    for k, (ii, di) in enumerate(conn):
+        orc.set_conn(k, ii, di)
+    runs = schedule(sp, stim, pops, orc.logf)
+    v, n_tr, n_rc, secs = _phase_sample(orc, runs, sample_ticks)
     sample = (f"{n_tr} training ticks + {n_rc} recall ticks of the 100x100 workload, including both all-cells "
-              f"catch-ups, {s_tr + s_rc:.1f} s of CPU; per-tick rates scaled to the 2e4-tick step")
-    return (c_tr + c_rc) / (t_tr + t_rc), sample, s_tr + s_rc
+              f"catch-ups, {secs:.1f} s of CPU; per-tick rates scaled to the 2e4-tick step")
+    return v, sample, secs
+
+
+def cpu_multi_sample(ring, sample_ticks=1200):
+    """The compiled ProcUpdMulti oracle (oracle/bcpnn_oracle_multi.cpp) on a
+    bounded sample of the ProcUpdMulti workload, one core, as cpu_sample.
+    Returns (cells/s, sample description)."""
+    from gsbn_b200 import workloads
+    from oracle import multi, sim
+    from tests.harness import load_workload, schedule
+    work = tempfile.mkdtemp(prefix="gsbn_cpu_multi_")
+    sp, pops, projs, stim, conn, seed, phz = load_workload(workloads.config1(), work)
+    pops = [dict(p, taua=0.05, adgain=1.0) for p in pops]
+    orc = multi.MultiNetC(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed, spike_buffer=ring)
+    for k, (ii, di) in enumerate(conn):
+        orc.set_conn(k, ii, di)
+    lib = sim.load()
+    runs = schedule(sp, stim, pops, lambda x: lib.oracle_logf(sim.MATH_SHARED, float(x)))
+    v, n_tr, n_rc, secs = _phase_sample(orc, runs, sample_ticks)
+    sample = (f"{n_tr} training ticks + {n_rc} recall ticks, including both all-cells catch-ups, {secs:.1f} s "
+              f"on 1 core; per-tick rates scaled to the 2e4-tick step")
+    return v, sample
 
 
 def _lginp_row(row, hcu, mcu, hit, miss):
@@ -793,7 +833,7 @@ def main():
             ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates,
                                                        cpu=cpu),
                    "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
-                   "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1)}
+                   "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
             print(json.dumps({"extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank)
@@ -801,7 +841,7 @@ def main():
         out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
                                                                  args.recall_replicates, cpu=cpu),
                              "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
-                             "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1)}
+                             "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, sample, secs = cpu_sample(args.cpu_ticks)

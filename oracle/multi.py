@@ -303,3 +303,92 @@ class MultiNet:
         if base == ".counter":
             return self.pops[k]["counter"].copy()
         return self.projs[k][base].copy()
+
+
+POP_KEYS = ("taum", "wtagain", "maxfq", "igain", "wgain", "lgbias", "snoise", "taua", "adgain")
+
+
+def _declare(lib):
+    vp, i32, u32, fl, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, ctypes.c_size_t
+    lib.oracle_multi_create.restype = vp
+    lib.oracle_multi_create.argtypes = [fl, u32, i32, i32, vp, vp, i32, vp, vp]
+    lib.oracle_multi_destroy.argtypes = [vp]
+    lib.oracle_multi_set_stimulus.argtypes = [vp, vp, vp]
+    lib.oracle_multi_run.argtypes = [vp, i32, i32, fl, fl, vp]
+    lib.oracle_multi_state_info.restype = ctypes.c_longlong
+    lib.oracle_multi_state_info.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i32)]
+    lib.oracle_multi_read_state.argtypes = [vp, ctypes.c_char_p, vp, sz]
+    lib.oracle_multi_write_state.argtypes = [vp, ctypes.c_char_p, vp, sz]
+    lib.oracle_multi_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    return lib
+
+
+class MultiNetC:
+    """The same restatement compiled (oracle/bcpnn_oracle_multi.cpp), for
+    networks beyond 10x10; the call shape of MultiNet, plus write() and
+    counters() (active-row cells, 0 column cells, all-cells sweeps)."""
+
+    def __init__(self, pops, projs, dt, seed=0, spike_buffer=1):
+        self.lib = _declare(sim.load())
+        dims = np.array([[p["hcu_num"], p["mcu_num"]] for p in pops], np.int32).reshape(-1)
+        pf = np.array([[p.get(k, 0.0) for k in POP_KEYS] for p in pops], np.float32).reshape(-1)
+        pi = np.array([[q["src_pop"], q["dest_pop"]] for q in projs] or [[0, 0]], np.int32).reshape(-1)
+        qf = np.array([[q.get(k, 0.0) for k in sim.PROJ_KEYS] for q in projs] or [[0.0] * 9], np.float32).reshape(-1)
+        self.h = self.lib.oracle_multi_create(float(f32(dt)), seed, int(spike_buffer), len(pops), sim._p(dims),
+                                              sim._p(pf), len(projs), sim._p(pi), sim._p(qf))
+        if not self.h:
+            raise ValueError("oracle_multi_create refused the description")
+        self.sizes = [int(p["hcu_num"]) * int(p["mcu_num"]) for p in pops]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_multi_destroy(self.h)
+            self.h = None
+
+    def _vec(self, name):
+        kind = ctypes.c_int()
+        n = self.lib.oracle_multi_state_info(self.h, name.encode(), ctypes.byref(kind))
+        if n < 0:
+            raise KeyError(name)
+        return n, {0: np.float32, 1: np.int32, 2: np.int8}[kind.value]
+
+    def read(self, name):
+        n, dt = self._vec(name)
+        out = np.zeros(n, dt)
+        assert self.lib.oracle_multi_read_state(self.h, name.encode(), sim._p(out), out.nbytes) == 0
+        return out
+
+    def write(self, name, arr):
+        n, dt = self._vec(name)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        assert a.size == n
+        assert self.lib.oracle_multi_write_state(self.h, name.encode(), sim._p(a), a.nbytes) == 0
+
+    def set_conn(self, proj, ii, di):
+        self.write(f"ii_{proj}", ii)
+        self.write(f"di_{proj}", di)
+
+    def set_stimulus(self, lginp, wmask_row):
+        self._lg = np.ascontiguousarray(lginp, np.float32)
+        self._wm = np.ascontiguousarray(wmask_row, np.float32)
+        self.lib.oracle_multi_set_stimulus(self.h, sim._p(self._lg), sim._p(self._wm))
+
+    def run(self, first, n, prn, old_prn, spikes=True):
+        """ticks first .. first+n-1; the spike log [n, words] of every
+        population (None without `spikes`)"""
+        words = [(s + 31) // 32 for s in self.sizes]
+        buf = np.zeros(n * sum(words), np.uint32) if spikes else None
+        rc = self.lib.oracle_multi_run(self.h, first, n, prn, old_prn, sim._p(buf) if spikes else None)
+        assert rc == 0, rc
+        if not spikes:
+            return None
+        out, off = [], 0
+        for w in words:
+            out.append(buf[off:off + n * w].reshape(n, w).copy())
+            off += n * w
+        return out
+
+    def counters(self):
+        c = (ctypes.c_ulonglong * 2)()
+        self.lib.oracle_multi_counters(self.h, c)
+        return [int(c[0]), 0, int(c[1])]
