@@ -54,7 +54,8 @@ def test_expf_within_one_ulp_of_correctly_rounded():
     x = np.concatenate([rng.uniform(-104, 89, 1_000_000), rng.uniform(-1e-3, 1e-3, 100_000),
                         rng.standard_normal(100_000)]).astype(np.float32)
     got = sim.expf(x)
-    want = np.exp(x.astype(np.float64)).astype(np.float32)
+    with np.errstate(over="ignore"):  # x above ~88.72 rounds to inf in float32, as it should
+        want = np.exp(x.astype(np.float64)).astype(np.float32)
     assert ulp_diff(got, want).max() <= 1
 
 
