@@ -494,8 +494,9 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   }
   for (int p = 0; p < desc->n_projs; ++p) {
     const bcpnn_proj_desc& d = desc->projs[p];
+    /* slot_num is a float in gsbn's schema; (int) of it must be defined and >= 1 */
     if (d.src_pop < 0 || d.src_pop >= desc->n_pops || d.dest_pop < 0 || d.dest_pop >= desc->n_pops ||
-        (int)d.slot_num <= 0)
+        !(d.slot_num >= 1.0f && d.slot_num < 2147483648.0f))
       return BCPNN_ERR_INVALID;
   }
   bcpnn_net* net = new bcpnn_net();
@@ -701,7 +702,6 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     if ((rc = dalloc(net, &D.si[1], J.Ns))) return bail(rc);
     if ((rc = dalloc(net, &D.list, R))) return bail(rc);
     if ((rc = dalloc(net, &D.list_cnt, J.H))) return bail(rc);
-    float pij0 = (float)(1.0 / J.C / J.M);                                         /* Proj.cpp:99 */
   }
   for (int q = 0; q < desc->n_projs; ++q) {
     const ProjHost& J = net->projs[q];
@@ -986,7 +986,12 @@ int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t
                              int32_t n_wmask_rows, const float* wmask_rows) {
   if (!net) return BCPNN_ERR_INVALID;
   if (n_lgidx_rows <= 0 || !lgidx_rows) return fail(net, BCPNN_ERR_INVALID, "bcpnn_upload_stimuli_idx: empty table");
-  std::vector<float> lg((size_t)n_lgidx_rows * net->total_mcu);
+  std::vector<float> lg;
+  try {
+    lg.resize((size_t)n_lgidx_rows * net->total_mcu);
+  } catch (const std::bad_alloc&) { /* nothing may be thrown across the C ABI */
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_upload_stimuli_idx: no host memory for the expanded table");
+  }
   for (int r = 0; r < n_lgidx_rows; ++r)
     lginp_from_idx(net, lgidx_rows + (size_t)r * net->total_hcu, eps, lg.data() + (size_t)r * net->total_mcu);
   return bcpnn_upload_stimuli(net, n_lgidx_rows, lg.data(), n_wmask_rows, wmask_rows);
@@ -1017,8 +1022,10 @@ int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* 
   std::map<int, std::pair<int, int>> by_tick;
   int t0 = 0, t1 = 0;
   for (int k = 0; k < n; ++k) {
-    if (ticks[k] < 0) continue;
-    if (offsets[k + 1] < offsets[k]) return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_ext_spikes: bad offsets");
+    /* ticks a run can never reach (bcpnn_run: simsteps in [1, 2^24)) are dropped */
+    if (ticks[k] < 0 || ticks[k] >= (1 << 24)) continue;
+    if (offsets[k] < 0 || offsets[k + 1] < offsets[k])
+      return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_ext_spikes: bad offsets");
     for (int e = offsets[k]; e < offsets[k + 1]; ++e)
       if (idx[e] < 0 || idx[e] >= P.n)
         return fail(net, BCPNN_ERR_INVALID, "bcpnn_set_ext_spikes: MCU index outside the population");
@@ -1041,8 +1048,14 @@ int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* 
   }
   CU(cudaSetDevice(net->device));
   CU(cudaStreamSynchronize(net->stream));
-  if (P.ext_off) { CU(cudaFree(P.ext_off)); P.ext_off = nullptr; }
-  if (P.ext_idx) { CU(cudaFree(P.ext_idx)); P.ext_idx = nullptr; }
+  /* an earlier table is freed here and leaves the list bcpnn_net_destroy frees */
+  for (int* old : {P.ext_off, P.ext_idx})
+    if (old) {
+      net->allocs.erase(std::remove(net->allocs.begin(), net->allocs.end(), (void*)old), net->allocs.end());
+      CU(cudaFree(old));
+    }
+  P.ext_off = nullptr;
+  P.ext_idx = nullptr;
   CU(cudaMalloc((void**)&P.ext_off, off.size() * sizeof(int)));
   CU(cudaMalloc((void**)&P.ext_idx, std::max<size_t>(1, flat.size()) * sizeof(int)));
   CU(cudaMemcpy(P.ext_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1522,6 +1535,7 @@ bool resolve_noalloc(const bcpnn_net* net, const char* name, Resolved* r) {
     if (is("act")) return plain(D.act, BCPNN_F32, n);
     if (is("spike")) return plain(D.spike, BCPNN_I8, n);
     if (is(".counter")) return plain(D.counter, BCPNN_I32, n);
+    if (is("ada") && D.ada) return plain(D.ada, BCPNN_F32, n);
   }
   if (id < (int)net->projs.size()) {
     const ProjHost& J = net->projs[id];

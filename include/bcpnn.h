@@ -148,8 +148,11 @@ int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t
 
 /* External spike replay of one population (ProcUpdLazy args "external spike",
    ProcUpdLazy/Pop.cpp:67-110 and fill_spike :389-409): n entries, entry k
-   overrides the spikes of tick ticks[k] with idx[offsets[k] .. offsets[k+1]).
-   Once set, every tick is overridden (ticks not listed give no spikes). */
+   overrides the spikes of tick ticks[k] with idx[offsets[k] .. offsets[k+1]);
+   offsets holds n + 1 non-negative, non-decreasing values.  Ticks outside
+   [0, 2^24) are ignored (no run reaches them).  Once set, every tick is
+   overridden (ticks not listed give no spikes); a later call replaces the
+   table. */
 int bcpnn_set_ext_spikes(bcpnn_net* net, int32_t pop, int32_t n, const int32_t* ticks, const int32_t* offsets,
                          const int32_t* idx);
 
