@@ -115,6 +115,14 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _out_buffer(a, dtype):
+    """A caller's array that the library writes into by element count: it
+    must be a writable C-contiguous array of exactly that element type, or
+    the copy would write past its end."""
+    if not isinstance(a, np.ndarray) or a.dtype != dtype or not a.flags.c_contiguous or not a.flags.writeable:
+        raise ValueError(f"expected a writable C-contiguous {np.dtype(dtype).name} array")
+
+
 class Net:
     """One network on one GPU, driven through the C ABI."""
 
@@ -219,6 +227,7 @@ class Net:
         """Queue the copy of the last run's spike log of `pop` into `out`
         (uint32 [ticks, words], page-locked for an asynchronous copy); `out`
         is complete after the next sync()."""
+        _out_buffer(out, np.uint32)
         self._check(self._lib.bcpnn_get_spike_log_async(self._h, pop, _ptr(out), out.size))
 
     def check_count(self, pop, k0, k1):
@@ -228,6 +237,10 @@ class Net:
     def check_result_async(self, pop, idx, cnt):
         """queue per-HCU (first most-spiking MCU or -1, its count) of `pop`
         into int32 idx/cnt and clear the counters; complete after sync()"""
+        _out_buffer(idx, np.int32)
+        _out_buffer(cnt, np.int32)
+        if cnt.size != idx.size:
+            raise ValueError("idx and cnt must have the same size")
         self._check(self._lib.bcpnn_check_result_async(self._h, pop, _ptr(idx), _ptr(cnt), idx.size))
 
     def ss_flags(self):

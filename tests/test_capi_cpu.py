@@ -61,6 +61,8 @@ PROJ = dict(src_pop=0, dest_pop=0, tauzi=0.01, tauzj=0.01, taue=0.02, taup=1.0, 
     ([dict(POP, mcu_num=513)], [], {}),
     ([POP], [dict(PROJ, dest_pop=1)], {}),
     ([POP], [dict(PROJ, slot_num=0.0)], {}),
+    ([POP], [dict(PROJ, slot_num=float("nan"))], {}),
+    ([POP], [dict(PROJ, slot_num=1e30)], {}),
     ([POP], [PROJ] * 9, {}),
     ([POP], [PROJ], dict(dt=0.0)),
     ([POP], [PROJ], dict(max_ticks=0)),
@@ -82,3 +84,19 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.bcpnn_last_error(None) == b"null handle"
     out = ctypes.c_void_p()
     assert lib.bcpnn_net_create(None, ctypes.byref(out)) == -1
+
+
+def test_output_buffers_are_checked_before_the_library_writes():
+    """The asynchronous copies write by element count into the caller's
+    array: a wrong element type, a strided view or a read-only array is
+    refused in Python, before any pointer reaches the library."""
+    import numpy as np
+    good = np.zeros((4, 3), np.uint32)
+    capi._out_buffer(good, np.uint32)
+    for bad in (np.zeros((4, 3), np.uint8), np.zeros((4, 6), np.uint32)[:, ::2], [0, 1, 2]):
+        with pytest.raises(ValueError):
+            capi._out_buffer(bad, np.uint32)
+    ro = np.zeros(3, np.int32)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        capi._out_buffer(ro, np.int32)
