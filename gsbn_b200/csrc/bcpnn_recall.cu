@@ -652,10 +652,14 @@ int bcpnn_recall_load(bcpnn_recall* r, const float* w, const float* bj, const fl
   float* row_f = nullptr;
   int8_t* row_s = nullptr;
   RCU(cudaMalloc((void**)&row_f, (size_t)N * 4));
-  RCU(cudaMalloc((void**)&row_s, (size_t)N * 3));
+  cudaError_t e = cudaMalloc((void**)&row_s, (size_t)N * 3);
+  if (e != cudaSuccess) {
+    cudaFree(row_f);
+    return fail(r, BCPNN_ERR_CUDA, std::string("recall load: ") + cudaGetErrorString(e));
+  }
   r->kk = 0;
   const int prev = 1; /* parity buffer read by the next tick (kk = 0) */
-  cudaError_t e = cudaMemcpy(row_f, epsc, (size_t)N * 4, cudaMemcpyHostToDevice);
+  e = cudaMemcpy(row_f, epsc, (size_t)N * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     broadcast_f32_kernel<<<592, 256, 0, r->stream>>>(r->epsc[prev], R, N, row_f);
     e = cudaStreamSynchronize(r->stream);
@@ -706,7 +710,8 @@ int bcpnn_recall_clear_counts(bcpnn_recall* r) {
 int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t count_first, int32_t count_last) {
   if (!r) return BCPNN_ERR_INVALID;
   if (!r->loaded || !r->cued) return fail(r, BCPNN_ERR_STATE, "bcpnn_recall_run before load and set_cues");
-  if (n_ticks < 0 || first < 0) return fail(r, BCPNN_ERR_INVALID, "bad tick range");
+  if (n_ticks < 0 || first < 0 || (long long)first + n_ticks > 0x7fffffffLL)
+    return fail(r, BCPNN_ERR_INVALID, "bad tick range");
   int counted = 0;
   for (int t = first; t < first + n_ticks; t++) counted += (t >= count_first && t <= count_last);
   if (r->counted + counted > 255)
