@@ -7,7 +7,6 @@ import struct
 
 import numpy as np
 import pytest
-from google.protobuf import text_format
 
 from gsbn_b200 import engine, schema, workloads
 
