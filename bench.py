@@ -837,7 +837,9 @@ def main():
             print(json.dumps({"extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank)
-    if rank == 0 and not args.no_extensions:
+    # the extensions are single-GPU measurements: under torchrun the other
+    # ranks would hold their GPUs at the final barrier while rank 0 runs them
+    if rank == 0 and world == 1 and not args.no_extensions:
         out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
                                                                  args.recall_replicates, cpu=cpu),
                              "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
