@@ -30,7 +30,23 @@ def _run(cmd):
     subprocess.run(cmd, check=True)
 
 
-def build(verbose_ptxas=False):
+def _headers():
+    out = []
+    for d in (CSRC, os.path.join(CSRC, "engine"), INC):
+        out += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".h", ".cuh", ".hpp"))]
+    return out
+
+
+def _stale(obj, src, force):
+    """An object is rebuilt when it is missing or older than its source or
+    any header of the library."""
+    if force or not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(f) > t for f in [src, __file__] + _headers())
+
+
+def build(verbose_ptxas=False, force=False):
     nvcc = os.environ.get("NVCC", "nvcc")
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -38,11 +54,13 @@ def build(verbose_ptxas=False):
     for src in sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-        _run([nvcc] + ARCH + COMMON + PLAIN + extra + ["-c", src, "-o", obj])
+        if _stale(obj, src, force or verbose_ptxas):
+            _run([nvcc] + ARCH + COMMON + PLAIN + extra + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in _sources("engine", ".cpp"):
         obj = os.path.join(objdir, "engine_" + os.path.basename(src) + ".o")
-        _run([nvcc] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", "-c", src, "-o", obj])
+        if _stale(obj, src, force):
+            _run([nvcc] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", "-c", src, "-o", obj])
         objs.append(obj)
     lib = os.path.join(HERE, "libgsbn_b200.so")
     _run([nvcc] + ARCH + ["-shared", "-o", lib] + objs + ["-cudart", "static"])
@@ -55,4 +73,4 @@ def build(verbose_ptxas=False):
 
 
 if __name__ == "__main__":
-    build(verbose_ptxas="-v" in sys.argv)
+    build(verbose_ptxas="-v" in sys.argv, force="--force" in sys.argv)

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -480,6 +481,20 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
       desc->update_variant < 0 || desc->update_variant > 1 || desc->spike_buffer_size < 0 ||
       desc->spike_buffer_size > 1024 || (desc->update_variant == 1 && desc->fp64_tables))
     return BCPNN_ERR_INVALID;
+  /* a rate dt/tau must be a finite positive number: a zero, negative,
+     infinite or NaN time constant (or frequency) makes the closed forms and
+     the FP64 propagator meaningless, so it is refused here, before any device
+     work */
+  auto pos = [](float x) { return x > 0.0f && x <= 3.4028234663852886e38f; };
+  if (!pos(desc->dt)) return BCPNN_ERR_INVALID;
+  for (int p = 0; p < desc->n_pops; ++p)
+    if (!pos(desc->pops[p].taum)) return BCPNN_ERR_INVALID;
+  for (int p = 0; p < desc->n_projs; ++p) {
+    const bcpnn_proj_desc& d = desc->projs[p];
+    if (!pos(d.tauzi) || !pos(d.tauzj) || !pos(d.taue) || !pos(d.taup) || !pos(d.maxfq) ||
+        !(d.tauepsc <= 3.4028234663852886e38f))
+      return BCPNN_ERR_INVALID;
+  }
   for (int p = 0; p < desc->n_pops; ++p)
     if (desc->pops[p].hcu_num <= 0 || desc->pops[p].mcu_num <= 0 ||
         desc->pops[p].mcu_num > (desc->tick_threads == 256 ? 256 : 512) ||
@@ -941,7 +956,7 @@ int bcpnn_use_stimulus(bcpnn_net* net, int32_t lginp_row, int32_t wmask_row) {
    indexed MCU, log(0+eps) elsewhere, float logs as the reference computes
    them. */
 static void lginp_from_idx(const bcpnn_net* net, const int32_t* lgidx_row, float eps, float* out) {
-  float hit = bx_logf(1 + eps), miss = bx_logf(0 + eps);
+  float hit = bx_extgen_logf(1 + eps), miss = bx_extgen_logf(0 + eps);
   size_t k = 0;
   int h = 0;
   for (const PopHost& P : net->pops)
@@ -972,8 +987,8 @@ int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hc
     if (rc) return rc;
   }
   CU(cudaMemcpyAsync(net->d_lgidx, lgidx_row, n_hcu * sizeof(int32_t), cudaMemcpyHostToDevice, net->stream));
-  lginp_idx_kernel<<<net->total_hcu, 128, 0, net->stream>>>(net->d_net, net->d_lgidx, bx_logf(1 + eps),
-                                                            bx_logf(0 + eps), net->h.lginp);
+  lginp_idx_kernel<<<net->total_hcu, 128, 0, net->stream>>>(net->d_net, net->d_lgidx, bx_extgen_logf(1 + eps),
+                                                            bx_extgen_logf(0 + eps), net->h.lginp);
   CU(cudaGetLastError());
   net->launches += 1;
   CU(cudaMemcpyAsync(net->h.wmask, wmask_row, n_wmask * sizeof(float), cudaMemcpyHostToDevice, net->stream));
@@ -1090,6 +1105,8 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     return fail(net, BCPNN_ERR_INVALID, "bcpnn_run: n_ticks outside [1, max_ticks_per_run]");
   if (first_simstep < 1 || (int64_t)first_simstep + n_ticks > (1 << 24))
     return fail(net, BCPNN_ERR_INVALID, "bcpnn_run: simstep outside [1, 2^24)");
+  if (!(std::fabs(prn) <= 3.4028234663852886e38f) || !(std::fabs(old_prn) <= 3.4028234663852886e38f))
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_run: prn and old_prn must be finite");
   CU(cudaSetDevice(net->device));
   bool with_all = (old_prn != prn);
   int need = first_simstep + n_ticks + 1;
@@ -1502,7 +1519,11 @@ int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns) {
 static constexpr size_t kNoAllocScratchFloats = (size_t)1 << 20; /* 4 MiB */
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
 static constexpr int kNoAllocMaxDevices = 64;
-static float* g_noalloc_scratch_dev[kNoAllocMaxDevices];  /* device address per ordinal, set on first use */
+/* device address per ordinal, set on the first call on that device.  Several
+   host threads may set an entry at once (all store the same address), so the
+   entries are atomics.  The cached address assumes the device is not reset
+   (cudaDeviceReset) while the library is loaded. */
+static std::atomic<float*> g_noalloc_scratch_dev[kNoAllocMaxDevices];
 
 namespace {
 
@@ -1591,12 +1612,12 @@ extern "C" int bcpnn_read_state_noalloc(bcpnn_net* net, const char* name, void* 
     case K_CELL: {
       /* set-up, once per device with that device current: the device address
          of the static scratch */
-      float* scratch = g_noalloc_scratch_dev[net->device];
+      float* scratch = g_noalloc_scratch_dev[net->device].load(std::memory_order_relaxed);
       if (!scratch) {
         void* p = nullptr;
         CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         scratch = (float*)p;
-        g_noalloc_scratch_dev[net->device] = scratch;
+        g_noalloc_scratch_dev[net->device].store(scratch, std::memory_order_relaxed);
       }
       /* every element read back is written by the gather first, so nothing
          of an earlier call's contents is used */

@@ -217,11 +217,14 @@ __device__ __forceinline__ void expm3_upper(double a00, double a01, double a11, 
   /* M = d A = [[m00, m01, 0], [0, m11, m12], [0, 0, m22]]; E = (E00, E01, E02, E11, E12, E22) */
   double m00 = a00 * d, m01 = a01 * d, m11 = a11 * d, m12 = a12 * d, m22 = a22 * d;
   double nrm = fmax(fabs(m00) + 0.0, fmax(fabs(m01) + fabs(m11), fabs(m12) + fabs(m22)));
-  int sq = 0;
-  while (nrm > 0.125) {
-    nrm *= 0.5;
-    sq++;
+  if (!(nrm <= 1.7976931348623157e308)) { /* an infinite or NaN rate: no propagator exists */
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int k = 0; k < 6; k++) E[k] = qnan;
+    return;
   }
+  /* a finite norm is below 2^1024, so at most 1027 halvings reach 1/8 */
+  int sq = 0;
+  for (; sq < 1100 && nrm > 0.125; sq++) nrm *= 0.5;
   const double sc = ldexp(1.0, -sq);
   m00 *= sc; m01 *= sc; m11 *= sc; m12 *= sc; m22 *= sc;
   /* Taylor sum of exp(M): term T_k = T_{k-1} M / k, upper triangular */

@@ -693,8 +693,8 @@ int bcpnn_recall_set_cues(bcpnn_recall* r, const int32_t* lgidx, float eps, cons
   RCU(cudaMemcpyAsync(r->lgidx, lgidx, n * 4, cudaMemcpyHostToDevice, r->stream));
   RCU(cudaMemcpyAsync(r->wmask, wmask, n * 4, cudaMemcpyHostToDevice, r->stream));
   RCU(cudaStreamSynchronize(r->stream));
-  r->lg_hit = bx_logf(1 + eps);
-  r->lg_miss = bx_logf(0 + eps);
+  r->lg_hit = bx_extgen_logf(1 + eps);
+  r->lg_miss = bx_extgen_logf(0 + eps);
   r->cued = true;
   return BCPNN_OK;
 }

@@ -164,8 +164,8 @@ class ProcExtGen : public ProcedureBase {
     }
     _lginp->data.assign(mcu_num, 0.f);
     _lginp->ld = mcu_num;
-    _lg_hit = bx_logf(1.0f + _eps);
-    _lg_miss = bx_logf(0.0f + _eps);
+    _lg_hit = bx_extgen_logf(1.0f + _eps);
+    _lg_miss = bx_extgen_logf(0.0f + _eps);
     /* every row read later must be wide enough (gsbn reads past the row) */
     for (const Mode& m : _modes) {
       if (m.lgidx_id >= (int)s.data_rows) fatal("ProcExtGen: lgidx row " + std::to_string(m.lgidx_id) + " not in stimulus file");

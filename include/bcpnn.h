@@ -247,20 +247,22 @@ int bcpnn_write_state(bcpnn_net* net, const char* name, const void* host, size_t
 
 /* The same read as bcpnn_read_state, for callers that cannot allocate device
    memory: an embedding whose device memory is entirely pre-reserved by its
-   own pool or budget, or code that reads state while a CUDA stream capture is
-   open, where cudaMalloc/cudaFree are not allowed.  bcpnn_read_state may
+   own pool or budget (a cudaMalloc there fails or breaks the embedder's
+   accounting), or a simulation loop that must not stall on cudaMalloc/
+   cudaFree, which can synchronise the whole device.  bcpnn_read_state may
    cudaMalloc a staging buffer the first time it gathers a cell field
    (pij/eij/zi2/zj2 are interleaved on the device); this entry point gathers
    into a fixed 4 MiB array compiled into the library instead, which every GPU
    that loads the library keeps until the process exits, and allocates
    nothing.  Limits: a cell field read this way has at most 1048576 elements
    (larger ones return BCPNN_ERR_SIZE); .siq_<proj> is not offered.  The first
-   call on a device looks up the array's device address (make that first call
-   before any stream capture).  All calls on a device share the array: calls
-   that overlap on the GPU (from several threads or handles at once) race, so
-   serialise them; each call synchronises its network's stream before it
-   returns.  No counterpart in the reference, which reads state through
-   SyncVector host mirrors. */
+   call on a device looks up the array's device address and keeps it (make
+   that first call before any stream capture; the kept address assumes the
+   device is not reset with cudaDeviceReset while the library is loaded).
+   All calls on a device share the array: calls that overlap on the GPU (from
+   several threads or handles at once) race, so serialise them; each call
+   synchronises its network's stream before it returns.  No counterpart in
+   the reference, which reads state through SyncVector host mirrors. */
 int bcpnn_read_state_noalloc(bcpnn_net* net, const char* name, void* host, size_t bytes);
 
 /* Cumulative cell updates since creation: out[0] row cells, out[1] column

@@ -41,6 +41,7 @@
 #ifndef BCPNN_NUMERICS_H
 #define BCPNN_NUMERICS_H
 
+#include <math.h>
 #include <stdint.h>
 
 #if defined(__CUDACC__)
@@ -338,6 +339,20 @@ BX_HD float bx_normal01(uint32_t seed, uint32_t pop, uint32_t tick, uint32_t mcu
 #endif
   return (float)(rad * bx_cos2pi_d(u2));
 }
+
+/* ------------------------------------------------------------------------ */
+/* ProcExtGen's stimulus values                                              */
+/* ------------------------------------------------------------------------ */
+
+/* log(1+eps) and log(0+eps), the two lginp values (ProcExtGen.cpp:130-144).
+   gsbn computes them on the host with the C library's float log in every
+   mode, so host code here calls the same function and the stimulus rows are
+   gsbn's bit for bit.  Host only. */
+#if defined(__CUDACC__)
+static inline __host__ float bx_extgen_logf(float x) { return logf(x); }
+#else
+static inline float bx_extgen_logf(float x) { return logf(x); }
+#endif
 
 #ifdef __cplusplus
 }

@@ -39,13 +39,54 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "bcpnn_numerics.h"
 
+#ifdef BCPNN_ORACLE_REF
+/* gsbn's own kernels (ProcUpdLazy/Proj.cpp:209-536, ProcUpdLazy/Pop.cpp:
+   229-323), compiled from the gsbn sources by oracle/extract_ref_kernels.sh.
+   In math mode MATH_REF the oracle's loops call these instead of its own
+   restatement, so the arithmetic is the reference's, unmodified. */
+namespace gsbn {
+namespace proc_upd_lazy {
+void update_all_kernel_cpu(int i, int j, int dim_conn, int dim_mcu, float* ptr_pi, float* ptr_ei, float* ptr_zi,
+                           int* ptr_ti, const float* ptr_pj, float* ptr_pij, float* ptr_eij, float* ptr_zi2,
+                           float* ptr_zj2, int* ptr_tij, float* ptr_wij, int simstep, float kp, float ke, float kzi,
+                           float kzj, float wgain, float eps, float eps2);
+void update_jxx_kernel_cpu(int idx, const int8_t* ptr_sj, float* ptr_pj, float* ptr_ej, float* ptr_zj,
+                           float* ptr_bj, float* ptr_epsc, float kp, float ke, float kzj, float kzi, float kepsc,
+                           float kftj, float bgain, float eps);
+void update_row_kernel_cpu(int i, int j, int dim_conn, int dim_mcu, const int* ptr_ssi, float* ptr_pi,
+                           float* ptr_ei, float* ptr_zi, int* ptr_ti, const float* ptr_pj, float* ptr_pij,
+                           float* ptr_eij, float* ptr_zi2, float* ptr_zj2, int* ptr_tij, float* ptr_wij,
+                           float* ptr_epsc, int simstep, float kp, float ke, float kzi, float kzj, float kfti,
+                           float wgain, float eps, float eps2);
+void update_col_kernel_cpu(int i, int j, int dim_conn, int dim_mcu, const int* ptr_ii, const int* ptr_ssj,
+                           float* ptr_pij, float* ptr_eij, float* ptr_zi2, float* ptr_zj2, int* ptr_tij,
+                           int simstep, float kp, float ke, float kzi, float kzj, float kftj);
+void update_sup_kernel_1_cpu(int i, int j, int dim_proj, int dim_hcu, int dim_mcu, const float* ptr_epsc,
+                             const float* ptr_bj, const float* ptr_lginp, const float* ptr_wmask,
+                             const float* ptr_rnd_normal, const float* ptr_ada, float* ptr_dsup, float wgain,
+                             float lgbias, float igain, float taumdt);
+void update_sup_kernel_2_cpu(int i, int dim_mcu, const float* ptr_dsup, float* ptr_act, float wtagain);
+void update_sup_kernel_3_cpu(int i, int j, int dim_mcu, const float* ptr_act, const float* ptr_rnd_uniform01,
+                             int8_t* ptr_spk, int* ptr_counter, float* ptr_ada, float maxfqdt, float adgain,
+                             float ka);
+}  // namespace proc_upd_lazy
+}  // namespace gsbn
+namespace ref = gsbn::proc_upd_lazy;
+static constexpr bool kHaveRef = true;
+#else
+static constexpr bool kHaveRef = false;
+#endif
+
+
 namespace oracle {
 
-enum { MATH_LIBM = 0, MATH_SHARED = 1 };
+enum { MATH_LIBM = 0, MATH_SHARED = 1, MATH_REF = 2 };
+
 
 /* exp/log as the reference calls them (on the value type), or the shared
    definition. */
@@ -278,6 +319,36 @@ template <typename T>
 void pop_update_sup(Net<T>& net, Pop<T>* p, int simstep) {
   const T* ptr_wmask = net.wmask_row.data() + p->hcu_start;
   const T* ptr_lginp = net.lginp.data() + p->mcu_start;
+#ifdef BCPNN_ORACLE_REF
+  if constexpr (std::is_same<T, float>::value) {
+    if (net.math == MATH_REF) {
+      /* Pop::update_sup_cpu's loop (Pop.cpp:343-386) over gsbn's kernels;
+         the adaptation pointer is unused there (its lines are commented out,
+         Pop.cpp:258,322).  The project-defined Poisson input noise is OR-ed
+         in afterwards with the same effect on spike and counter. */
+      for (int i = 0; i < p->dim_hcu; i++) {
+        for (int j = 0; j < p->dim_mcu; j++)
+          ref::update_sup_kernel_1_cpu(i, j, p->dim_proj, p->dim_hcu, p->dim_mcu, p->epsc.data(), p->bj.data(),
+                                       ptr_lginp, ptr_wmask, p->rnd_normal.data(), nullptr, p->dsup.data(),
+                                       p->wgain, p->lgbias, p->igain, p->taumdt);
+        ref::update_sup_kernel_2_cpu(i, p->dim_mcu, p->dsup.data(), p->act.data(), p->wtagain);
+        for (int j = 0; j < p->dim_mcu; j++) {
+          ref::update_sup_kernel_3_cpu(i, j, p->dim_mcu, p->act.data(), p->rnd_uniform01.data(), p->spike.data(),
+                                       p->counter.data(), nullptr, p->maxfqdt, 0.0f, 0.0f);
+          if (net.poisson_hz > 0.0f) {
+            int idx = i * p->dim_mcu + j;
+            float u = bx_uniform01_poisson(net.seed, (uint32_t)p->id, (uint32_t)simstep, (uint32_t)idx);
+            if (u < net.poisson_hz * net.dt && p->spike[idx] == 0) {
+              p->spike[idx] = 1;
+              p->counter[idx] += 1;
+            }
+          }
+        }
+      }
+      return;
+    }
+  }
+#endif
   for (int i = 0; i < p->dim_hcu; i++) {
     for (int j = 0; j < p->dim_mcu; j++) {
       sup_kernel_1<T>(i, j, p->dim_proj, p->dim_hcu, p->dim_mcu, p->epsc.data(), p->bj.data(), ptr_lginp,
@@ -502,6 +573,21 @@ template <typename T>
 void proj_update_all(Net<T>& net, Proj<T>* j, int simstep, float prn, float old_prn) {
   if (old_prn == prn) return;
   int R = j->dim_hcu * j->dim_conn;
+#ifdef BCPNN_ORACLE_REF
+  if constexpr (std::is_same<T, float>::value) {
+    if (net.math == MATH_REF) {
+      for (int i = 0; i < R; i++)
+        for (int k = 0; k < j->dim_mcu; k++)
+          ref::update_all_kernel_cpu(i, k, j->dim_conn, j->dim_mcu, j->pi.data(), j->ei.data(), j->zi.data(),
+                                     j->ti.data(), j->pj.data(), j->pij.data(), j->eij.data(), j->zi2.data(),
+                                     j->zj2.data(), j->tij.data(), j->wij.data(), simstep - 1,
+                                     j->taupdt * old_prn, j->tauedt, j->tauzidt, j->tauzjdt, j->wgain, j->eps,
+                                     j->eps2);
+      net.cnt.all_cells += (uint64_t)R * j->dim_mcu;
+      return;
+    }
+  }
+#endif
   for (int i = 0; i < R; i++) {
     for (int k = 0; k < j->dim_mcu; k++) {
       all_kernel<T>(net.math, i, k, j->dim_conn, j->dim_mcu, j->pi.data(), j->ei.data(), j->zi.data(),
@@ -520,6 +606,17 @@ void proj_update_jxx(Net<T>& net, Proj<T>* j, float prn) {
   T* ptr_epsc = j->dest->epsc.data() + off;
   T* ptr_bj = j->dest->bj.data() + off;
   const int8_t* ptr_sj = j->dest->spike.data();
+#ifdef BCPNN_ORACLE_REF
+  if constexpr (std::is_same<T, float>::value) {
+    if (net.math == MATH_REF) {
+      for (int i = 0; i < j->dim_hcu * j->dim_mcu; i++)
+        ref::update_jxx_kernel_cpu(i, ptr_sj, j->pj.data(), j->ej.data(), j->zj.data(), ptr_bj, ptr_epsc,
+                                   j->taupdt * prn, j->tauedt, j->tauzjdt, j->tauzidt, j->tauepscdt, j->kftj,
+                                   j->bgain, j->eps);
+      return;
+    }
+  }
+#endif
   for (int i = 0; i < j->dim_hcu * j->dim_mcu; i++) {
     jxx_kernel<T>(net.math, i, ptr_sj, j->pj.data(), j->ej.data(), j->zj.data(), ptr_bj, ptr_epsc,
                   j->taupdt * (T)prn, j->tauedt, j->tauzjdt, j->tauepscdt, j->kftj, j->bgain, j->eps);
@@ -555,6 +652,21 @@ template <typename T>
 void proj_update_row(Net<T>& net, Proj<T>* j, int simstep, float prn) {
   T* ptr_epsc = j->dest->epsc.data() + (size_t)j->proj_in_pop * j->dim_hcu * j->dim_mcu;
   int active_row_num = (int)j->ssi.size();
+#ifdef BCPNN_ORACLE_REF
+  if constexpr (std::is_same<T, float>::value) {
+    if (net.math == MATH_REF) {
+      for (int i = 0; i < active_row_num; i++)
+        for (int k = 0; k < j->dim_mcu; k++)
+          ref::update_row_kernel_cpu(i, k, j->dim_conn, j->dim_mcu, j->ssi.data(), j->pi.data(), j->ei.data(),
+                                     j->zi.data(), j->ti.data(), j->pj.data(), j->pij.data(), j->eij.data(),
+                                     j->zi2.data(), j->zj2.data(), j->tij.data(), j->wij.data(), ptr_epsc, simstep,
+                                     j->taupdt * prn, j->tauedt, j->tauzidt, j->tauzjdt, j->kfti, j->wgain,
+                                     j->eps, j->eps2);
+      net.cnt.row_cells += (uint64_t)active_row_num * j->dim_mcu;
+      return;
+    }
+  }
+#endif
   for (int i = 0; i < active_row_num; i++) {
     for (int k = 0; k < j->dim_mcu; k++) {
       row_kernel<T>(net.math, i, k, j->dim_conn, j->dim_mcu, j->ssi.data(), j->pi.data(), j->ei.data(),
@@ -570,6 +682,19 @@ void proj_update_row(Net<T>& net, Proj<T>* j, int simstep, float prn) {
 template <typename T>
 void proj_update_col(Net<T>& net, Proj<T>* j, int simstep, float prn) {
   int active_col_num = (int)j->ssj.size();
+#ifdef BCPNN_ORACLE_REF
+  if constexpr (std::is_same<T, float>::value) {
+    if (net.math == MATH_REF) {
+      for (int k = 0; k < active_col_num; k++)
+        for (int i = 0; i < j->dim_conn; i++)
+          ref::update_col_kernel_cpu(i, k, j->dim_conn, j->dim_mcu, j->ii.data(), j->ssj.data(), j->pij.data(),
+                                     j->eij.data(), j->zi2.data(), j->zj2.data(), j->tij.data(), simstep,
+                                     j->taupdt * prn, j->tauedt, j->tauzidt, j->tauzjdt, j->kftj);
+      net.cnt.col_cells += (uint64_t)active_col_num * j->dim_conn;
+      return;
+    }
+  }
+#endif
   for (int k = 0; k < active_col_num; k++) {
     for (int i = 0; i < j->dim_conn; i++) {
       col_kernel<T>(net.math, i, k, j->dim_conn, j->dim_mcu, j->ii.data(), j->ssj.data(), j->pij.data(),
@@ -723,6 +848,8 @@ extern "C" {
 void* oracle_create(int real_bits, int math, float dt, uint32_t seed, float poisson_hz, int n_pops,
                     const int* pop_dims, const float* pop_params, int n_projs, const int* proj_ints,
                     const float* proj_floats) {
+  /* gsbn's own kernels exist only in the oracle/_ref build, and only in float */
+  if (math == MATH_REF && (!kHaveRef || real_bits != 32)) return nullptr;
   OracleHandle* h = new OracleHandle();
   h->real_bits = real_bits;
   if (real_bits == 64)
@@ -848,6 +975,9 @@ void oracle_normal_array(uint32_t seed, uint32_t pop, uint32_t tick, int n, floa
   for (int i = 0; i < n; ++i) out[i] = bx_normal01(seed, pop, tick, (uint32_t)i);
 }
 float oracle_logf(int math, float x) { return Fn<float>::log(math, x); }
+
+/* 1 when this build carries gsbn's own kernels (math mode MATH_REF). */
+int oracle_has_ref(void) { return kHaveRef ? 1 : 0; }
 double oracle_log_double(int math, double x) { return log_double(math, x); }
 
 }  // extern "C"

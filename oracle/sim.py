@@ -14,9 +14,16 @@ procedures around the hot path, each citing the reference code it follows
   Solver loop       src/gsbn/Solver.cpp:67-92, src/gsbn/Upd.cpp:28-40
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use it.
-Parity against a reference binary is unpinned (the reference cannot be built
-here); the restatement is pinned on the reference's fixtures and on the
-published Philox known-answer vectors.
+
+Math modes of the C++ oracle:
+  MATH_SHARED  the restatement with the shared exp/log (bit-exact with the GPU);
+  MATH_LIBM    the restatement with glibc expf/logf, as gsbn's float calls;
+  MATH_REF     gsbn's own update_*_kernel_cpu functions, compiled from the gsbn
+               sources into oracle/_ref/libbcpnn_oracle_ref.so (oracle/Makefile
+               target `ref`), driven by the same loops.  The whole gsbn program
+               cannot be built (protobuf, MPI), but these free functions can.
+The restatement is pinned against MATH_REF, on the reference's fixtures and on
+the published Philox known-answer vectors.
 """
 import ctypes
 import os
@@ -26,23 +33,53 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libbcpnn_oracle.so")
-MATH_LIBM, MATH_SHARED = 0, 1
+LIB_REF = os.path.join(HERE, "_ref", "libbcpnn_oracle_ref.so")
+MATH_LIBM, MATH_SHARED, MATH_REF = 0, 1, 2
 f32 = np.float32
 
 _lib = None
+_lib_ref = None
 
 
 def build():
+    """The oracle, and oracle/_ref when the gsbn sources are present."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
 
 
-def load():
-    global _lib
+def reference_root():
+    """The gsbn source tree ($GSBN_REFERENCE_ROOT, else oracle/Makefile's
+    REF_ROOT), or None when it is not present."""
+    r = os.environ.get("GSBN_REFERENCE_ROOT")
+    if not r:
+        r = subprocess.run(["make", "-s", "-C", HERE, "ref-root"], capture_output=True, text=True).stdout.strip()
+    return r if r and os.path.isdir(r) else None
+
+
+def ref_available():
+    """True when oracle/_ref (gsbn's own kernels) is built."""
+    return os.path.exists(LIB_REF)
+
+
+def load(ref=False):
+    """The oracle library; ref=True: the build that carries gsbn's kernels."""
+    global _lib, _lib_ref
+    if ref:
+        if _lib_ref is not None:
+            return _lib_ref
+        if not os.path.exists(LIB_REF):
+            raise RuntimeError("oracle/_ref is not built (make -C oracle ref, with the gsbn sources present)")
+        _lib_ref = _bind(ctypes.CDLL(LIB_REF))
+        return _lib_ref
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB):
         build()
-    lib = ctypes.CDLL(LIB)
+    _lib = _bind(ctypes.CDLL(LIB))
+    return _lib
+
+
+def _bind(lib):
     vp, i32, u32, fl, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, ctypes.c_size_t
     lib.oracle_create.restype = vp
     lib.oracle_create.argtypes = [i32, i32, fl, u32, fl, i32, vp, vp, i32, vp, vp]
@@ -68,7 +105,7 @@ def load():
     lib.oracle_uniform_array.argtypes = [u32, u32, u32, i32, vp]
     lib.oracle_uniform_poisson_array.argtypes = [u32, u32, u32, i32, vp]
     lib.oracle_normal_array.argtypes = [u32, u32, u32, i32, vp]
-    _lib = lib
+    lib.oracle_has_ref.restype = i32
     return lib
 
 
@@ -88,6 +125,13 @@ def logf(x, math=MATH_SHARED):
     out = np.empty_like(x)
     load().oracle_logf_array(math, x.size, _p(x), _p(out))
     return out
+
+
+def extgen_logf(x):
+    """ProcExtGen's lginp values log(1+eps), log(0+eps) (ProcExtGen.cpp:130-144):
+    gsbn computes them on the host with glibc's float log in every mode, and
+    so does the product's host code; the stimulus rows are gsbn's bit for bit."""
+    return np.float32(load().oracle_logf(MATH_LIBM, float(np.float32(x))))
 
 
 def philox(ctr, key):
@@ -124,7 +168,7 @@ class OracleNet:
     """CPU restatement of one network (same call shape as gsbn_b200.capi.Net)."""
 
     def __init__(self, pops, projs, dt, seed=0, poisson_hz=0.0, real_bits=32, math=MATH_SHARED):
-        self.lib = load()
+        self.lib = load(ref=(math == MATH_REF))
         self.real_bits = real_bits
         self.math = math
         dims = np.array([[p["hcu_num"], p["mcu_num"]] for p in pops], dtype=np.int32).reshape(-1)
@@ -136,6 +180,8 @@ class OracleNet:
             pf = np.zeros(9, np.float32)
         self.h = self.lib.oracle_create(real_bits, math, dt, seed, poisson_hz, len(pops), _p(dims), _p(pp),
                                         len(projs), _p(pi), _p(pf))
+        if not self.h:
+            raise RuntimeError("MATH_REF needs the float oracle built with gsbn's kernels (oracle/_ref)")
         self.n_pops, self.n_projs = len(pops), len(projs)
 
     def __del__(self):
@@ -209,7 +255,9 @@ class OracleNet:
         return [int(c[0]), int(c[1]), int(c[2])]
 
     def logf(self, x):
-        return self.lib.oracle_logf(self.math, float(x))
+        """ProcExtGen's float log (host code in gsbn, glibc logf in every math
+        mode): the stimulus values log(1+eps) and log(eps)."""
+        return extgen_logf(x)
 
 
 # ---------------------------------------------------------------------------

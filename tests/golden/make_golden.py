@@ -3,8 +3,8 @@ files, decoded with the protobuf runtime (gsbn_b200.schema declares the
 reference schema) and plain Python: the inputs the oracle, the schedule
 expansion and the C++ engine's parsers are pinned against.
 
-Run in a checkout next to the reference sources:
-    python tests/golden/make_golden.py /root/reference
+Run with the path of a gsbn source tree:
+    python tests/golden/make_golden.py <gsbn source root>
 """
 import hashlib
 import json
@@ -84,4 +84,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <gsbn source root>")
+    main(sys.argv[1])

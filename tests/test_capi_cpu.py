@@ -65,7 +65,19 @@ PROJ = dict(src_pop=0, dest_pop=0, tauzi=0.01, tauzj=0.01, taue=0.02, taup=1.0, 
     ([POP], [dict(PROJ, slot_num=1e30)], {}),
     ([POP], [PROJ] * 9, {}),
     ([POP], [PROJ], dict(dt=0.0)),
+    ([POP], [PROJ], dict(dt=float("inf"))),
     ([POP], [PROJ], dict(max_ticks=0)),
+    # time constants and frequencies whose rate dt/tau is not a finite
+    # positive number (the FP64 propagator and the closed forms need one)
+    ([dict(POP, taum=0.0)], [PROJ], {}),
+    ([POP], [dict(PROJ, tauzi=0.0)], {}),
+    ([POP], [dict(PROJ, tauzj=-0.01)], {}),
+    ([POP], [dict(PROJ, taue=0.0)], {}),
+    ([POP], [dict(PROJ, taup=float("inf"))], {}),
+    ([POP], [dict(PROJ, taup=float("nan"))], {}),
+    ([POP], [dict(PROJ, maxfq=0.0)], {}),
+    ([POP], [dict(PROJ, tauepsc=float("inf"))], {}),
+    ([POP], [dict(PROJ, taue=0.0)], dict(fp64_tables=1)),
 ])
 def test_invalid_descriptions_are_rejected(pops, projs, kw):
     args = dict(dt=0.001, max_ticks=16)
@@ -100,3 +112,23 @@ def test_output_buffers_are_checked_before_the_library_writes():
     ro.flags.writeable = False
     with pytest.raises(ValueError):
         capi._out_buffer(ro, np.int32)
+
+
+@pytest.mark.parametrize("prn,old_prn", [(float("inf"), 1.0), (1.0, float("-inf")), (float("nan"), 0.0)])
+def test_non_finite_prn_is_rejected_before_any_launch(prn, old_prn):
+    """bcpnn_run refuses a prn that is not finite before it touches the device
+    (kp = prn dt/taup would be infinite).  Without a GPU the network's creation
+    stops at cudaSetDevice but still hands back a handle; with one it
+    succeeds.  Either way the run returns BCPNN_ERR_INVALID."""
+    lib = capi.load()
+    pops = (capi.PopDesc * 1)(capi.PopDesc(**POP))
+    projs = (capi.ProjDesc * 1)(capi.ProjDesc(**PROJ))
+    desc = capi.NetDesc(1, pops, 1, projs, 0.001, 0, 0.0, 1, 0, 16, 0, 0, 0, 1)
+    h = ctypes.c_void_p()
+    lib.bcpnn_net_create(ctypes.byref(desc), ctypes.byref(h))
+    assert h
+    try:
+        assert lib.bcpnn_run(h, 1, 1, prn, old_prn) == -1
+        assert b"finite" in lib.bcpnn_last_error(h)
+    finally:
+        lib.bcpnn_net_destroy(h)

@@ -9,8 +9,11 @@ import numpy as np
 import pytest
 
 from gsbn_b200 import engine, schema, workloads
+from oracle import sim
 
-REF_DATA = "/root/reference/data"
+# the gsbn source tree ($GSBN_REFERENCE_ROOT, else oracle/Makefile's REF_ROOT);
+# the tests that read its data files skip when it is absent
+REF_DATA = os.path.join(sim.reference_root() or "", "data")
 
 PROCEDURES = {"ProcExtGen", "ProcUpdLazy", "ProcExchangeSpike", "ProcInitConn", "ProcSpkRec", "ProcCheck",
               "ProcSnapshot", "ProcStructuralPlasticity", "ProcUpdMulti"}

@@ -31,7 +31,7 @@ def setup(net):
     di = np.ones(1000, np.int32)
     net.set_conn(0, ii, di)
     net.set_ext_spikes(0, spikes())
-    lg = np.full(100, np.float32(sim.logf(np.array([np.float32(1e-4)]))[0]), np.float32)
+    lg = np.full(100, np.float32(sim.extgen_logf(np.float32(1e-4))), np.float32)
     wm = np.ones(10, np.float32)
     net.set_stimulus(lg, wm)
 

@@ -17,8 +17,8 @@ ARRAYS = ("dsup_0", "act_0", "ada_0", ".counter_0", "epsc_0", "bj_0", "pi_0", "e
 
 
 def lginp_row(row, pops, eps):
-    hit = np.float32(sim.logf(np.array([np.float32(1) + eps], np.float32))[0])
-    miss = np.float32(sim.logf(np.array([np.float32(0) + eps], np.float32))[0])
+    hit = np.float32(sim.extgen_logf(np.float32(1) + eps))
+    miss = np.float32(sim.extgen_logf(np.float32(0) + eps))
     H, M = pops[0]["hcu_num"], pops[0]["mcu_num"]
     return np.array([hit if row[h] == m else miss for h in range(H) for m in range(M)], np.float32)
 

@@ -22,8 +22,8 @@ def test_multi_oracle_runs_config0(tmp_path):
     conn = workloads.read_conn_map(w.conn, pops, projs)
     lgidx, wmask = extgen.stim_tables(schema.read_stim(sp.gen_param.stim_file))
     eps = np.float32(sp.gen_param.eps)
-    hit = np.float32(sim.logf(np.array([np.float32(1) + eps], np.float32))[0])
-    miss = np.float32(sim.logf(np.array([np.float32(0) + eps], np.float32))[0])
+    hit = np.float32(sim.extgen_logf(np.float32(1) + eps))
+    miss = np.float32(sim.extgen_logf(np.float32(0) + eps))
     net = multi.MultiNet(pops, projs, float(np.float32(sp.gen_param.dt)), seed=w.meta["seed"], spike_buffer=25)
     assert np.all(net.read("pij_0") == np.float32(1.0 / 100 / 10))
     assert np.all(net.read("dsup_0") == np.float32(np.log(0.1)))
@@ -44,8 +44,8 @@ def test_multi_oracle_runs_config0(tmp_path):
 
 
 def _lginp(row, pops, eps):
-    hit = np.float32(sim.logf(np.array([np.float32(1) + eps], np.float32))[0])
-    miss = np.float32(sim.logf(np.array([np.float32(0) + eps], np.float32))[0])
+    hit = np.float32(sim.extgen_logf(np.float32(1) + eps))
+    miss = np.float32(sim.extgen_logf(np.float32(0) + eps))
     out, hoff = [], 0
     for p in pops:
         H, M = p["hcu_num"], p["mcu_num"]

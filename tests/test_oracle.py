@@ -13,7 +13,8 @@ from gsbn_b200 import schema, workloads
 from oracle import sim
 from tests.harness import load_workload, schedule
 
-REF = "/root/reference"
+# the gsbn source tree ($GSBN_REFERENCE_ROOT, else oracle/Makefile's REF_ROOT), or None
+REF = sim.reference_root()
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_fixtures.json")
 
 
@@ -143,7 +144,7 @@ def golden():
         return json.load(f)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(REF is None, reason="reference tree not present")
 def test_extgen_expansion_of_reference_prototxts(golden):
     for name, g in golden["prototxt"].items():
         with open(os.path.join(REF, "data", name)) as f:
@@ -153,7 +154,7 @@ def test_extgen_expansion_of_reference_prototxts(golden):
         assert got == g["modes"], name
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(REF is None, reason="reference tree not present")
 def test_conn_map_of_reference_fixtures(golden):
     pops = [dict(hcu_num=400, mcu_num=10)]
     for name, g in golden["conn_map"].items():

@@ -42,8 +42,8 @@ class Pop:
         H, M, N = self.H, self.M, self.N
         R = dsup_prev.shape[0]
         d = self.d
-        hit = sim.logf(np.array([f32(1) + f32(self.eps)]))[0]
-        miss = sim.logf(np.array([f32(0) + f32(self.eps)]))[0]
+        hit = sim.extgen_logf(f32(1) + f32(self.eps))
+        miss = sim.extgen_logf(f32(0) + f32(self.eps))
         m_idx = np.tile(np.arange(M), H)
         h_idx = np.repeat(np.arange(H), M)
         lginp = np.where(lgidx[:, h_idx] == m_idx[None, :], hit, miss).astype(f32)

@@ -29,8 +29,8 @@ NAMES = ("pij_0", "eij_0", "zi2_0", "zj2_0", "tij_0", "wij_0", "pi_0", "ei_0", "
 
 
 def lginp_row(lg, H, M, eps):
-    hit = sim.logf(np.array([np.float32(1) + np.float32(eps)]))[0]
-    miss = sim.logf(np.array([np.float32(0) + np.float32(eps)]))[0]
+    hit = sim.extgen_logf(np.float32(1) + np.float32(eps))
+    miss = sim.extgen_logf(np.float32(0) + np.float32(eps))
     m = np.tile(np.arange(M), H)
     return np.where(lg[np.repeat(np.arange(H), M)] == m, hit, miss).astype(np.float32)
 

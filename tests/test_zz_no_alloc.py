@@ -1,13 +1,17 @@
 """bcpnn_read_state_noalloc, the read for callers that cannot allocate device
-memory (a fully pre-reserved device memory budget, or an open stream
-capture where cudaMalloc is not allowed), against bcpnn_read_state.
+memory (an embedder whose device memory is pre-reserved for its own pool, or
+a loop that must not stall on cudaMalloc/cudaFree), against bcpnn_read_state.
 
 It gathers the interleaved cell fields into a fixed array compiled into the
 library instead of a cudaMalloc'd staging buffer; its results must be the
-same bits as the allocating read, on two calls in a row, whether this file
-runs alone in a fresh process (the first call looks the array up) or after
-the other tests.
+same bits as the allocating read, on two calls in a row.  The first call on a
+device looks the array's address up: test_first_call_in_a_fresh_process
+makes that first call in a new process, whatever ran before in this one.
 """
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -19,7 +23,7 @@ pytestmark = pytest.mark.gpu
 NAMES = ("pij_0", "eij_0", "zi2_0", "zj2_0", "wij_0", "tij_0", "pi_0", "dsup_0", "epsc_0", "spike_0", "si_0")
 
 
-def trained_net(tmp_path, segments):
+def trained_net(tmp_path):
     sp, pops, projs, stim, conn, seed, phz = load_workload(workloads.config0(), str(tmp_path))
     net = capi.Net(pops, projs, 0.001, seed=seed, max_ticks=128)
     for k, (ii, di) in enumerate(conn):
@@ -35,7 +39,7 @@ def same_bits(a, b):
 
 
 def test_noalloc_read_matches_allocating_read(tmp_path):
-    net, runs = trained_net(tmp_path, 4)
+    net, runs = trained_net(tmp_path)
     for r in runs[:3]:
         net.set_stimulus(r.lginp, r.wmask)
         net.run(r.first, r.n, r.prn, r.old_prn)
@@ -70,3 +74,28 @@ def test_noalloc_read_rejects_fields_beyond_the_static_array():
     assert net.read("pij_0").size == 1100000
     assert same_bits(net.read_noalloc("wij_0"), net.read("wij_0"))
     net.close()
+
+
+FRESH = """
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from tests.test_zz_no_alloc import NAMES, same_bits, trained_net
+net, runs = trained_net(sys.argv[2])
+for r in runs[:2]:
+    net.set_stimulus(r.lginp, r.wmask)
+    net.run(r.first, r.n, r.prn, r.old_prn)
+for n in NAMES:
+    a, b, ref = net.read_noalloc(n), net.read_noalloc(n), net.read(n)
+    assert same_bits(a, ref) and same_bits(b, ref), n
+net.close()
+print("fresh ok")
+"""
+
+
+def test_first_call_in_a_fresh_process(tmp_path):
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", FRESH, root, str(tmp_path)], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "fresh ok" in out.stdout
