@@ -115,6 +115,19 @@ def test_config2_two_projections_poisson(tmp_path, mode):
     assert orc.counters() == gpu.counters()
 
 
+def test_config2_full_size(tmp_path, mode):
+    """The two-population workload at its real size: 50 patterns, 5,000
+    ticks, in every launch mode."""
+    sp, pops, projs, orc, gpu, runs = make_pair(workloads.config2(), tmp_path, per_tick=mode)
+    try:
+        assert sum(r.n for r in runs) == 5000
+        n = compare_runs(pops, projs, orc, gpu, runs, full_every_run=False)
+        assert n > 1000
+        assert orc.counters() == gpu.counters()
+    finally:
+        gpu.close()
+
+
 def test_reduced_100x100(tmp_path, mode):
     w = workloads.small_scale(hcu=24, mcu=20, src=6, n_patterns=8, train_ticks=50, recall_ticks=30)
     sp, pops, projs, orc, gpu, runs = make_pair(w, tmp_path, per_tick=mode)
