@@ -19,11 +19,19 @@ device with their per-HCU results read back; all of it is queued behind the
 runs, with one synchronisation per step.  The network state (~0.25 GB) is larger than L2, so no flush is
 needed between steps.
 
---impl reference times the CPU oracle (a restatement of gsbn's
-single-threaded ProcUpdLazy CPU path; the reference itself cannot be built
-here) on a bounded sample of the same workload.
+--impl reference times gsbn's own CPU kernels (update_*_kernel_cpu of
+ProcUpdLazy, compiled from the gsbn sources into oracle/_ref and driven by the
+oracle's loops, single-threaded like gsbn's CPU path) over the whole step:
+the schedule is cut into warmup + steps contiguous windows and the timed
+windows cover everything after the warm-up ones.  The in-line cpu_baseline
+times the same kernels on windows spread over the schedule (early, middle
+and late segments of both phases), started from the device's state at each
+window.  `parity` compares the device's spike logs of one end-to-end step,
+segment by segment, with digests of gsbn's kernels running the same step
+(tests/golden/config1_spike_digests.json).
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -153,7 +161,7 @@ def algorithmic_bytes(pops, projs, row_cells, col_cells, ticks):
     return 44 * row_cells + 40 * col_cells + per_tick * ticks
 
 
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, rank, world, local_rank, cpu=False):
     import torch
     from gsbn_b200 import capi
     dev = local_rank
@@ -264,6 +272,18 @@ def run_ours(args, rank, world, local_rank):
     e_s = time.perf_counter() - t0
     e_cells = sum(net.counters()) - e0
     e_s, e_cells = combine_over_ranks(e_s, e_cells, f"cuda:{dev}")
+    # every e2e step is the same pass from the initial state: its spike logs
+    # are the step's spike trains
+    parity = spike_parity(pin_log)
+    cpu_base = None
+    if cpu:
+        n = len(runs)
+        first_recall = next(i for i, r in enumerate(runs) if r.prn == 0.0)
+        picks = sorted({0, first_recall // 2, first_recall - 1, first_recall, (first_recall + n) // 2, n - 1})
+        states = capture_states(net, runs, picks)
+        v, kind, sample, _ = cpu_spread_sample(sp, pops, projs, seed, runs, states, cells / args.steps / world)
+        cpu_base = {"value": v, "unit": "cell updates/s", "cores": 1, "kind": kind, "sample": sample,
+                    "cpu": cpu_model()}
 
     out = None
     if rank == 0:
@@ -285,6 +305,7 @@ def run_ours(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "state 0.25 GB > 126 MB L2, no flush"},
             "ticks_per_s": n_ticks * args.steps * world / (ms / 1e3),
+            "parity": parity,
             "recall": f"{recall[0]}/{recall[1]}",
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "tick_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
@@ -297,6 +318,8 @@ def run_ours(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h, "ms_per_step": e_s * 1e3 / args.steps},
             "clocks": clk.summary(),
         }
+        if cpu_base is not None:
+            out["cpu_baseline"] = cpu_base
     net.close()
     return out
 
@@ -632,24 +655,125 @@ def _phase_sample(orc, runs, sample_ticks):
     return (c_tr + c_rc) / (t_tr + t_rc), n_tr, n_rc, s_tr + s_rc
 
 
-def cpu_sample(sample_ticks=600):
-    """The oracle on a bounded sample of the workload: the first
-    `sample_ticks` training ticks (with the start-of-run all-cells pass), then
-    the training->recall all-cells catch-up and `sample_ticks // 2` recall
-    ticks.  Returns cells/s scaled to the full step by the phase rates."""
-    from gsbn_b200 import workloads
+GOLDEN_DIGESTS = os.path.join(ROOT, "tests", "golden", "config1_spike_digests.json")
+ORACLE_POP = ("dsup", "act", "epsc", "bj", "spike", ".counter")
+ORACLE_PROJ = ("ii", "di", "qi", "ti", "tij", "pi", "ei", "zi", "pj", "ej", "zj", "pij", "eij", "zi2", "zj2", "wij",
+               "si", ".siq")
+
+
+def reference_oracle(pops, projs, dt, seed):
+    """gsbn's own CPU kernels (oracle/_ref, math MATH_REF) when that build
+    exists, else the restatement with glibc math (MATH_LIBM, bit-identical to
+    them in the CPU tests).  Returns (oracle network, kind, math description)."""
     from oracle import sim
-    from tests.harness import load_workload, schedule
-    work = tempfile.mkdtemp(prefix="gsbn_cpu_")
-    sp, pops, projs, stim, conn, seed, phz = load_workload(workloads.config1(), work)
-    orc = sim.OracleNet(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed)
-    for k, (ii, di) in enumerate(conn):
-        orc.set_conn(k, ii, di)
-    runs = schedule(sp, stim, pops, orc.logf)
-    v, n_tr, n_rc, secs = _phase_sample(orc, runs, sample_ticks)
-    sample = (f"{n_tr} training ticks + {n_rc} recall ticks of the 100x100 workload, including both all-cells "
-              f"catch-ups, {secs:.1f} s of CPU; per-tick rates scaled to the 2e4-tick step")
-    return v, sample, secs
+    if sim.ref_available():
+        return (sim.OracleNet(pops, projs, dt, seed=seed, math=sim.MATH_REF), "reference",
+                "gsbn's update_*_kernel_cpu compiled from its sources (oracle/_ref), glibc expf/logf, 1 thread")
+    return (sim.OracleNet(pops, projs, dt, seed=seed, math=sim.MATH_LIBM), "port",
+            "oracle restatement with glibc expf/logf (oracle/_ref not built), 1 thread")
+
+
+def host_runs(sp, pops, runs):
+    """(first, n, prn, old_prn, lginp, wmask) per segment, with ProcExtGen's
+    lginp values from the host's float log, as gsbn computes them"""
+    from gsbn_b200 import extgen, schema
+    from oracle import sim
+    lgidx, wmask = extgen.stim_tables(schema.read_stim(sp.gen_param.stim_file))
+    eps = np.float32(sp.gen_param.eps)
+    H, M = pops[0]["hcu_num"], pops[0]["mcu_num"]
+    hit, miss = sim.extgen_logf(np.float32(1) + eps), sim.extgen_logf(np.float32(0) + eps)
+    return [(r.first, r.n, r.prn, r.old_prn, _lginp_row(lgidx[r.lgidx], H, M, hit, miss), wmask[r.wmask][:H])
+            for r in runs]
+
+
+def capture_states(net, runs, picks):
+    """The device state at the start of each picked segment, from one more
+    pass of the step (outside every timed region)."""
+    names = [f"{k}_0" for k in ORACLE_POP + ORACLE_PROJ]
+    net.reset()
+    states = {}
+    for i, r in enumerate(runs):
+        if i in picks:
+            net.sync()
+            states[i] = {n: net.read(n) for n in names}
+        net.use_stimulus(r.lgidx, r.wmask)
+        net.run(r.first, r.n, r.prn, r.old_prn)
+    net.sync()
+    return states
+
+
+def cpu_spread_sample(sp, pops, projs, seed, runs, states, cells_per_step):
+    """gsbn's kernels on one core, on windows spread over the schedule: each
+    picked segment is run from the device's state at its start.  A segment
+    whose prn differs from the previous one carries the all-cells catch-up in
+    its first tick, which is timed alone.  The step's CPU time is estimated as
+    the catch-up ticks as measured plus the mean per-tick time of each phase
+    times that phase's other ticks; the value is the device-counted cells of a
+    step over that time.  Returns (cells/s, kind, sample description, seconds
+    spent)."""
+    orc, kind, math = reference_oracle(pops, projs, float(np.float32(sp.gen_param.dt)), seed)
+    hr = host_runs(sp, pops, runs)
+    per_tick = {True: [0.0, 0], False: [0.0, 0]}   # training?: [seconds, ticks]
+    switch = {True: [], False: []}
+    spent = 0.0
+    for i in sorted(states):
+        for name, a in states[i].items():
+            orc.write(name, a)
+        first, n, prn, old_prn, lg, wm = hr[i]
+        orc.set_stimulus(lg, wm)
+        train = prn != 0.0
+        t0 = time.perf_counter()
+        orc.run(first, 1, prn, old_prn, spikes=False)
+        t1 = time.perf_counter()
+        orc.run(first + 1, n - 1, prn, prn, spikes=False)
+        t2 = time.perf_counter()
+        if prn != old_prn:
+            switch[train].append(t1 - t0)
+            per_tick[train][0] += t2 - t1
+            per_tick[train][1] += n - 1
+        else:
+            per_tick[train][0] += t2 - t0
+            per_tick[train][1] += n
+        spent += t2 - t0
+    est = 0.0
+    for train in (True, False):
+        rs = [r for r in runs if (r.prn != 0.0) == train]
+        n_sw = sum(1 for r in rs if r.prn != r.old_prn)
+        ticks = sum(r.n for r in rs)
+        sw = statistics.mean(switch[train]) if switch[train] else 0.0
+        est += n_sw * sw + per_tick[train][0] / max(1, per_tick[train][1]) * (ticks - n_sw)
+    picks = sorted(states)
+    sample = (f"{math}; {len(picks)} segments of the step (indices {picks}, "
+              f"{sum(runs[i].n for i in picks)} ticks: early, middle and late training and recall, each started "
+              f"from the device's state, catch-up ticks timed alone), {spent:.1f} s of CPU; step time = catch-ups "
+              f"+ per-phase tick time x phase ticks; value = device-counted cells per step / that time")
+    return cells_per_step / est, kind, sample, spent
+
+
+def spike_parity(pin_logs, path=GOLDEN_DIGESTS):
+    """The device's spike logs of one end-to-end step, segment by segment,
+    against the digests of gsbn's kernels running the same step."""
+    try:
+        with open(path) as f:
+            gold = json.load(f)
+    except OSError as e:
+        return {"status": "unchecked", "why": str(e)}
+    segs = gold["segments"]
+    if len(segs) != len(pin_logs):
+        return {"status": "unchecked", "why": f"{len(segs)} golden segments, {len(pin_logs)} device segments"}
+    same, first_bad = 0, None
+    for k, (g, log) in enumerate(zip(segs, pin_logs)):
+        if hashlib.sha256(np.ascontiguousarray(log).tobytes()).hexdigest() == g["sha256"]:
+            same += 1
+        elif first_bad is None:
+            got = int(np.unpackbits(log.view(np.uint8)).sum())
+            first_bad = {"segment": k, "first_tick": g["first"], "device_spikes": got, "reference_spikes": g["spikes"]}
+    out = {"status": "identical" if same == len(segs) else "differs", "segments_identical": f"{same}/{len(segs)}",
+           "ticks": gold["ticks"], "reference_spikes": gold["spikes"], "against": gold["math"],
+           "digests": "tests/golden/config1_spike_digests.json"}
+    if first_bad:
+        out["first_difference"] = first_bad
+    return out
 
 
 def cpu_multi_sample(ring, sample_ticks=1200):
@@ -665,8 +789,7 @@ def cpu_multi_sample(ring, sample_ticks=1200):
     orc = multi.MultiNetC(pops, projs, float(np.float32(sp.gen_param.dt)), seed=seed, spike_buffer=ring)
     for k, (ii, di) in enumerate(conn):
         orc.set_conn(k, ii, di)
-    lib = sim.load()
-    runs = schedule(sp, stim, pops, lambda x: lib.oracle_logf(sim.MATH_SHARED, float(x)))
+    runs = schedule(sp, stim, pops, sim.extgen_logf)
     v, n_tr, n_rc, secs = _phase_sample(orc, runs, sample_ticks)
     sample = (f"{n_tr} training ticks + {n_rc} recall ticks, including both all-cells catch-ups, {secs:.1f} s "
               f"on 1 core; per-tick rates scaled to the 2e4-tick step")
@@ -766,25 +889,65 @@ def cpu_recall_sample(pops, projs, dt, poisson_hz, state, lg_row, wm_row, eps, t
     return ticks / per_rep, sample
 
 
+def cut_windows(hruns, n_win):
+    """The runs (first, n, prn, old_prn, lginp, wmask) of a schedule cut into
+    n_win contiguous windows of equal tick counts; a run split across windows
+    continues with old_prn = prn, as one run of ticks does.  Returns (windows,
+    tick bounds)."""
+    total = sum(r[1] for r in hruns)
+    bounds = [round(total * k / n_win) for k in range(n_win + 1)]
+    windows = [[] for _ in range(n_win)]
+    t = 0
+    for first, n, prn, old_prn, lg, wm in hruns:
+        k = 0
+        while k < n:
+            win = max(i for i in range(n_win) if bounds[i] <= t)
+            take = min(n - k, bounds[win + 1] - t)
+            windows[win].append((first + k, take, prn, old_prn if k == 0 else prn, lg, wm))
+            k += take
+            t += take
+    return windows, bounds
+
+
 def run_reference(args):
-    """The reference arm: the single-threaded CPU path (oracle restatement)."""
-    vals = []
-    for _ in range(args.warmup):
-        cpu_sample(args.ref_ticks)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, sample, _ = cpu_sample(args.ref_ticks)
-        vals.append(v)
-    elapsed = time.perf_counter() - t0
-    value = statistics.mean(vals)
+    """The reference arm: gsbn's own CPU kernels (reference_oracle), one
+    thread like gsbn's ProcUpdLazy CPU path, on the same workload.  The step's
+    2e4-tick schedule is cut into warmup + steps contiguous windows of equal
+    tick counts; the warm-up windows run untimed and the timed windows cover
+    the rest of the schedule, training->recall catch-up included.  value =
+    cells the timed windows updated / their time."""
+    from gsbn_b200 import workloads
+    work = tempfile.mkdtemp(prefix="gsbn_ref_")
+    w, sp, pops, projs, stim, conn, runs = build_schedule(work)
+    orc, kind, math = reference_oracle(pops, projs, float(np.float32(sp.gen_param.dt)), w.meta["seed"])
+    for k, (ii, di) in enumerate(conn):
+        orc.set_conn(k, ii, di)
+    total = sum(r.n for r in runs)
+    n_win = args.warmup + args.steps
+    windows, bounds = cut_windows(host_runs(sp, pops, runs), n_win)
+    secs, cells = [], []
+    for i, win in enumerate(windows):
+        c0, t0 = sum(orc.counters()), time.perf_counter()
+        for first, n, prn, old_prn, lg, wm in win:
+            orc.set_stimulus(lg, wm)
+            orc.run(first, n, prn, old_prn, spikes=False)
+        if i >= args.warmup:
+            secs.append(time.perf_counter() - t0)
+            cells.append(sum(orc.counters()) - c0)
+    value = sum(cells) / sum(secs)
+    timed_ticks = total - bounds[args.warmup]
+    sample = (f"{math}; ticks {bounds[args.warmup] + 1}..{total} of the 2e4-tick step in {args.steps} contiguous "
+              f"windows of ~{total // n_win} ticks ({sum(secs):.1f} s timed) after {args.warmup} untimed warm-up "
+              f"windows; value = cells updated / time over the timed windows")
     return {
         "metric": "synaptic updates/s", "value": value, "unit": "cell updates/s", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(secs) * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded patterns and connectivity, gen_rnd.py conventions)", "impl": "reference",
         "config": {"workload": "100x100 HCU/MCU, recurrent HCU density 0.1 (C=1000, 1e7 cells), 100 patterns: "
-                               "1e4 training + 1e4 recall ticks per step"},
-        "cpu_baseline": {"value": value, "unit": "cell updates/s", "cores": 1, "kind": "port", "sample": sample,
+                               "1e4 training + 1e4 recall ticks per step",
+                   "ticks_timed": timed_ticks},
+        "cpu_baseline": {"value": value, "unit": "cell updates/s", "cores": 1, "kind": kind, "sample": sample,
                          "cpu": cpu_model()},
         "e2e": {"value": value, "unit": "cell updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -807,8 +970,6 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-ticks", type=int, default=400)
-    ap.add_argument("--cpu-ticks", type=int, default=3600)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extensions", action="store_true")
     ap.add_argument("--only-extensions", action="store_true", help="run the extension workloads alone (profiling)")
@@ -836,7 +997,7 @@ def main():
                    "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
             print(json.dumps({"extensions": ext}), flush=True)
         return
-    out = run_ours(args, rank, world, local_rank)
+    out = run_ours(args, rank, world, local_rank, cpu=cpu)
     # the extensions are single-GPU measurements: under torchrun the other
     # ranks would hold their GPUs at the final barrier while rank 0 runs them
     if rank == 0 and world == 1 and not args.no_extensions:
@@ -845,10 +1006,6 @@ def main():
                              "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
                              "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            v, sample, secs = cpu_sample(args.cpu_ticks)
-            out["cpu_baseline"] = {"value": v, "unit": "cell updates/s", "cores": 1, "kind": "port",
-                                   "sample": sample, "cpu": cpu_model()}
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch

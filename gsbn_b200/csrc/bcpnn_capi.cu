@@ -408,7 +408,9 @@ bool resolve(const bcpnn_net* net, const char* cname, Resolved* r) {
     if (base == "epsc") return parity(D.epsc[0], D.epsc[1], n * P.dim_proj);
     if (base == "bj") return parity(D.bj[0], D.bj[1], n * P.dim_proj);
     if (base == "act") return plain(D.act, BCPNN_F32, n);
-    if (base == "spike") return plain(D.spike, BCPNN_I8, n);
+    /* ProcUpdMulti's spike_<pop> is its ring of spike buffer size ticks, slot
+       simstep % size (ProcUpdMulti/Pop.cpp:69,329) */
+    if (base == "spike") return D.ring ? plain(D.ring, BCPNN_I8, n * (size_t)D.ring_len) : plain(D.spike, BCPNN_I8, n);
     if (base == ".counter") return plain(D.counter, BCPNN_I32, n);
     if (base == "ada" && D.ada) return plain(D.ada, BCPNN_F32, n);
   }
@@ -1554,7 +1556,7 @@ bool resolve_noalloc(const bcpnn_net* net, const char* name, Resolved* r) {
     if (is("epsc")) return parity(D.epsc[0], D.epsc[1], n * P.dim_proj);
     if (is("bj")) return parity(D.bj[0], D.bj[1], n * P.dim_proj);
     if (is("act")) return plain(D.act, BCPNN_F32, n);
-    if (is("spike")) return plain(D.spike, BCPNN_I8, n);
+    if (is("spike")) return D.ring ? plain(D.ring, BCPNN_I8, n * (size_t)D.ring_len) : plain(D.spike, BCPNN_I8, n);
     if (is(".counter")) return plain(D.counter, BCPNN_I32, n);
     if (is("ada") && D.ada) return plain(D.ada, BCPNN_F32, n);
   }

@@ -229,6 +229,8 @@ class Database {
   /* population / projection shapes as the network was built (ProcUpdLazy) */
   std::vector<bcpnn_pop_desc> pops;
   std::vector<bcpnn_proj_desc> projs;
+  /* 0: ProcUpdLazy, 1: ProcUpdMulti (the vectors each creates differ) */
+  int update_variant = 0;
 
   /* vectors of a restored snapshot (SolverState), by gsbn name; consumed by
      init_copy */

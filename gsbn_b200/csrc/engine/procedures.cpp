@@ -380,6 +380,7 @@ class ProcUpdLazy : public ProcedureBase {
     desc.device = device;
     desc.max_ticks_per_run = _max_ticks;
     desc.update_variant = variant;
+    db.update_variant = variant;
     if (variant == 1) {
       int ring = 1; /* ProcUpdMulti/Pop.cpp:31-36 */
       if (par.argi("spike buffer size", ring) && ring <= 0) fatal("ProcUpdMulti: spike buffer size must be > 0");
@@ -904,21 +905,47 @@ class ProcSnapshot : public ProcedureBase {
     _glv.getf("dt", dt);
     _glv.getf("prn", prn);
     std::vector<std::pair<std::string, Database::StateVec>> vecs;
-    static const char* pop_names[] = {"dsup", "act", "spike", "epsc", "bj"};
-    static const char* proj_names[] = {"ii", "di", "qi", "pi", "ei", "zi", "ti", "pj", "ej", "zj",
-                                       "pij", "eij", "zi2", "zj2", "tij", "wij", "si"};
+    /* the non-'.' vectors each variant's Pop/Proj create: ProcUpdLazy/Pop.cpp:
+       47-52, Proj.cpp:64-83; ProcUpdMulti/Pop.cpp:54-59, Proj.cpp:63-80 (no
+       per-cell zi2 or tij) */
+    static const char* pop_names[] = {"dsup", "act", "ada", "spike", "epsc", "bj"};
+    static const char* lazy_proj[] = {"ii", "di", "qi", "pi", "ei", "zi", "ti", "pj", "ej", "zj",
+                                      "pij", "eij", "zi2", "zj2", "tij", "wij", "si"};
+    static const char* multi_proj[] = {"ii", "di", "qi", "pi", "ei", "zi", "ti", "pj", "ej", "zj",
+                                       "pij", "eij", "zj2", "wij", "si"};
+    const bool multi = _db->update_variant == 1;
     auto add = [&](const std::string& name) {
       Database::StateVec v;
       v.bytes = _db->read_state(name, &v.type);
       vecs.emplace_back(name, std::move(v));
     };
     for (size_t p = 0; p < _db->pops.size(); p++)
-      for (const char* n : pop_names) add(std::string(n) + "_" + std::to_string(p));
-    for (size_t q = 0; q < _db->projs.size(); q++)
-      for (const char* n : proj_names) add(std::string(n) + "_" + std::to_string(q));
-    /* gsbn iterates its name-sorted vector map ("<name>_<type>") */
-    std::sort(vecs.begin(), vecs.end(), [](const std::pair<std::string, Database::StateVec>& a,
-                                           const std::pair<std::string, Database::StateVec>& b) { return a.first < b.first; });
+      for (const char* n : pop_names) {
+        std::string name = std::string(n) + "_" + std::to_string(p);
+        if (!multi && std::strcmp(n, "ada") == 0) {
+          /* ProcUpdLazy creates ada_<pop> and never updates it (its lines
+             are commented out, Pop.cpp:258,322): H*M zeros */
+          Database::StateVec v;
+          v.type = BCPNN_F32;
+          v.bytes.assign((size_t)_db->pops[p].hcu_num * _db->pops[p].mcu_num * sizeof(float), 0);
+          vecs.emplace_back(name, std::move(v));
+        } else {
+          add(name);
+        }
+      }
+    for (size_t q = 0; q < _db->projs.size(); q++) {
+      if (multi)
+        for (const char* n : multi_proj) add(std::string(n) + "_" + std::to_string(q));
+      else
+        for (const char* n : lazy_proj) add(std::string(n) + "_" + std::to_string(q));
+    }
+    /* gsbn iterates its vector map, keyed "<name>_<type>" (Database.cpp:
+       260-290): sort by that key, so "pi_10" comes before "pi_1" as there */
+    auto key = [](const std::pair<std::string, Database::StateVec>& a) {
+      return a.first + (a.second.type == BCPNN_I8 ? "_i08" : a.second.type == BCPNN_I32 ? "_i32" : "_f32");
+    };
+    std::sort(vecs.begin(), vecs.end(), [&](const std::pair<std::string, Database::StateVec>& a,
+                                            const std::pair<std::string, Database::StateVec>& b) { return key(a) < key(b); });
     std::string bytes = encode_solver_state(simstep * dt, prn, vecs);
     std::string path = _dir + "/Snapshot_" + std::to_string(simstep * dt) + ".bin";
     std::ofstream o(path, std::ios::out | std::ios::trunc | std::ios::binary);

@@ -158,6 +158,71 @@ def test_snapshot_and_restore(tmp_path):
     assert len(after) > 50
 
 
+def test_snapshot_and_restore_procupdmulti(tmp_path):
+    """ProcSnapshot of a ProcUpdMulti network holds the vectors gsbn's
+    ProcUpdMulti creates: ada_<pop> (its adaptation current) and the spike ring
+    spike_<pop> (spike buffer size x H x M), no per-cell zi2 or tij
+    (ProcUpdMulti/Pop.cpp:54-69, Proj.cpp:63-80).  Restored with -s, the run
+    continues the uninterrupted spike train, adaptation included."""
+    dt = np.float32(0.001)
+    t_snap = 1650
+    ring = 25
+
+    def multi(text):
+        text = text.replace('name: "ProcUpdLazy"', 'name: "ProcUpdMulti"\n  argi { key: "spike buffer size" val: %d }'
+                            % ring)
+        return text
+
+    def with_snapshot(text):
+        return multi(text) + f'proc_param {{ name: "ProcSnapshot" argi {{ key: "period" val: {t_snap} }} ' \
+                             f'argi {{ key: "offset" val: {t_snap} }} }}\n'
+
+    w = workloads.config0()
+    path, sp = write(w, tmp_path / "full", with_snapshot)
+    run(path)
+    snap_dir = os.path.join(sp.rec_param.directory, "ProcSnapshot")
+    names = os.listdir(snap_dir)
+    assert len(names) == 1 and names[0].startswith("Snapshot_1.65")
+    st = schema.SolverState()
+    with open(os.path.join(snap_dir, names[0]), "rb") as f:
+        st.ParseFromString(f.read())
+    f32 = {v.name: np.array(v.data, np.float32) for v in st.vector_state_f32}
+    i8 = {v.name: np.array(v.data, np.int8) for v in st.vector_state_i8}
+    i32 = {v.name for v in st.vector_state_i32}
+    assert "ada_0" in f32 and np.any(f32["ada_0"] != 0)
+    assert i8["spike_0"].size == ring * 100 and i8["spike_0"].sum() > 0
+    assert "zi2_0" not in f32 and "tij_0" not in i32 and "pij_0" in f32
+    path2, sp2 = write(w, tmp_path / "restored", multi)
+    run(path2, snapshot=os.path.join(snap_dir, names[0]))
+    full = rec_files(sp)["ProcSpkRec/spk_pop_0.csv"].splitlines()
+    rest = rec_files(sp2)["ProcSpkRec/spk_pop_0.csv"].splitlines()
+    after = [l for l in full[1:] if int(l.split(",")[0]) > t_snap]
+    assert rest[0] == full[0]
+    assert rest[1:] == after
+    assert len(after) > 50
+
+
+def test_snapshot_lists_gsbn_vectors_in_key_order(tmp_path):
+    """A ProcUpdLazy snapshot holds ada_<pop> (H x M zeros: gsbn creates it
+    and never updates it) and lists each type's vectors in the order of gsbn's
+    map keys "<name>_<type>" (Database.cpp:257-295)."""
+    t_snap = 400
+    w = workloads.config0()
+    path, sp = write(w, tmp_path, lambda text: text + f'proc_param {{ name: "ProcSnapshot" argi {{ key: "period" '
+                                                      f'val: {t_snap} }} argi {{ key: "offset" val: {t_snap} }} }}\n')
+    run(path)
+    snap_dir = os.path.join(sp.rec_param.directory, "ProcSnapshot")
+    st = schema.SolverState()
+    with open(os.path.join(snap_dir, os.listdir(snap_dir)[0]), "rb") as f:
+        st.ParseFromString(f.read())
+    for vs, suffix in ((st.vector_state_f32, "_f32"), (st.vector_state_i32, "_i32"), (st.vector_state_i8, "_i08")):
+        keys = [v.name + suffix for v in vs]
+        assert keys == sorted(keys)
+    f32 = {v.name: np.array(v.data, np.float32) for v in st.vector_state_f32}
+    assert f32["ada_0"].size == 100 and not f32["ada_0"].any()
+    assert {"zi2_0", "pij_0", "wij_0"} <= set(f32)
+
+
 def test_gsbn_sim_command(tmp_path):
     path, sp = write(workloads.config0(), tmp_path)
     r = subprocess.run([GSBN_SIM, "-n", path, "-m", "GPU"], capture_output=True, text=True, timeout=300)
