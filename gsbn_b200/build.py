@@ -46,26 +46,29 @@ def _stale(obj, src, force):
     return any(os.path.getmtime(f) > t for f in [src, __file__] + _headers())
 
 
-def build(verbose_ptxas=False, force=False):
+def build(verbose_ptxas=False, force=False, probe=False):
+    """probe: a second library, libgsbn_b200_probe.so, with the tick kernel's
+    phase probe compiled in (-DBCPNN_PHASE_PROBE); the default build has none."""
     nvcc = os.environ.get("NVCC", "nvcc")
-    objdir = os.path.join(HERE, "_build")
+    objdir = os.path.join(HERE, "_build_probe" if probe else "_build")
+    flags = ["-DBCPNN_PHASE_PROBE"] if probe else []
     os.makedirs(objdir, exist_ok=True)
     objs = []
     for src in sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         extra = ["-Xptxas", "-v"] if verbose_ptxas else []
         if _stale(obj, src, force or verbose_ptxas):
-            _run([nvcc] + ARCH + COMMON + PLAIN + extra + ["-c", src, "-o", obj])
+            _run([nvcc] + ARCH + COMMON + PLAIN + flags + extra + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in _sources("engine", ".cpp"):
         obj = os.path.join(objdir, "engine_" + os.path.basename(src) + ".o")
         if _stale(obj, src, force):
-            _run([nvcc] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", "-c", src, "-o", obj])
+            _run([nvcc] + COMMON + flags + ["-Wno-deprecated-gpu-targets", "-x", "c++", "-c", src, "-o", obj])
         objs.append(obj)
-    lib = os.path.join(HERE, "libgsbn_b200.so")
+    lib = os.path.join(HERE, "libgsbn_b200_probe.so" if probe else "libgsbn_b200.so")
     _run([nvcc] + ARCH + ["-shared", "-o", lib] + objs + ["-cudart", "static"])
     main = os.path.join(CSRC, "engine", "main", "gsbn_sim.cpp")
-    if os.path.exists(main):
+    if os.path.exists(main) and not probe:
         exe = os.path.join(HERE, "gsbn_sim")
         _run([nvcc] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", main, "-o", exe, "-L" + HERE, "-lgsbn_b200",
                                 "-Xlinker", "-rpath=$ORIGIN"])
@@ -73,4 +76,4 @@ def build(verbose_ptxas=False, force=False):
 
 
 if __name__ == "__main__":
-    build(verbose_ptxas="-v" in sys.argv, force="--force" in sys.argv)
+    build(verbose_ptxas="-v" in sys.argv, force="--force" in sys.argv, probe="--probe" in sys.argv)

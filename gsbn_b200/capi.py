@@ -10,7 +10,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgsbn_b200.so")
+# the library; GSBN_B200_LIB selects another build of it (the phase-probe
+# build, gsbn_b200/libgsbn_b200_probe.so)
+LIB_PATH = os.environ.get("GSBN_B200_LIB") or os.path.join(_HERE, "libgsbn_b200.so")
 
 F32, I32, I8 = 0, 1, 2
 _NP = {F32: np.float32, I32: np.int32, I8: np.int8}
@@ -22,7 +24,8 @@ EXPORTS = (
     "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_spike_log_async", "bcpnn_check_count",
     "bcpnn_check_result_async", "bcpnn_get_ss_flags",
     "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_read_state_noalloc", "bcpnn_counters", "bcpnn_kernel_launches",
-    "bcpnn_selftest_barrier_timeout", "bcpnn_selftest_division", "bcpnn_set_pop_rng", "bcpnn_prune", "bcpnn_last_error",
+    "bcpnn_selftest_barrier_timeout", "bcpnn_selftest_division", "bcpnn_phase_probe", "bcpnn_set_pop_rng", "bcpnn_prune",
+    "bcpnn_last_error",
     "bcpnn_status_string",
 )
 
@@ -82,6 +85,7 @@ def load():
         "bcpnn_reset": (ctypes.c_int, [vp]),
         "bcpnn_get_stream": (ctypes.c_int, [vp, P(vp)]),
         "bcpnn_run": (ctypes.c_int, [vp, i32, i32, ctypes.c_float, ctypes.c_float]),
+        "bcpnn_phase_probe": (ctypes.c_int, [vp, vp, i32, P(i32), i32]),
         "bcpnn_sync": (ctypes.c_int, [vp]),
         "bcpnn_spike_log_words": (ctypes.c_int, [vp, i32, P(i32)]),
         "bcpnn_get_spike_log": (ctypes.c_int, [vp, i32, vp, sz]),
@@ -211,6 +215,15 @@ class Net:
     def run(self, first_simstep, n_ticks, prn, old_prn):
         self._check(self._lib.bcpnn_run(self._h, first_simstep, n_ticks, prn, old_prn))
         self.last_ticks = n_ticks
+
+    def phase_probe(self, reset=True):
+        """uint64 [CTAs, 32] tick-kernel phase counters (library built with
+        BCPNN_PHASE_PROBE; see bcpnn_phase_probe)"""
+        n = ctypes.c_int32()
+        self._check(self._lib.bcpnn_phase_probe(self._h, None, 0, ctypes.byref(n), 0))
+        out = np.zeros((n.value, 32), np.uint64)
+        self._check(self._lib.bcpnn_phase_probe(self._h, _ptr(out), n.value, ctypes.byref(n), 1 if reset else 0))
+        return out
 
     def sync(self):
         self._check(self._lib.bcpnn_sync(self._h))

@@ -56,7 +56,8 @@ struct TableSlot {
   uint32_t kp_bits = 0;
   int len = 0;   /* valid entries */
   int cap = 0;   /* allocated entries */
-  float4* ptr = nullptr;
+  float4* ptr = nullptr;    /* cap * 4 float4, then cap * 4 double2 reciprocals (one allocation) */
+  double2* rptr = nullptr;
   uint64_t stamp = 0;
 };
 
@@ -181,6 +182,20 @@ int check_device_error(bcpnn_net* net) {
 
 /* (re)build the decay table of slot s of projection p for kp = taupdt*prn
    with at least `need` entries */
+/* the reciprocals of the constant divisors for kp = taupdt*prn; the divisors
+   are the float expressions of make_coef (host float arithmetic without
+   contraction gives the same bits), the reciprocals IEEE double divisions */
+RCoef rcoef(const ProjDev& D, float prn) {
+  const float kp = D.taupdt * prn;
+  RCoef r;
+  r.Dekp = 1.0 / (double)(D.ke - kp);
+  r.D2 = 1.0 / (double)((D.kzi - kp) + D.kzj);
+  r.D3 = 1.0 / (double)((D.kzi - D.ke) + D.kzj);
+  r.Dpzi = 1.0 / (double)(kp - D.kzi);
+  r.Dezi = 1.0 / (double)(D.ke - D.kzi);
+  return r;
+}
+
 int fill_slot(bcpnn_net* net, int p, int s, float prn, int need) {
   ProjHost& J = net->projs[p];
   const ProjDev& D = net->hq[p];
@@ -192,13 +207,15 @@ int fill_slot(bcpnn_net* net, int p, int s, float prn, int need) {
     while (cap < need) cap *= 2;
     if (T.ptr) CU(cudaFree(T.ptr));
     T.ptr = nullptr;
-    CU(cudaMalloc((void**)&T.ptr, (size_t)cap * 4 * sizeof(float4)));
+    T.rptr = nullptr;
+    CU(cudaMalloc((void**)&T.ptr, (size_t)cap * 4 * (sizeof(float4) + sizeof(double2))));
+    T.rptr = (double2*)(T.ptr + (size_t)cap * 4);
     T.cap = cap;
   }
   if (D.fp64)
     build_table_fp64_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.cap, kp, D.ke, D.kzi, D.kzj);
   else
-    build_table_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.cap, kp, D.ke, D.kzi, D.kzj);
+    build_table_kernel<<<grid_for(T.cap, 256), 256, 0, net->stream>>>(T.ptr, T.rptr, T.cap, kp, D.ke, D.kzi, D.kzj);
   CU(cudaGetLastError());
   net->launches++;
   T.kp_bits = bx_fbits(kp);
@@ -1117,6 +1134,8 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     if ((rc = prepare_tables(net, p, prn, old_prn, with_all, need, first_simstep + 1, &s, &so))) return rc;
     const ProjHost& J = net->projs[p];
     net->tabs[p].tab = J.slot[s].ptr;
+    net->tabs[p].rtab = J.slot[s].rptr;
+    net->tabs[p].rk = rcoef(net->hq[p], prn);
     net->tabs[p].len = J.slot[s].len;
     if (with_all) {
       net->tabs[p].tab_old = J.slot[so].ptr;
@@ -1457,6 +1476,15 @@ __global__ void division_check_kernel(uint64_t n, uint64_t seed, unsigned long l
       case 7: ua = (ua & 0x80ffffffu) | 0x7e000000u; ub = (ub & 0x80ffffffu) | 0x01000000u; break; /* overflow */
       case 8: ub = (ub & 0x807fffffu) | (((ua >> 23) & 0xffu) + 100u > 254u ? 0x3f800000u : (((ua >> 23) & 0xffu) + 100u) << 23); break;
       case 9: ua = (ua & 0x807fffffu) | 0x3f800000u; ub = (ub & 0x807fffffu) | 0x3f800000u; break; /* [1, 2) */
+      case 10:
+      case 11: { /* a / d within an ulp of a float midpoint: a = RN(m d), m = q + ulp(q)/2 */
+        const uint32_t uq = (ua & 0x807fffffu) | (((ua >> 23) & 0x3fu) + 96u) << 23;
+        ub = (ub & 0x807fffffu) | (((ub >> 23) & 0x3fu) + 96u) << 23;
+        const double m = (double)__uint_as_float(uq) + (double)__uint_as_float(uq & 0x7f800000u) * 0x1p-24;
+        ua = __float_as_uint(__double2float_rn(m * (double)__uint_as_float(ub))) + (uint32_t)(ua >> 31) -
+             (uint32_t)((ua >> 30) & 1u);
+        break;
+      }
       default: break;
     }
     const float a = __uint_as_float(ua), d = __uint_as_float(ub);
@@ -1464,9 +1492,38 @@ __global__ void division_check_kernel(uint64_t n, uint64_t seed, unsigned long l
     const float q0 = a / d, q1 = div_rn(a, d);
     ++t;
     if (__float_as_uint(q0) != __float_as_uint(q1) && !(q0 != q0 && q1 != q1)) ++b;
+    /* the reciprocal form of the closed forms (qmul), where it claims the
+       quotient; a subnormal quotient is left to div_rn by its callers */
+    bool slow = false;
+    const float q2 = qmul(a, __drcp_rn((double)d), slow);
+    if (!slow && __float_as_uint(q0) != __float_as_uint(q2) && !(q0 != q0 && q2 != q2)) ++b;
   }
   atomicAdd(tested, t);
   atomicAdd(bad, b);
+}
+
+int bcpnn_phase_probe(bcpnn_net* net, uint64_t* out, int32_t max_ctas, int32_t* n_ctas, int32_t reset) {
+  if (!net) return BCPNN_ERR_INVALID;
+#ifdef BCPNN_PHASE_PROBE
+  if (!n_ctas || (max_ctas > 0 && !out)) return fail(net, BCPNN_ERR_INVALID, "bcpnn_phase_probe: null buffer");
+  const int n = std::min(net->total_hcu, kProbeCtas);
+  *n_ctas = n;
+  CU(cudaSetDevice(net->device));
+  CU(cudaStreamSynchronize(net->stream));
+  if (max_ctas > 0) {
+    const size_t k = (size_t)std::min(n, (int)max_ctas) * kProbeSlots;
+    CU(cudaMemcpyFromSymbol(out, g_phase_probe, k * sizeof(uint64_t)));
+  }
+  if (reset) {
+    static const uint64_t zeros[kProbeCtas * kProbeSlots] = {};
+    CU(cudaMemcpyToSymbol(g_phase_probe, zeros, sizeof(zeros)));
+  }
+  return BCPNN_OK;
+#else
+  (void)out; (void)max_ctas; (void)reset;
+  if (n_ctas) *n_ctas = 0;
+  return fail(net, BCPNN_ERR_STATE, "bcpnn_phase_probe: this library was built without BCPNN_PHASE_PROBE");
+#endif
 }
 
 int bcpnn_selftest_division(bcpnn_net* net, uint64_t n_pairs, uint64_t seed, uint64_t* tested, uint64_t* mismatches) {

@@ -55,6 +55,17 @@ constexpr int kErrIndex = 1;        /* ii out of the source population range   *
 constexpr int kErrBarrier = 2;      /* a grid barrier wait ran out of time      */
 constexpr int kErrColumns = 4;      /* a wait for deferred column work ran out of time */
 
+/* Phase probe of the tick kernel (compile-time flag BCPNN_PHASE_PROBE, off in
+   the default build): per CTA, the SM clock cycles spent in each phase of a
+   tick, summed over ticks.  Group A's first thread records slots 0-15, group
+   B's first thread slots 16-30; slot kProbeTicks counts the ticks. */
+constexpr int kProbeSlots = 32;
+constexpr int kProbeTicks = 31;
+constexpr int kProbeCtas = 4096;
+#ifdef BCPNN_PHASE_PROBE
+__device__ unsigned long long g_phase_probe[kProbeCtas * kProbeSlots];
+#endif
+
 struct PopDev {
   int H, M, n, hcu_start, mcu_start, dim_proj, id;
   uint32_t rng_seed, rng_pop; /* Philox key of this population's streams: (rng_seed, rng_pop*16 + stream) */
@@ -139,11 +150,20 @@ struct RunParams {
   const struct TabRef* tabs;  /* [n_projs] decay tables of the run */
 };
 
+/* reciprocals (double, correctly rounded) of the closed form's constant
+   divisors for one kp: 1/(ke-kp), 1/((kzi-kp)+kzj), 1/((kzi-ke)+kzj),
+   1/(kp-kzi), 1/(ke-kzi), with the divisors evaluated in float as gsbn does */
+struct RCoef {
+  double Dekp, D2, D3, Dpzi, Dezi;
+};
+
 /* decay tables of one projection for a run */
 struct TabRef {
   const float4* tab;      /* kp = taupdt*prn     */
   const float4* tab_old;  /* kp = taupdt*old_prn */
+  const double2* rtab;    /* kp = taupdt*prn: reciprocals of the divisor entries, see build_table_kernel */
   int len, old_len;
+  RCoef rk;               /* kp = taupdt*prn */
 };
 
 /* constants of the closed form for one kp */
@@ -439,9 +459,113 @@ __device__ __noinline__ float4 row_decay_nl(float4 r, const Coef k, float4 A, fl
   return r;
 }
 
+/* The closed forms with every division a / b evaluated as
+   RN_float(RN_double(a * r)), r = RN_double(1/b) precomputed (RCoef for the
+   constant divisors, the reciprocal table for the table entries).  This is
+   the correctly rounded float quotient whenever that quotient is a normal
+   float: |a*r - a/b| <= 2^-51.9 |a/b|, while a/b, with 24-bit a and b, is
+   never exactly a float midpoint and lies at least 2^-49 |a/b| away from
+   every midpoint (a - m*b is a nonzero multiple of ulp(m)/2 * ulp(b)), so
+   both round to the same float.  Below 2^-126 the float grid is uniform
+   (2^-149): there a/b can be exactly a midpoint, and is otherwise at least
+   2^-174 away from one (a - m*b is a nonzero multiple of 2^-150 ulp(b)),
+   while |a*r - a/b| < 2^-178.  So a result in that range whose scaled value
+   a*r*2^150 lies within 2^-25 of an odd integer (a midpoint) is ambiguous:
+   the lane sets `slow` and the caller recomputes the whole decay with div_rn;
+   every other result is RN(a/b).  Zeros, infinities and NaNs come out as IEEE
+   division gives them (0*r, a*0, a*inf).  No branch and no vote per
+   division, so the ten divisions of a cell overlap (checked against `/` on
+   the GPU on random, subnormal, extreme and near-midpoint pairs, see
+   bcpnn_selftest_division). */
+__device__ __forceinline__ float qmul(float a, double r, bool& slow) {
+  const double qd = (double)a * r;
+  const float q = __double2float_rn(qd);
+  if (fabs(qd) < 0x1p-126) {
+    const double t = qd * 0x1p150; /* exact: the subnormal grid in half-units */
+    const double n = rint(t);
+    slow |= (fabs(t - n) < 0x1p-25) && ((((long long)n) & 1) != 0);
+  }
+  return q;
+}
+
+/* cell: A = entry[0], B = entry[1], R0 = (1/A.x, 1/A.w), R1 = (1/B.x, 1/B.y) */
+__device__ __forceinline__ bool cell_decay_fast(float4& c, const Coef& k, const RCoef& rk, float4 A, float4 B,
+                                                double2 R0, double2 R1) {
+  bool slow = false;
+  const float pij = c.x, eij = c.y, zi2 = c.z, zj2 = c.w;
+  const float U = (((eij * k.kp) * k.kzi - (eij * k.ke) * k.kp) + (eij * k.kp) * k.kzj) + (k.kekp * zi2) * zj2;
+  const float V = (k.kekp * zi2) * zj2;
+  const float pn = qmul(pij + qmul(qmul(U, rk.Dekp, slow) - qmul(V, rk.D2, slow), rk.D3, slow), R0.x, slow) -
+                   qmul(qmul(A.y * U, rk.Dekp, slow) - qmul(V * A.z, rk.D2, slow), R0.y, slow);
+  const float W = (k.ke * zi2) * zj2;
+  const float en = qmul(eij + qmul(W, rk.D3, slow), R1.x, slow) - qmul(W, R1.y, slow);
+  if (slow) return false;
+  c = make_float4(pn, en, zi2 * B.z, zj2 * B.w);
+  return true;
+}
+
+/* row: A = entry[2], B = entry[3], R0 = (1/A.x, 1/A.w), R1 = (1/B.x, 1/B.z) */
+__device__ __forceinline__ bool row_decay_fast(float4& r, const Coef& k, const RCoef& rk, float4 A, float4 B,
+                                               double2 R0, double2 R1) {
+  bool slow = false;
+  const float pi = r.x, ei = r.y, zi = r.z;
+  const float X = ((ei * k.kp) * k.kzi - (ei * k.ke) * k.kp) + k.kekp * zi;
+  const float Y = k.kekp * zi;
+  const float pn = qmul(pi - qmul(qmul(X, rk.Dekp, slow) + qmul(Y, rk.Dpzi, slow), rk.Dezi, slow), R0.x, slow) +
+                   qmul(qmul(A.y * X, rk.Dekp, slow) + qmul(Y * A.z, rk.Dpzi, slow), R0.y, slow);
+  const float KZ = k.ke * zi;
+  const float en = qmul(ei - qmul(KZ, rk.Dezi, slow), R1.x, slow) + qmul(KZ * B.y, R1.y, slow);
+  if (slow) return false;
+  r = make_float4(pn, en, zi * B.w, r.w);
+  return true;
+}
+
+/* One decay of a cell (row) on the float closed-form path: the reciprocal
+   form, falling back to div_rn for a lane that meets a subnormal quotient.
+   Out of line: one copy of each body for all call sites. */
+#ifdef BCPNN_PHASE_PROBE
+/* decays taken by the reciprocal form / by the div_rn fallback, per CTA */
+#define PROBE_DECAY(slow) atomicAdd(&g_phase_probe[blockIdx.x % kProbeCtas * kProbeSlots + ((slow) ? 14 : 15)], 1ull)
+#else
+#define PROBE_DECAY(slow) do {} while (0)
+#endif
+
+__device__ __noinline__ float4 cell_step_nl(float4 c, const Coef k, const RCoef rk, float4 A, float4 B, double2 R0,
+                                            double2 R1) {
+  float4 f = c;
+  if (!k.fp64 && cell_decay_fast(f, k, rk, A, B, R0, R1)) {
+    PROBE_DECAY(false);
+    return f;
+  }
+  PROBE_DECAY(true);
+  cell_decay(c.x, c.y, c.z, c.w, k, A, B);
+  return c;
+}
+
+__device__ __noinline__ float4 row_step_nl(float4 r, const Coef k, const RCoef rk, float4 A, float4 B, double2 R0,
+                                           double2 R1) {
+  float4 f = r;
+  if (!k.fp64 && row_decay_fast(f, k, rk, A, B, R0, R1)) {
+    PROBE_DECAY(false);
+    return f;
+  }
+  PROBE_DECAY(true);
+  row_decay(r.x, r.y, r.z, k, A, B);
+  return r;
+}
+
 /* ------------------------------------------------------------------------ */
 
-__global__ void build_table_kernel(float4* tab, int len, float kp, float ke, float kzi, float kzj) {
+/* rtab, beside tab: for every d four double2, the correctly rounded
+   reciprocals of the float divisor entries
+     [0] cell: 1/Ep, 1/(Ep*D3)      [1] cell: 1/Ee, 1/((Ezi*Ezj)*D3)
+     [2] row:  1/Ep, 1/(Ep*Dezi)    [3] row:  1/Ee, 1/(Ee*Dezi)           */
+__device__ __forceinline__ void recip_part(float4 A, float4 B, int part, double2& R0, double2& R1) {
+  R0 = make_double2(__drcp_rn((double)A.x), __drcp_rn((double)A.w));
+  R1 = make_double2(__drcp_rn((double)B.x), __drcp_rn((double)(part == 0 ? B.y : B.z)));
+}
+
+__global__ void build_table_kernel(float4* tab, double2* rtab, int len, float kp, float ke, float kzi, float kzj) {
   for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < len; d += gridDim.x * blockDim.x) {
     float4 t0, t1, t2, t3;
     table_entry(kp, ke, kzi, kzj, d, t0, t1, t2, t3);
@@ -449,6 +573,13 @@ __global__ void build_table_kernel(float4* tab, int len, float kp, float ke, flo
     tab[(size_t)d * 4 + 1] = t1;
     tab[(size_t)d * 4 + 2] = t2;
     tab[(size_t)d * 4 + 3] = t3;
+    double2 r0, r1, r2, r3;
+    recip_part(t0, t1, 0, r0, r1);
+    recip_part(t2, t3, 2, r2, r3);
+    rtab[(size_t)d * 4 + 0] = r0;
+    rtab[(size_t)d * 4 + 1] = r1;
+    rtab[(size_t)d * 4 + 2] = r2;
+    rtab[(size_t)d * 4 + 3] = r3;
   }
 }
 

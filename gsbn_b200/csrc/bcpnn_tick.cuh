@@ -62,6 +62,30 @@ __device__ __forceinline__ void group_sync(int id) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kGroup) : "memory");
 }
 
+/* phase probe (BCPNN_PHASE_PROBE): the recording thread adds the cycles since
+   its previous mark to slot `slot` of its CTA's row of g_phase_probe */
+#ifdef BCPNN_PHASE_PROBE
+#define PROBE_DECL long long probe_t = clock64(); const bool probe_on = (threadIdx.x % kGroup) == 0
+#define PROBE(slot)                                                                 \
+  do {                                                                              \
+    if (probe_on) {                                                                 \
+      const long long t_ = clock64();                                               \
+      if (blockIdx.x < kProbeCtas)                                                  \
+        g_phase_probe[blockIdx.x * kProbeSlots + (threadIdx.x < kGroup ? 0 : 16) + (slot)] +=      \
+            (unsigned long long)(t_ - probe_t);                                     \
+      probe_t = t_;                                                                 \
+    }                                                                               \
+  } while (0)
+#define PROBE_TICK()                                                                \
+  do {                                                                              \
+    if (threadIdx.x == 0 && blockIdx.x < kProbeCtas) g_phase_probe[blockIdx.x * kProbeSlots + kProbeTicks] += 1; \
+  } while (0)
+#else
+#define PROBE_DECL do {} while (0)
+#define PROBE(slot) do {} while (0)
+#define PROBE_TICK() do {} while (0)
+#endif
+
 /* ordered compaction within a warp group (see block_prefix) */
 __device__ __forceinline__ int group_prefix(bool flag, int gtid, int bar_id, int* s_warp, int* s_total, int* total) {
   int lane = gtid & 31, warp = gtid >> 5;
@@ -108,9 +132,10 @@ __device__ __forceinline__ float group_max(float v, int gtid, int bar_id, float*
 /* shared-memory layout of a CTA, in 32-bit words from the dynamic base;
    float4 arrays first (16-byte alignment) */
 struct TickLayout {
-  int stg_rtr, stg_rA, stg_rB;   /* [kBlock] float4: row traces (pi,ei,zi), table parts 2,3 */
+  int stg_rtr, stg_rA, stg_rB;   /* [rows] float4: row traces (pi,ei,zi), table parts 2,3   */
   int stg_cv, stg_cA, stg_cB;    /* [kRowChunkCells] float4: cell, table parts 0,1          */
-  int stg_row, stg_ti;           /* [kBlock] int                                           */
+  int stg_rR, stg_cR;            /* [rows] / [kRowChunkCells] 2 x double2: divisor reciprocals */
+  int stg_row, stg_ti;           /* [rows] int                                             */
   int stg_tv, stg_wv;            /* [kRowChunkCells] int / float                           */
   int w_dsup, w_act, w_spkl, w_pi, w_w;
   int w_spkp;                    /* [2][M] int: spike lists by tick parity (deferred columns) */
@@ -124,22 +149,31 @@ struct TickLayout {
    [C]; list [2][C]; bits [2][ceil(C/32)]; nlist [2] */
 __host__ __device__ inline int qblock_words(int M, int C) { return 5 * M + 5 * C + 2 * ((C + 31) / 32) + 2; }
 
+__host__ __device__ inline int row_chunk_rows(int M) {
+  int r = kRowChunkCells / M;
+  if (r < 1) r = 1;
+  return r;
+}
+
 __host__ __device__ inline void tick_layout(int M, int n_in, const int* C, TickLayout& L) {
+  const int rows = (row_chunk_rows(M) + 3) & ~3; /* rows of one chunk, padded to 16 bytes */
   int o = 0;
-  L.stg_rtr = o; o += 4 * kBlock;
-  L.stg_rA = o; o += 4 * kBlock;
-  L.stg_rB = o; o += 4 * kBlock;
+  L.stg_rtr = o; o += 4 * rows;
+  L.stg_rA = o; o += 4 * rows;
+  L.stg_rB = o; o += 4 * rows;
   L.stg_cv = o; o += 4 * kRowChunkCells;
   L.stg_cA = o; o += 4 * kRowChunkCells;
   L.stg_cB = o; o += 4 * kRowChunkCells;
-  L.stg_row = o; o += kBlock;
-  L.stg_ti = o; o += kBlock;
+  L.stg_rR = o; o += 8 * rows;
+  L.stg_cR = o; o += 8 * kRowChunkCells;
+  L.stg_row = o; o += rows;
+  L.stg_ti = o; o += rows;
   L.stg_tv = o; o += kRowChunkCells;
   L.stg_wv = o; o += kRowChunkCells;
   L.w_dsup = o; o += M;
   L.w_act = o; o += M;
   L.w_spkl = o; o += M;
-  L.w_pi = o; o += kBlock;
+  L.w_pi = o; o += rows;
   L.w_w = o; o += kRowChunkCells;
   L.w_spkp = o; o += 2 * M;
   L.w_spk = o; o += (M + 3) / 4;
@@ -183,24 +217,20 @@ __device__ __forceinline__ QView qview(float* sm, const TickLayout& L, int q, in
   return v;
 }
 
-__device__ __forceinline__ int row_chunk_rows(int M) {
-  int r = kRowChunkCells / M;
-  if (r < 1) r = 1;
-  return r;
-}
-
 /* Stage rows [base, base+nr) of `list` of projection J for a tick at
    `simstep`: row traces, cells of the chunk, and the decay-table entries for
    their elapsed ticks.  Threads gtid, gtid+gsize, ... of a group of gsize. */
 __device__ __forceinline__ void stage_rows(const ProjDev& J, const int* list, int base, int nr, int M, int simstep,
-                                           const float4* tab, int tlen, float* sm, const TickLayout& L, int gtid,
-                                           int gsize) {
+                                           const float4* tab, const double2* rtab, int tlen, float* sm,
+                                           const TickLayout& L, int gtid, int gsize) {
   float4* rtr = (float4*)(sm + L.stg_rtr);
   float4* rA = (float4*)(sm + L.stg_rA);
   float4* rB = (float4*)(sm + L.stg_rB);
   float4* cv = (float4*)(sm + L.stg_cv);
   float4* cA = (float4*)(sm + L.stg_cA);
   float4* cB = (float4*)(sm + L.stg_cB);
+  double2* rR = (double2*)(sm + L.stg_rR);
+  double2* cR = (double2*)(sm + L.stg_cR);
   int* srow = (int*)(sm + L.stg_row);
   int* sti = (int*)(sm + L.stg_ti);
   int* stv = (int*)(sm + L.stg_tv);
@@ -211,15 +241,20 @@ __device__ __forceinline__ void stage_rows(const ProjDev& J, const int* list, in
     float pi = J.pi[r], ei = J.ei[r], zi = J.zi[r];
     int pdt = simstep - ti;
     float4 A = make_float4(0, 0, 0, 0), B = A;
+    double2 R0 = make_double2(0, 0), R1 = R0;
     if (pdt > 0 && pdt < tlen) {
       A = tab[(size_t)pdt * 4 + 2];
       B = tab[(size_t)pdt * 4 + 3];
+      R0 = rtab[(size_t)pdt * 4 + 2];
+      R1 = rtab[(size_t)pdt * 4 + 3];
     }
     srow[t] = r;
     sti[t] = ti;
     rtr[t] = make_float4(pi, ei, zi, 0.0f);
     rA[t] = A;
     rB[t] = B;
+    rR[2 * t] = R0;
+    rR[2 * t + 1] = R1;
   }
   for (int c = gtid; c < nr * M; c += gsize) {
     int rr = c / M;
@@ -230,15 +265,20 @@ __device__ __forceinline__ void stage_rows(const ProjDev& J, const int* list, in
     float wv = J.wij[index];
     int pdt = simstep - tv;
     float4 A = make_float4(0, 0, 0, 0), B = A;
+    double2 R0 = make_double2(0, 0), R1 = R0;
     if (pdt > 0 && pdt < tlen) {
       A = tab[(size_t)pdt * 4 + 0];
       B = tab[(size_t)pdt * 4 + 1];
+      R0 = rtab[(size_t)pdt * 4 + 0];
+      R1 = rtab[(size_t)pdt * 4 + 1];
     }
     stv[c] = tv;
     cv[c] = c4;
     swv[c] = wv;
     cA[c] = A;
     cB[c] = B;
+    cR[2 * c] = R0;
+    cR[2 * c + 1] = R1;
   }
 }
 
@@ -338,6 +378,7 @@ __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, con
       }
     }
     float4 tA[kColU], tB[kColU];
+    double2 tR0[kColU], tR1[kColU];
 #pragma unroll
     for (int u = 0; u < kColU; ++u) {
       if (!ok[u]) continue;
@@ -346,6 +387,8 @@ __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, con
       if (pdt > 0 && pdt < T.len) {
         tA[u] = T.tab[(size_t)pdt * 4 + 0];
         tB[u] = T.tab[(size_t)pdt * 4 + 1];
+        tR0[u] = T.rtab[(size_t)pdt * 4 + 0];
+        tR1[u] = T.rtab[(size_t)pdt * 4 + 1];
       }
     }
 #pragma unroll
@@ -359,13 +402,15 @@ __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, con
       } else {
         const Coef k = make_coef(J.taupdt * prn, J.ke, J.kzi, J.kzj, kF64);
         float4 A = tA[u], B = tB[u];
+        double2 R0 = tR0[u], R1 = tR1[u];
         if (pdt >= rp->tabs[pj[u]].len) {
           if (kF64)
             table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, B, 1);
           else
             cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+          recip_part(A, B, 0, R0, R1);
         }
-        c4 = cell_decay_nl(c4, k, A, B);
+        c4 = cell_step_nl(c4, k, rp->tabs[pj[u]].rk, A, B, R0, R1);
         c4.w = c4.w + J.kftj;
       }
       J.cell[index[u]] = c4;
@@ -509,16 +554,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
     const ProjDev& J = s_proj[0];
     QView V = qview(sm, L, 0, M, J.C);
     int nr = V.nlist[cur0] < row_chunk_rows(M) ? V.nlist[cur0] : row_chunk_rows(M);
-    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, s_tab[0].tab, s_tab[0].len, sm, L, tid,
-               kBlock);
+    stage_rows(J, V.list + cur0 * J.C, 0, nr, M, rp->simstep0 + it0, s_tab[0].tab, s_tab[0].rtab, s_tab[0].len, sm,
+               L, tid, kBlock);
   }
 
+  PROBE_DECL;
   for (int it = it0; it < it0 + n_ticks; ++it) {
     if (it > it0) {
       if (!grid_sync(bar, (unsigned int)(it - it0) * gridDim.x, net->err, &s_ok)) return;
     } else {
       __syncthreads();
     }
+    PROBE(0);
+    PROBE_TICK();
     const int simstep = rp->simstep0 + it;
     const int kk = rp->k0 + it;
     const int cur = kk & 1, prev = cur ^ 1, nxt = cur ^ 1;
@@ -546,6 +594,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         float d = st_dsup[j];
         w_dsup[j] = d + (sup - d) * pop.taumdt;
       }
+      PROBE(1);
       /* the softmax max of every HCU is seeded with the population's first
          MCU (Pop.cpp:270), published by HCU 0's CTA in the previous tick */
       const int tseed = (M < kGroup) ? kGroup - 1 : 0;
@@ -599,6 +648,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         s_vsum = vsum;
       }
       group_sync(kBarA);
+      PROBE(2);
       const float vsum = s_vsum;
       const float pr = net->poisson_hz * net->dt;
       for (int j = gtid; j < M; j += kGroup) {
@@ -656,6 +706,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       }
       /* hand the spike list to group B */
       asm volatile("bar.arrive %0, %1;" ::"r"(kBarSpikes), "r"(kBlock) : "memory");
+      PROBE(3);
 
       for (int q = 0; q < n_in; ++q) {
         const int p = s_inp[q];
@@ -665,6 +716,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         const float kp = J.taupdt * prn;
         const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
         const float4* tab = s_tab[q].tab;
+        const double2* rtab = s_tab[q].rtab;
+        const RCoef& rk = s_tab[q].rk;
         const int tlen = s_tab[q].len;
         const size_t eoff = (size_t)J.proj_in_pop * n;
 
@@ -688,6 +741,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           if (h == 0) pop.bj[cur][eoff] = V.bj[0];
         }
         group_sync(kBarA);
+        PROBE(4);
         if (defer && q == 0 && it > it0) {
           /* the previous tick's columns of this HCU, done by the grid, must be
              in place before its rows; then refresh the staged cells they hit */
@@ -709,6 +763,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
             float4* fcv = (float4*)(sm + L.stg_cv);
             float4* fcA = (float4*)(sm + L.stg_cA);
             float4* fcB = (float4*)(sm + L.stg_cB);
+            double2* fcR = (double2*)(sm + L.stg_cR);
             int* ftv = (int*)(sm + L.stg_tv);
             const int* frow = (const int*)(sm + L.stg_row);
             for (int c = gtid; c < nr0 * np; c += kGroup) {
@@ -719,19 +774,25 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
               const float4 c4 = __ldcg(J.cell + index);
               const int pdt = simstep - tv;
               float4 A = make_float4(0, 0, 0, 0), B = A;
+              double2 R0 = make_double2(0, 0), R1 = R0;
               if (pdt > 0 && pdt < tlen) {
                 A = tab[(size_t)pdt * 4 + 0];
                 B = tab[(size_t)pdt * 4 + 1];
+                R0 = rtab[(size_t)pdt * 4 + 0];
+                R1 = rtab[(size_t)pdt * 4 + 1];
               }
               ftv[rr * M + j] = tv;
               fcv[rr * M + j] = c4;
               fcA[rr * M + j] = A;
               fcB[rr * M + j] = B;
+              fcR[2 * (rr * M + j)] = R0;
+              fcR[2 * (rr * M + j) + 1] = R1;
             }
             group_sync(kBarA);
           }
         }
 
+        PROBE(5);
         /* row updates of this HCU's active rows, ascending, Proj.cpp:365-479 */
         const int nrow = V.nlist[cur];
         const int* list = V.list + cur * C;
@@ -742,6 +803,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         const float4* stg_cv = (const float4*)(sm + L.stg_cv);
         const float4* stg_cA = (const float4*)(sm + L.stg_cA);
         const float4* stg_cB = (const float4*)(sm + L.stg_cB);
+        const double2* stg_rR = (const double2*)(sm + L.stg_rR);
+        const double2* stg_cR = (const double2*)(sm + L.stg_cR);
         const int* stg_row = (const int*)(sm + L.stg_row);
         const int* stg_ti = (const int*)(sm + L.stg_ti);
         const int* stg_tv = (const int*)(sm + L.stg_tv);
@@ -749,7 +812,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         for (int base = 0; base < nrow; base += rch) {
           const int nr = (nrow - base) < rch ? (nrow - base) : rch;
           if (!(q == 0 && base == 0)) {
-            stage_rows(J, list, base, nr, M, simstep, tab, tlen, sm, L, gtid, kGroup);
+            stage_rows(J, list, base, nr, M, simstep, tab, rtab, tlen, sm, L, gtid, kGroup);
             group_sync(kBarA);
           }
           /* row traces (threads from the top of the group) beside the cell
@@ -767,9 +830,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
             } else {
               float pi = tr.x, ei = tr.y, zi = tr.z;
               float4 A = stg_rA[t], B = stg_rB[t];
-              if (pdt >= tlen) load_entry(tab, tlen, k, pdt, 2, A, B);
+              double2 R0 = stg_rR[2 * t], R1 = stg_rR[2 * t + 1];
+              if (pdt >= tlen) {
+                load_entry(tab, tlen, k, pdt, 2, A, B);
+                recip_part(A, B, 2, R0, R1);
+              }
               {
-                const float4 rt = row_decay_nl(make_float4(pi, ei, zi, 0.0f), k, A, B);
+                const float4 rt = row_step_nl(make_float4(pi, ei, zi, 0.0f), k, rk, A, B, R0, R1);
                 pi = rt.x;
                 ei = rt.y;
                 zi = rt.z;
@@ -795,8 +862,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
               w_skip[c] = 1;
             } else {
               float4 A = stg_cA[c], B = stg_cB[c];
-              if (pdt >= tlen) load_entry(tab, tlen, k, pdt, 0, A, B);
-              cv = cell_decay_nl(cv, k, A, B);
+              double2 R0 = stg_cR[2 * c], R1 = stg_cR[2 * c + 1];
+              if (pdt >= tlen) {
+                load_entry(tab, tlen, k, pdt, 0, A, B);
+                recip_part(A, B, 0, R0, R1);
+              }
+              cv = cell_step_nl(cv, k, rk, A, B, R0, R1);
               cv.z = cv.z + J.kfti;
               J.cell[index] = cv;
               J.tij[index] = simstep;
@@ -828,6 +899,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           }
           group_sync(kBarA);
         }
+        PROBE(6);
         if (gtid == 0) {
           if (h == 0) pop.epsc[cur][eoff] = V.epsc[0];
           /* debug flags of ProcSpkRec (ssi/ssj contain index 9) */
@@ -840,6 +912,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       }
       /* rows done: group B may now update column cells of active rows */
       if (!defer) asm volatile("bar.arrive %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
+      PROBE(7);
     } else {
       /* ================= group B: delay queue, columns =================== */
       if (defer) {
@@ -854,6 +927,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         help_columns<kF64>(net, rp, net->col_ring + (size_t)prev * net->col_cap, s_hbeg, s_hend, simstep - 1, col_done,
                            gtid, kBarB);
       }
+      PROBE(10);
       for (int q = 0; q < n_in; ++q) {
         const ProjDev& J = s_proj[q];
         const int C = J.C;
@@ -923,8 +997,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         }
         if (gtid == 0) V.nlist[nxt] = cnt;
       }
+      PROBE(11);
       /* wait for group A's spike list */
       asm volatile("bar.sync %0, %1;" ::"r"(kBarSpikes), "r"(kBlock) : "memory");
+      PROBE(12);
       const int nspk = s_nspk;
       if (defer) {
         /* publish this tick's column units; the grid does them next tick */
@@ -976,6 +1052,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           const float kp = J.taupdt * prn;
           const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
           const float4* tab = s_tab[q].tab;
+          const double2* rtab = s_tab[q].rtab;
+          const RCoef& rk = s_tab[q].rk;
           const int tlen = s_tab[q].len;
           const uint32_t* cbits = V.bits + cur * V.W;
           const int* clist = V.list + cur * C;
@@ -1011,12 +1089,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
             }
             /* decay-table entries of the whole batch, then the compute */
             float4 tA[kColU], tB[kColU];
+            double2 tR0[kColU], tR1[kColU];
 #pragma unroll
             for (int u = 0; u < kColU; ++u) {
               int pdt = simstep - tv[u];
               if (ok[u] && pdt > 0 && pdt < tlen) {
                 tA[u] = tab[(size_t)pdt * 4 + 0];
                 tB[u] = tab[(size_t)pdt * 4 + 1];
+                tR0[u] = rtab[(size_t)pdt * 4 + 0];
+                tR1[u] = rtab[(size_t)pdt * 4 + 1];
               }
             }
 #pragma unroll
@@ -1028,13 +1109,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                 c4.w += J.kftj;
               } else {
                 float4 A = tA[u], B = tB[u];
+                double2 R0 = tR0[u], R1 = tR1[u];
                 if (pdt >= tlen) {
                   if (k.fp64)
                     table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, B, 1);
                   else
                     cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+                  recip_part(A, B, 0, R0, R1);
                 }
-                c4 = cell_decay_nl(c4, k, A, B);
+                c4 = cell_step_nl(c4, k, rk, A, B, R0, R1);
                 c4.w = c4.w + J.kftj;
               }
               J.cell[index[u]] = c4;
@@ -1045,15 +1128,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         }
       }
     }
+    PROBE(13);
     __syncthreads();
+    PROBE(8);
 
     /* stage the next tick's first row chunk before the barrier */
     if (it + 1 < it0 + n_ticks && n_in > 0) {
       const ProjDev& J = s_proj[0];
       QView V = qview(sm, L, 0, M, J.C);
       int nr = V.nlist[nxt] < row_chunk_rows(M) ? V.nlist[nxt] : row_chunk_rows(M);
-      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, s_tab[0].tab, s_tab[0].len, sm, L, tid, kBlock);
+      stage_rows(J, V.list + nxt * J.C, 0, nr, M, simstep + 1, s_tab[0].tab, s_tab[0].rtab, s_tab[0].len, sm, L,
+                 tid, kBlock);
     }
+    PROBE(9);
   }
 
   /* ---- the last tick's deferred columns -------------------------------- */

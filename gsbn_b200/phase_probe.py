@@ -1,0 +1,86 @@
+"""Phase breakdown of the tick kernel on the 100x100 workload.
+
+Needs the phase-probe build of the library (python -m gsbn_b200.build
+--probe, which writes gsbn_b200/libgsbn_b200_probe.so) and a GPU:
+
+    GSBN_B200_LIB=gsbn_b200/libgsbn_b200_probe.so python -m gsbn_b200.phase_probe
+
+Runs the first `--train` training segments and, after the switch to recall,
+`--recall` recall segments of the 100x100 density-0.1 workload (100 ticks
+each, one persistent launch per segment), then prints, per phase, the time
+per tick of the median CTA and of the slowest CTA, in microseconds at the SM
+clock given by --mhz (the counters are SM clock cycles).  The probe adds a
+clock read and a store per phase boundary, so the total is a little above
+the default build's time per tick.  Slots 14 and 15 count the cell and row
+decays done by the div_rn fallback and by the reciprocal form.
+"""
+import argparse
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+from gsbn_b200 import capi, extgen, schema, workloads
+
+PHASES_A = ["barrier wait", "support", "softmax", "spikes", "j-traces", "column wait + refresh", "rows",
+            "end of rows", "join wait", "staging next chunk"]
+PHASES_B = {16: "barrier wait", 26: "column units of the grid", 27: "delay queue", 28: "spike wait",
+            29: "unit publication", 24: "join wait", 25: "staging next chunk"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=20)
+    ap.add_argument("--recall", type=int, default=20)
+    ap.add_argument("--mhz", type=float, default=1965.0)
+    ap.add_argument("--threads", type=int, default=0)
+    a = ap.parse_args()
+    if "probe" not in capi.LIB_PATH:
+        sys.exit("set GSBN_B200_LIB to the phase-probe build (gsbn_b200/libgsbn_b200_probe.so)")
+    w = workloads.config1()
+    sp, _ = w.solver_param(tempfile.mkdtemp(prefix="gsbn_probe_"))
+    pops, projs = workloads.net_from_solver_param(sp)
+    conn = workloads.read_conn_map(w.conn, pops, projs)
+    lgidx, wmask = extgen.stim_tables(schema.read_stim(sp.gen_param.stim_file))
+    runs = extgen.segments(sp)
+    first_recall = next(i for i, r in enumerate(runs) if r.prn == 0.0)
+    net = capi.Net(pops, projs, float(np.float32(sp.gen_param.dt)), seed=w.meta["seed"], max_ticks=128,
+                   tick_threads=a.threads)
+    for k, (ii, di) in enumerate(conn):
+        net.set_conn(k, ii, di)
+    net.upload_stimuli_idx(lgidx, float(np.float32(sp.gen_param.eps)), wmask)
+    out, counts = {}, {}
+    for name, sel in (("training", runs[1:1 + a.train]), ("recall", runs[first_recall + 1:first_recall + 1 + a.recall])):
+        # run up to the selection without the probe, then the selection with it
+        net.reset()
+        for r in runs[:runs.index(sel[0])]:
+            net.use_stimulus(r.lgidx, r.wmask)
+            net.run(r.first, r.n, r.prn, r.old_prn)
+        net.phase_probe(reset=True)
+        for r in sel:
+            net.use_stimulus(r.lgidx, r.wmask)
+            net.run(r.first, r.n, r.prn, r.old_prn)
+        c = net.phase_probe(reset=True).astype(np.float64)
+        counts[name] = c
+        ticks = c[:, 31:32]
+        per_tick = c / np.maximum(ticks, 1) / a.mhz  # us per tick
+        out[name] = per_tick
+    net.close()
+    for name, pt in out.items():
+        print(f"== {name} segments: us per tick at {a.mhz:.0f} MHz (median CTA / slowest CTA)")
+        tot = 0.0
+        for k, ph in enumerate(PHASES_A):
+            med, mx = float(np.median(pt[:, k])), float(pt[:, k].max())
+            tot += med
+            print(f"  A {ph:<24} {med:7.3f} {mx:7.3f}")
+        print(f"  A {'total (median)':<24} {tot:7.3f}")
+        for k, ph in sorted(PHASES_B.items()):
+            print(f"  B {ph:<24} {float(np.median(pt[:, k])):7.3f} {float(pt[:, k].max()):7.3f}")
+        slow, fast = float(counts[name][:, 14].sum()), float(counts[name][:, 15].sum())
+        print(f"  decays: {fast:.0f} by the reciprocal form, {slow:.0f} by the div_rn fallback "
+              f"({100.0 * slow / max(1.0, slow + fast):.3f} %)")
+
+
+if __name__ == "__main__":
+    main()

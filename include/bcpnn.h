@@ -283,14 +283,29 @@ int bcpnn_kernel_launches(const bcpnn_net* net, uint64_t* out);
 int bcpnn_selftest_barrier_timeout(bcpnn_net* net, int64_t limit_ns);
 
 /* Numerics self-test (no counterpart in the reference): the decay closed
-   forms divide with a warp-uniform exact division instead of `/` (zero and
-   infinite operands by their exact results, a double-precision quotient
-   rounded once for subnormal or extreme operands).  This runs n_pairs float
-   pairs drawn from `seed` (with biased draws of zero, infinite, subnormal and
-   extreme-exponent operands) through both on the network's device and
-   reports how many pairs were compared (NaN operands skipped) and how many
-   quotients differed in any bit (NaN results compare equal). */
+   forms divide by a multiplication with a correctly rounded double
+   reciprocal, RN_float(a * RN_double(1/b)), and fall back to a warp-uniform
+   exact division (zero and infinite operands by their exact results, a
+   double-precision quotient rounded once for subnormal or extreme operands)
+   where the quotient is subnormal.  This runs n_pairs float pairs drawn from
+   `seed` (with biased draws of zero, infinite, subnormal, extreme-exponent
+   and near-midpoint quotients) through both forms and `/` on the network's
+   device and reports how many pairs were compared (NaN operands skipped) and
+   how many quotients of either form differed from `/` in any bit (NaN
+   results compare equal). */
 int bcpnn_selftest_division(bcpnn_net* net, uint64_t n_pairs, uint64_t seed, uint64_t* tested, uint64_t* mismatches);
+
+/* Phase probe of the tick kernel (no counterpart in the reference): in a
+   library built with -DBCPNN_PHASE_PROBE, copies per CTA (up to max_ctas) the
+   32 counters of kernel phases -- SM clock cycles summed over ticks; slots
+   0-9 group A (barrier wait, support, softmax, spikes, j-traces, column wait,
+   rows, end of rows, join wait, staging), 16-29 group B (barrier wait, join
+   wait, staging, column units of the grid, delay queue, spike wait, unit
+   publication), slot 31 the tick count; slots 14 and 15 count the closed-form
+   decays done by the exact fallback and by the reciprocal form -- sets
+   *n_ctas and, if reset, zeroes them.  The default build returns
+   BCPNN_ERR_STATE. */
+int bcpnn_phase_probe(bcpnn_net* net, uint64_t* out, int32_t max_ctas, int32_t* n_ctas, int32_t reset);
 
 /* Message of the last failing call on this handle ("" if none). */
 const char* bcpnn_last_error(const bcpnn_net* net);
