@@ -100,6 +100,7 @@ struct bcpnn_net {
   uint32_t* log_buf = nullptr;
   size_t log_words_per_tick = 0;
   int64_t k_total = 0;      /* ticks executed since creation */
+  uint32_t tick_serial = 1; /* tags of the softmax seeds (NetDev::seed64); never reset */
   int last_run_ticks = 0;
   bool exchange = false;
   bool direct = false;      /* GSBN_DIRECT_LAUNCH=1: launch kernels one by one (profilers) */
@@ -175,6 +176,7 @@ int check_device_error(bcpnn_net* net) {
     if (e & kErrIndex) why += " a slot's source MCU index is outside the source population;";
     if (e & kErrBarrier) why += " a grid barrier of the persistent tick kernel timed out;";
     if (e & kErrColumns) why += " a wait for the grid's column updates in the persistent tick kernel timed out;";
+    if (e & kErrSeed) why += " a softmax seed published for the next tick carried the wrong tick tag;";
     return fail(net, BCPNN_ERR_DEVICE, "kernel reported error word " + std::to_string(e) + ":" + why);
   }
   return BCPNN_OK;
@@ -628,6 +630,13 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   int* errw = nullptr;
   if ((rc = dalloc(net, &errw, 1))) return bail(rc);
   H.err = errw;
+  unsigned long long* seeds = nullptr;
+  if ((rc = dalloc(net, &seeds, (size_t)desc->n_pops))) return bail(rc);
+  if (cudaMemsetAsync(seeds, 0, (size_t)desc->n_pops * sizeof(unsigned long long), net->stream) != cudaSuccess) {
+    net->err = "memset failed";
+    return bail(BCPNN_ERR_CUDA);
+  }
+  H.seed64 = seeds;
   if (cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), net->stream) != cudaSuccess ||
       cudaMemsetAsync(errw, 0, sizeof(int), net->stream) != cudaSuccess) {
     net->err = "memset failed";
@@ -1136,6 +1145,7 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
     net->tabs[p].tab = J.slot[s].ptr;
     net->tabs[p].rtab = J.slot[s].rptr;
     net->tabs[p].rk = rcoef(net->hq[p], prn);
+    net->tabs[p].k = make_coef(net->hq[p].taupdt * prn, net->hq[p].ke, net->hq[p].kzi, net->hq[p].kzj, net->hq[p].fp64);
     net->tabs[p].len = J.slot[s].len;
     if (with_all) {
       net->tabs[p].tab_old = J.slot[so].ptr;
@@ -1152,6 +1162,9 @@ int bcpnn_run(bcpnn_net* net, int32_t first_simstep, int32_t n_ticks, float prn,
   net->rp.old_prn = old_prn;
   net->rp.lginp = net->cur_lg;
   net->rp.wmask = net->cur_wm;
+  net->rp.serial0 = net->tick_serial;
+  net->tick_serial += (uint32_t)n_ticks;
+  if (net->tick_serial == 0) net->tick_serial = 1; /* tag 0 is the slots' initial value */
   CU(cudaMemcpyAsync(net->d_tabs, net->tabs.data(), net->tabs.size() * sizeof(TabRef), cudaMemcpyHostToDevice,
                      net->stream));
   CU(cudaMemcpyAsync(net->d_rp, &net->rp, sizeof(RunParams), cudaMemcpyHostToDevice, net->stream));

@@ -54,6 +54,7 @@ constexpr int kMaxIn = 8;           /* incoming projections per population      
 constexpr int kErrIndex = 1;        /* ii out of the source population range   */
 constexpr int kErrBarrier = 2;      /* a grid barrier wait ran out of time      */
 constexpr int kErrColumns = 4;      /* a wait for deferred column work ran out of time */
+constexpr int kErrSeed = 8;         /* a published softmax seed carried the wrong tick tag */
 
 /* Phase probe of the tick kernel (compile-time flag BCPNN_PHASE_PROBE, off in
    the default build): per CTA, the SM clock cycles spent in each phase of a
@@ -64,6 +65,9 @@ constexpr int kProbeTicks = 31;
 constexpr int kProbeCtas = 4096;
 #ifdef BCPNN_PHASE_PROBE
 __device__ unsigned long long g_phase_probe[kProbeCtas * kProbeSlots];
+/* the CTA's counters during a launch: shared memory, so that a mark costs a
+   clock read and a shared-memory add, not a global round trip */
+__shared__ unsigned long long g_probe_smem[kProbeSlots];
 #endif
 
 struct PopDev {
@@ -129,6 +133,12 @@ struct NetDev {
      MCU | rows << 16).  Two ring halves by tick parity, col_cap units each. */
   int4* col_ring;
   int col_cap;
+  /* [n_pops] the softmax seed of the next tick (dsup of the population's MCU
+     0, Pop.cpp:270), published by the population's HCU-0 CTA at the end of a
+     tick of the persistent launch: (tick tag << 32) | float bits.  The other
+     CTAs' barrier threads load it while they poll, so it costs no round trip
+     after the barrier; the tag (RunParams::serial0 + tick) certifies it. */
+  unsigned long long* seed64;
 };
 
 /* Decay table entry for one elapsed-tick count d: four float4
@@ -148,7 +158,27 @@ struct RunParams {
   const float* lginp;   /* stimulus of the run: [total MCUs] */
   const float* wmask;   /* [total HCUs] */
   const struct TabRef* tabs;  /* [n_projs] decay tables of the run */
+  unsigned int serial0; /* tag of the run's first tick (never repeats between consecutive ticks, see seed64) */
 };
+
+/* constants of the closed form for one kp */
+struct Coef {
+  float kp, ke, kzi, kzj, kekp, Dekp, Dpzi, Dezi, D2, D3;
+  int fp64; /* tables hold FP64-built propagator coefficients (see fp64_entry) */
+};
+
+__host__ __device__ __forceinline__ Coef make_coef(float kp, float ke, float kzi, float kzj, int fp64 = 0) {
+  Coef k;
+  k.fp64 = fp64;
+  k.kp = kp; k.ke = ke; k.kzi = kzi; k.kzj = kzj;
+  k.kekp = ke * kp;
+  k.Dekp = ke - kp;
+  k.Dpzi = kp - kzi;
+  k.Dezi = ke - kzi;
+  k.D2 = (kzi - kp) + kzj;
+  k.D3 = (kzi - ke) + kzj;
+  return k;
+}
 
 /* reciprocals (double, correctly rounded) of the closed form's constant
    divisors for one kp: 1/(ke-kp), 1/((kzi-kp)+kzj), 1/((kzi-ke)+kzj),
@@ -163,27 +193,10 @@ struct TabRef {
   const float4* tab_old;  /* kp = taupdt*old_prn */
   const double2* rtab;    /* kp = taupdt*prn: reciprocals of the divisor entries, see build_table_kernel */
   int len, old_len;
+  Coef k;                 /* kp = taupdt*prn */
   RCoef rk;               /* kp = taupdt*prn */
 };
 
-/* constants of the closed form for one kp */
-struct Coef {
-  float kp, ke, kzi, kzj, kekp, Dekp, Dpzi, Dezi, D2, D3;
-  int fp64; /* tables hold FP64-built propagator coefficients (see fp64_entry) */
-};
-
-__device__ __forceinline__ Coef make_coef(float kp, float ke, float kzi, float kzj, int fp64 = 0) {
-  Coef k;
-  k.fp64 = fp64;
-  k.kp = kp; k.ke = ke; k.kzi = kzi; k.kzj = kzj;
-  k.kekp = ke * kp;
-  k.Dekp = ke - kp;
-  k.Dpzi = kp - kzi;
-  k.Dezi = ke - kzi;
-  k.D2 = (kzi - kp) + kzj;
-  k.D3 = (kzi - ke) + kzj;
-  return k;
-}
 
 /* The transcendental functions are real calls in device code: several call
    sites share one copy of their instructions, which keeps the tick kernel's
@@ -521,8 +534,10 @@ __device__ __forceinline__ bool row_decay_fast(float4& r, const Coef& k, const R
 }
 
 /* One decay of a cell (row) on the float closed-form path: the reciprocal
-   form, falling back to div_rn for a lane that meets a subnormal quotient.
-   Out of line: one copy of each body for all call sites. */
+   form, falling back to div_rn for a lane whose quotient is ambiguous.  Out
+   of line: one copy of each body for all call sites; the constants come from
+   the run's TabRef (in shared memory where the caller has a copy), so the
+   call passes one pointer instead of 21 words of constants. */
 #ifdef BCPNN_PHASE_PROBE
 /* decays taken by the reciprocal form / by the div_rn fallback, per CTA */
 #define PROBE_DECAY(slow) atomicAdd(&g_phase_probe[blockIdx.x % kProbeCtas * kProbeSlots + ((slow) ? 14 : 15)], 1ull)
@@ -530,8 +545,10 @@ __device__ __forceinline__ bool row_decay_fast(float4& r, const Coef& k, const R
 #define PROBE_DECAY(slow) do {} while (0)
 #endif
 
-__device__ __noinline__ float4 cell_step_nl(float4 c, const Coef k, const RCoef rk, float4 A, float4 B, double2 R0,
+__device__ __noinline__ float4 cell_step_nl(float4 c, const TabRef* __restrict__ T, float4 A, float4 B, double2 R0,
                                             double2 R1) {
+  const Coef k = T->k;
+  const RCoef rk = T->rk;
   float4 f = c;
   if (!k.fp64 && cell_decay_fast(f, k, rk, A, B, R0, R1)) {
     PROBE_DECAY(false);
@@ -542,8 +559,10 @@ __device__ __noinline__ float4 cell_step_nl(float4 c, const Coef k, const RCoef 
   return c;
 }
 
-__device__ __noinline__ float4 row_step_nl(float4 r, const Coef k, const RCoef rk, float4 A, float4 B, double2 R0,
+__device__ __noinline__ float4 row_step_nl(float4 r, const TabRef* __restrict__ T, float4 A, float4 B, double2 R0,
                                            double2 R1) {
+  const Coef k = T->k;
+  const RCoef rk = T->rk;
   float4 f = r;
   if (!k.fp64 && row_decay_fast(f, k, rk, A, B, R0, R1)) {
     PROBE_DECAY(false);

@@ -63,27 +63,39 @@ __device__ __forceinline__ void group_sync(int id) {
 }
 
 /* phase probe (BCPNN_PHASE_PROBE): the recording thread adds the cycles since
-   its previous mark to slot `slot` of its CTA's row of g_phase_probe */
+   its previous mark to slot `slot` of its CTA's row of g_phase_probe, slot
+   0-15 for group A's thread and 16 + slot for group B's */
 #ifdef BCPNN_PHASE_PROBE
 #define PROBE_DECL long long probe_t = clock64(); const bool probe_on = (threadIdx.x % kGroup) == 0
 #define PROBE(slot)                                                                 \
   do {                                                                              \
     if (probe_on) {                                                                 \
       const long long t_ = clock64();                                               \
-      if (blockIdx.x < kProbeCtas)                                                  \
-        g_phase_probe[blockIdx.x * kProbeSlots + (threadIdx.x < kGroup ? 0 : 16) + (slot)] +=      \
-            (unsigned long long)(t_ - probe_t);                                     \
+      g_probe_smem[(threadIdx.x < kGroup ? 0 : 16) + (slot)] += (unsigned long long)(t_ - probe_t); \
       probe_t = t_;                                                                 \
     }                                                                               \
   } while (0)
 #define PROBE_TICK()                                                                \
   do {                                                                              \
-    if (threadIdx.x == 0 && blockIdx.x < kProbeCtas) g_phase_probe[blockIdx.x * kProbeSlots + kProbeTicks] += 1; \
+    if (threadIdx.x == 0) g_probe_smem[kProbeTicks] += 1;                           \
+  } while (0)
+#define PROBE_BEGIN()                                                               \
+  do {                                                                              \
+    if (threadIdx.x < kProbeSlots) g_probe_smem[threadIdx.x] = 0;                   \
+    __syncthreads();                                                                \
+  } while (0)
+#define PROBE_FLUSH()                                                               \
+  do {                                                                              \
+    __syncthreads();                                                                \
+    if (threadIdx.x < kProbeSlots && blockIdx.x < kProbeCtas)                       \
+      atomicAdd(&g_phase_probe[blockIdx.x * kProbeSlots + threadIdx.x], g_probe_smem[threadIdx.x]); \
   } while (0)
 #else
 #define PROBE_DECL do {} while (0)
 #define PROBE(slot) do {} while (0)
 #define PROBE_TICK() do {} while (0)
+#define PROBE_BEGIN() do {} while (0)
+#define PROBE_FLUSH() do {} while (0)
 #endif
 
 /* ordered compaction within a warp group (see block_prefix) */
@@ -137,7 +149,7 @@ struct TickLayout {
   int stg_rR, stg_cR;            /* [rows] / [kRowChunkCells] 2 x double2: divisor reciprocals */
   int stg_row, stg_ti;           /* [rows] int                                             */
   int stg_tv, stg_wv;            /* [kRowChunkCells] int / float                           */
-  int w_dsup, w_act, w_spkl, w_pi, w_w;
+  int w_dsup, w_act, w_spkl, w_pi, w_w, w_lg;
   int w_spkp;                    /* [2][M] int: spike lists by tick parity (deferred columns) */
   int w_spk, w_skip;             /* bytes                                                  */
   int st_dsup, st_act, st_cnt;
@@ -171,6 +183,7 @@ __host__ __device__ inline void tick_layout(int M, int n_in, const int* C, TickL
   L.stg_tv = o; o += kRowChunkCells;
   L.stg_wv = o; o += kRowChunkCells;
   L.w_dsup = o; o += M;
+  L.w_lg = o; o += M;
   L.w_act = o; o += M;
   L.w_spkl = o; o += M;
   L.w_pi = o; o += rows;
@@ -282,6 +295,8 @@ __device__ __forceinline__ void stage_rows(const ProjDev& J, const int* list, in
   }
 }
 
+__device__ __forceinline__ bool tid_is_zero() { return threadIdx.x == 0; }
+
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -329,6 +344,70 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int target
   return *s_ok != 0;
 }
 
+__device__ __forceinline__ unsigned long long load_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void store_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+/* The two halves of grid_sync, for a CTA that has work to do between its
+   arrival and the point where it needs the others' arrivals: grid_arrive
+   after a __syncthreads (the release covers every write of the CTA before
+   it), grid_wait before the next reads of other CTAs' data.  grid_wait with
+   a seed slot (NetDev::seed64) also fetches the population's softmax seed
+   for the tick it opens: the barrier thread loads the slot beside every poll
+   of the arrival counter, so the value is usually in hand when the barrier
+   completes; a slot whose tag is not `tag` yet is read again after the
+   completing acquire, which orders it after the publisher's store (made
+   before the publisher's release arrival).  *s_seed gets the float. */
+__device__ __forceinline__ void grid_arrive(unsigned int* bar) {
+  if (threadIdx.x == 0) atomic_add_release(bar, 1u);
+}
+
+__device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target, int* err, int* s_ok,
+                                          const unsigned long long* seed, unsigned int tag, float* s_seed) {
+  if (threadIdx.x == 0) {
+    unsigned long long t0 = globaltimer_ns();
+    int ok = 1;
+    unsigned long long sv = 0;
+    for (;;) {
+      if (seed) sv = load_relaxed_u64(seed);
+      if (load_acquire(bar) >= target) break;
+      if (*(volatile int*)err) {
+        ok = 0;
+        break;
+      }
+      if (globaltimer_ns() - t0 > kBarrierNs) {
+        atomicOr(err, kErrBarrier);
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+    if (ok && seed) {
+      if ((unsigned int)(sv >> 32) != tag) sv = load_acquire_u64(seed);
+      if ((unsigned int)(sv >> 32) != tag) {
+        atomicOr(err, kErrSeed);
+        ok = 0;
+      }
+      *s_seed = __uint_as_float((unsigned int)sv);
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
 /* Failure-detection self-test: every CTA enters grid_sync with a target one
    arrival above the grid size, which nothing provides, so each wait runs out
    after limit_ns, sets kErrBarrier in *err and returns. */
@@ -338,88 +417,129 @@ __global__ void barrier_probe_kernel(unsigned int* bar, int* err, unsigned long 
 }
 
 /* Deferred column updates, Proj.cpp:481-536, of the MCUs that spiked in the
-   tick at `simstep`.  Units [beg, end) of the ring half are split evenly over
-   the CTAs of the grid; the calling group (gsize kGroup, named barrier bar_id)
-   does this CTA's share, then signals each unit's owner CTA with a release add
-   on col_done[owner].  A unit's slots were published by their owner after its
-   row updates of that tick, so every cell sees the row update first, as in
-   gsbn (rows, then columns). */
+   tick at `simstep`.  Units [beg, *tail) of the ring half go round robin to
+   the CTAs of the grid (unit b + i*G to CTA b); the calling group (kGroup
+   threads, named barrier bar_id) does this CTA's units, kHelpUnits at a time,
+   then signals each unit's owner CTA with a release add on col_done[owner].
+   The descriptors of the first units are loaded beside the tail count (one
+   round trip for both; a descriptor beyond the tail is never used), and the
+   projection and decay constants come from the CTA's shared copies when the
+   unit's projection is one of them.  A unit's slots were published by their
+   owner after its row updates of that tick, so every cell sees the row update
+   first, as in gsbn (rows, then columns). */
+constexpr int kCellsPerUnit = kColUnit / kGroup;          /* cells of one unit per thread */
+constexpr int kHelpUnits = kCellsPerUnit >= 2 ? 1 : 2;    /* units per pass */
+
 template <int kF64>
 __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, const RunParams* __restrict__ rp,
-                                             const int4* __restrict__ ring, unsigned beg, unsigned end, int simstep,
-                                             unsigned int* col_done, int gtid, int bar_id) {
-  const unsigned n = end - beg, G = gridDim.x;
-  const unsigned per = (n + G - 1) / G;
-  const unsigned lo = min(n, blockIdx.x * per), hi = min(n, lo + per);
+                                             const int4* __restrict__ ring, unsigned beg,
+                                             const unsigned int* tail, int simstep, unsigned int* col_done,
+                                             int gtid, int bar_id, unsigned int* s_end, const int* s_inp,
+                                             const ProjDev* s_proj, const TabRef* s_tab, int n_in) {
+  const unsigned G = gridDim.x;
   const unsigned cap = (unsigned)net->col_cap;
   const float prn = rp->prn;
-  const int ncell = (int)(hi - lo) * kColUnit;
-  for (int b0 = 0; b0 < ncell; b0 += kColU * kGroup) {
-    size_t index[kColU];
-    int tv[kColU], pj[kColU];
-    float4 cv[kColU];
-    bool ok[kColU];
+  PROBE_DECL;
+  int4 d[kHelpUnits];
 #pragma unroll
-    for (int u = 0; u < kColU; ++u) {
-      const int k = b0 + u * kGroup + gtid;
-      ok[u] = false;
-      if (k < ncell) {
-        const int4 d = __ldcg(ring + (beg + lo + (unsigned)(k / kColUnit)) % cap);
-        const int r = k % kColUnit;
-        if (r < (d.w >> 16)) {
-          const ProjDev& J = net->projs[d.y];
-          const int row = d.z + r;
-          index[u] = (size_t)row * J.M + (d.w & 0xffff);
-          ok[u] = J.ii[row] >= 0;
-          pj[u] = d.y;
-          tv[u] = __ldcg(J.tij + index[u]);
-          cv[u] = __ldcg(J.cell + index[u]);
-        }
-      }
-    }
-    float4 tA[kColU], tB[kColU];
-    double2 tR0[kColU], tR1[kColU];
-#pragma unroll
-    for (int u = 0; u < kColU; ++u) {
-      if (!ok[u]) continue;
-      const TabRef& T = rp->tabs[pj[u]];
-      const int pdt = simstep - tv[u];
-      if (pdt > 0 && pdt < T.len) {
-        tA[u] = T.tab[(size_t)pdt * 4 + 0];
-        tB[u] = T.tab[(size_t)pdt * 4 + 1];
-        tR0[u] = T.rtab[(size_t)pdt * 4 + 0];
-        tR1[u] = T.rtab[(size_t)pdt * 4 + 1];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kColU; ++u) {
-      if (!ok[u]) continue;
-      const ProjDev& J = net->projs[pj[u]];
-      const int pdt = simstep - tv[u];
-      float4 c4 = cv[u];
-      if (pdt <= 0) {
-        c4.w += J.kftj;
-      } else {
-        const Coef k = make_coef(J.taupdt * prn, J.ke, J.kzi, J.kzj, kF64);
-        float4 A = tA[u], B = tB[u];
-        double2 R0 = tR0[u], R1 = tR1[u];
-        if (pdt >= rp->tabs[pj[u]].len) {
-          if (kF64)
-            table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, B, 1);
-          else
-            cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
-          recip_part(A, B, 0, R0, R1);
-        }
-        c4 = cell_step_nl(c4, k, rp->tabs[pj[u]].rk, A, B, R0, R1);
-        c4.w = c4.w + J.kftj;
-      }
-      J.cell[index[u]] = c4;
-      J.tij[index[u]] = simstep;
-    }
-  }
+  for (int u = 0; u < kHelpUnits; ++u) d[u] = __ldcg(ring + (beg + blockIdx.x + (unsigned)u * G) % cap);
+  if (gtid == 0) *s_end = __ldcg(tail);
   group_sync(bar_id);
-  if (gtid == 0)
-    for (unsigned u = lo; u < hi; ++u) atomic_add_release(&col_done[__ldcg(ring + (beg + u) % cap).x], 1u);
+  const unsigned n = *s_end - beg;
+  for (unsigned u0 = blockIdx.x; u0 < n; u0 += kHelpUnits * G) {
+    if (u0 != blockIdx.x) {
+#pragma unroll
+      for (int u = 0; u < kHelpUnits; ++u)
+        if (u0 + u * G < n) d[u] = __ldcg(ring + (beg + u0 + (unsigned)u * G) % cap);
+    }
+    size_t index[kHelpUnits][kCellsPerUnit];
+    int tv[kHelpUnits][kCellsPerUnit];
+    float4 cv[kHelpUnits][kCellsPerUnit];
+    bool ok[kHelpUnits][kCellsPerUnit];
+    const ProjDev* Jp[kHelpUnits];
+    const TabRef* Tp[kHelpUnits];
+#pragma unroll
+    for (int u = 0; u < kHelpUnits; ++u) {
+      const bool valid = u0 + u * G < n;
+      Jp[u] = nullptr;
+      Tp[u] = nullptr;
+      if (valid) {
+        for (int q = 0; q < n_in; ++q)
+          if (s_inp[q] == d[u].y) {
+            Jp[u] = &s_proj[q];
+            Tp[u] = &s_tab[q];
+          }
+        if (!Jp[u]) {
+          Jp[u] = &net->projs[d[u].y];
+          Tp[u] = &rp->tabs[d[u].y];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < kCellsPerUnit; ++c) {
+        const int r = c * kGroup + gtid;
+        ok[u][c] = false;
+        if (valid && r < (d[u].w >> 16)) {
+          const ProjDev& J = *Jp[u];
+          const int row = d[u].z + r;
+          index[u][c] = (size_t)row * J.M + (d[u].w & 0xffff);
+          ok[u][c] = J.ii[row] >= 0;
+          tv[u][c] = __ldcg(J.tij + index[u][c]);
+          cv[u][c] = __ldcg(J.cell + index[u][c]);
+        }
+      }
+    }
+    PROBE(3); /* B slot 19 */
+    float4 tA[kHelpUnits][kCellsPerUnit], tB[kHelpUnits][kCellsPerUnit];
+    double2 tR0[kHelpUnits][kCellsPerUnit], tR1[kHelpUnits][kCellsPerUnit];
+#pragma unroll
+    for (int u = 0; u < kHelpUnits; ++u)
+#pragma unroll
+      for (int c = 0; c < kCellsPerUnit; ++c) {
+        if (!ok[u][c]) continue;
+        const TabRef& T = *Tp[u];
+        const int pdt = simstep - tv[u][c];
+        if (pdt > 0 && pdt < T.len) {
+          tA[u][c] = T.tab[(size_t)pdt * 4 + 0];
+          tB[u][c] = T.tab[(size_t)pdt * 4 + 1];
+          tR0[u][c] = T.rtab[(size_t)pdt * 4 + 0];
+          tR1[u][c] = T.rtab[(size_t)pdt * 4 + 1];
+        }
+      }
+#pragma unroll
+    for (int u = 0; u < kHelpUnits; ++u)
+#pragma unroll
+      for (int c = 0; c < kCellsPerUnit; ++c) {
+        if (!ok[u][c]) continue;
+        const ProjDev& J = *Jp[u];
+        const int pdt = simstep - tv[u][c];
+        float4 c4 = cv[u][c];
+        if (pdt <= 0) {
+          c4.w += J.kftj;
+        } else {
+          float4 A = tA[u][c], B = tB[u][c];
+          double2 R0 = tR0[u][c], R1 = tR1[u][c];
+          if (pdt >= Tp[u]->len) {
+            const Coef k = make_coef(J.taupdt * prn, J.ke, J.kzi, J.kzj, kF64);
+            if (kF64)
+              table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, B, 1);
+            else
+              cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
+            recip_part(A, B, 0, R0, R1);
+          }
+          c4 = cell_step_nl(c4, Tp[u], A, B, R0, R1);
+          c4.w = c4.w + J.kftj;
+        }
+        J.cell[index[u][c]] = c4;
+        J.tij[index[u][c]] = simstep;
+      }
+    PROBE(4); /* B slot 20 */
+    group_sync(bar_id);
+    PROBE(5); /* B slot 21 */
+    if (gtid == 0)
+#pragma unroll
+      for (int u = 0; u < kHelpUnits; ++u)
+        if (u0 + u * G < n) atomic_add_release(&col_done[d[u].x], 1u);
+  }
 }
 
 /* Ticks it0 .. it0+n_ticks-1 of the run for this CTA's (population, HCU). */
@@ -430,19 +550,34 @@ __device__ __forceinline__ void help_columns(const NetDev* __restrict__ net, con
    ring) or done by the CTA itself in the tick (one launch per tick); each
    instance holds only its own form. */
 template <int kF64, int kDefer>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* __restrict__ net,
-                                                         const RunParams* __restrict__ rp, int it0, int n_ticks,
+__global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* __restrict__ net_g,
+                                                         const RunParams* __restrict__ rp_g, int it0, int n_ticks,
                                                          unsigned int* bar) {
   extern __shared__ __align__(16) float sm[];
+  /* the network descriptor and the run's parameters, read every tick: shared
+     copies, so that no read of them waits on an L1 miss behind the cell
+     traffic of the tick */
+  __shared__ NetDev s_net;
+  __shared__ RunParams s_rp;
+  if (threadIdx.x == 0) {
+    s_net = *net_g;
+    s_rp = *rp_g;
+  }
+  __syncthreads();
+  const NetDev* __restrict__ net = &s_net;
+  const RunParams* __restrict__ rp = &s_rp;
   __shared__ int s_warpA[kGroupWarps];
   __shared__ float s_red[kGroupWarps];
   __shared__ int s_totalA;
   __shared__ float s_dsup0;
+  __shared__ float s_wm;
   __shared__ float s_vsum;
   __shared__ int s_flag9;
   __shared__ int s_nspk;
   __shared__ int s_ok;
-  __shared__ unsigned int s_hbeg, s_hend, s_upos, s_exp_total, s_last_end[2];
+  __shared__ unsigned int s_hend, s_upos, s_exp_total, s_last_end[2];
+  /* cell updates of the launch, added to NetDev::counters once at its end */
+  __shared__ unsigned long long s_rows_acc, s_cols_acc;
   __shared__ int s_nspkp[2];
   __shared__ int s_dq[kDQ * kGroupWarps];
 
@@ -484,11 +619,23 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   unsigned int* const col_tail = bar + 1;
   unsigned int* const col_done = bar + 4;
 
-  int Cq[kMaxIn];
+  /* the shared-memory layout lives in shared memory itself: indexed by
+     projection at run time, a register copy would sit in local memory, whose
+     per-thread frames (x 512 threads) do not fit in L1 next to this kernel's
+     shared memory, and every read would be an L2 round trip */
+  __shared__ TickLayout s_L;
+  __shared__ int s_C[kMaxIn];
+  if (tid_is_zero()) {
+    int c[kMaxIn];
 #pragma unroll
-  for (int q = 0; q < kMaxIn; ++q) Cq[q] = q < n_in ? s_proj[q].C : 0;
-  TickLayout L;
-  tick_layout(M, n_in, Cq, L);
+    for (int q = 0; q < kMaxIn; ++q) c[q] = q < n_in ? s_proj[q].C : 0;
+#pragma unroll
+    for (int q = 0; q < kMaxIn; ++q) s_C[q] = c[q];
+    tick_layout(M, n_in, c, s_L);
+  }
+  __syncthreads();
+  const TickLayout& L = s_L;
+  const int* Cq = s_C;
 
   float* w_dsup = sm + L.w_dsup;
   float* w_act = sm + L.w_act;
@@ -498,6 +645,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   int8_t* w_spk = (int8_t*)(sm + L.w_spk);
   int* w_spkp = (int*)(sm + L.w_spkp);
   int8_t* w_skip = (int8_t*)(sm + L.w_skip);
+  float* w_lgc = sm + L.w_lg;
   float* st_dsup = sm + L.st_dsup;
   float* st_act = sm + L.st_act;
   int* st_cnt = (int*)(sm + L.st_cnt);
@@ -535,10 +683,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       for (int w = tid; w < V.W; w += kBlock) V.bits[cur0 * V.W + w] = 0u;
       if (tid == 0) V.nlist[cur0] = J.list_cnt[h];
     }
+    /* the run's stimulus of this HCU (constant within the launch) */
+    for (int j = tid; j < M; j += kBlock) w_lgc[j] = rp->lginp[pop.mcu_start + h * M + j];
     if (tid == 0) {
+      s_rows_acc = 0;
+      s_cols_acc = 0;
       s_exp_total = 0;
       s_last_end[0] = s_last_end[1] = 0;
       s_nspkp[0] = s_nspkp[1] = 0;
+      s_wm = rp->wmask[pop.hcu_start + h];
     }
   }
   __syncthreads();
@@ -558,10 +711,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                L, tid, kBlock);
   }
 
+  PROBE_BEGIN();
   PROBE_DECL;
   for (int it = it0; it < it0 + n_ticks; ++it) {
     if (it > it0) {
-      if (!grid_sync(bar, (unsigned int)(it - it0) * gridDim.x, net->err, &s_ok)) return;
+      /* this CTA arrived at the end of the previous tick (grid_arrive) */
+      if (!grid_wait(bar, (unsigned int)(it - it0) * gridDim.x, net->err, &s_ok,
+                     (defer && h != 0) ? net->seed64 + P : nullptr, rp->serial0 + (unsigned int)(it - it0),
+                     &s_dsup0))
+        return;
     } else {
       __syncthreads();
     }
@@ -589,16 +747,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         float noise = 0.0f;
         if (pop.snoise != 0.0f)
           noise = pop.snoise * dev_normal01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
-        float sup = pop.lgbias + pop.igain * lginp[idx] + noise;
-        sup += (pop.wgain * wmask[h]) * wsup;
+        float sup = pop.lgbias + pop.igain * w_lgc[j] + noise;
+        sup += (pop.wgain * s_wm) * wsup;
         float d = st_dsup[j];
         w_dsup[j] = d + (sup - d) * pop.taumdt;
       }
       PROBE(1);
       /* the softmax max of every HCU is seeded with the population's first
          MCU (Pop.cpp:270), published by HCU 0's CTA in the previous tick */
+      /* in a launch's first tick (or without the deferred-column form) from
+         global memory; later the barrier brought it (grid_wait) */
       const int tseed = (M < kGroup) ? kGroup - 1 : 0;
-      if (gtid == tseed && h != 0) {
+      if (gtid == tseed && h != 0 && (it == it0 || !defer)) {
         float wsup = 0.0f;
         int offset = 0;
         for (int m = 0; m < pop.dim_proj; m++) {
@@ -617,6 +777,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       float tmax = seed0;
       for (int j = gtid; j < M; j += kGroup) tmax = (w_dsup[j] > tmax) ? w_dsup[j] : tmax;
       const float maxdsup = group_max(tmax, gtid, kBarA, s_red);
+      PROBE(10);
       const float maxact = bx_expf(pop.wtagain * maxdsup);
       for (int j = gtid; j < M; j += kGroup) {
         float a = bx_expf(pop.wtagain * (w_dsup[j] - maxdsup));
@@ -624,6 +785,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         w_act[j] = a;
       }
       group_sync(kBarA);
+      PROBE(11);
       if (gtid == 0) {
         /* serial, in MCU order (Pop.cpp:281-293) */
         float vsum = 0.0f;
@@ -666,6 +828,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         st_cnt[j] += spk;
         w_spk[j] = spk;
       }
+      PROBE(12);
       if (h == 0 && gtid == 0) pop.dsup[cur][0] = w_dsup[0];
       /* external spike replay overrides the sampled spikes (Pop.cpp:389-409) */
       if (pop.ext) {
@@ -717,7 +880,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
         const float4* tab = s_tab[q].tab;
         const double2* rtab = s_tab[q].rtab;
-        const RCoef& rk = s_tab[q].rk;
         const int tlen = s_tab[q].len;
         const size_t eoff = (size_t)J.proj_in_pop * n;
 
@@ -836,7 +998,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                 recip_part(A, B, 2, R0, R1);
               }
               {
-                const float4 rt = row_step_nl(make_float4(pi, ei, zi, 0.0f), k, rk, A, B, R0, R1);
+                const float4 rt = row_step_nl(make_float4(pi, ei, zi, 0.0f), &s_tab[q], A, B, R0, R1);
                 pi = rt.x;
                 ei = rt.y;
                 zi = rt.z;
@@ -867,7 +1029,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                 load_entry(tab, tlen, k, pdt, 0, A, B);
                 recip_part(A, B, 0, R0, R1);
               }
-              cv = cell_step_nl(cv, k, rk, A, B, R0, R1);
+              cv = cell_step_nl(cv, &s_tab[q], A, B, R0, R1);
               cv.z = cv.z + J.kfti;
               J.cell[index] = cv;
               J.tij[index] = simstep;
@@ -907,25 +1069,55 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           if (s_flag9) f |= 1;
           if (h == 9 / M && 9 < n && w_spk[9 - h * M] > 0) f |= 2;
           if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + p], f);
-          atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
+          s_rows_acc += (unsigned long long)nrow * M;
         }
+      }
+      /* HCU 0 publishes the next tick's softmax seed, dsup of MCU 0 after
+         that tick's support step (NetDev::seed64): its terms are final now
+         (the deferred columns leave epsc and bj alone), and this thread's
+         barrier arrival releases the store */
+      if (defer && h == 0 && gtid == 0 && it + 1 < it0 + n_ticks) {
+        float wsup = 0.0f;
+        for (int m = 0; m < pop.dim_proj; m++) {
+          const float* b = sm + L.st_q[m];
+          wsup += b[4 * M] + b[3 * M];   /* bj + epsc of MCU 0 */
+        }
+        float noise = 0.0f;
+        if (pop.snoise != 0.0f) noise = pop.snoise * dev_normal01(pop.rng_seed, pop.rng_pop, (uint32_t)(simstep + 1), 0u);
+        float sup = pop.lgbias + pop.igain * w_lgc[0] + noise;
+        sup += (pop.wgain * s_wm) * wsup;
+        const float d = st_dsup[0];
+        const float next = d + (sup - d) * pop.taumdt;
+        store_relaxed_u64(net->seed64 + P, ((unsigned long long)(rp->serial0 + (unsigned int)(it + 1 - it0)) << 32) |
+                                               __float_as_uint(next));
       }
       /* rows done: group B may now update column cells of active rows */
       if (!defer) asm volatile("bar.arrive %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
       PROBE(7);
     } else {
       /* ================= group B: delay queue, columns =================== */
+      /* the delay queue's first spike flags (first projection, first chunk of
+         slots), loaded now so that their round trip overlaps the column work;
+         one byte per chunk, packed in one register */
+      uint32_t dq_pre = 0;
+      if (n_in > 0) {
+        const ProjDev& J0 = s_proj[0];
+        const int* ii0 = qview(sm, L, 0, M, J0.C).ii;
+        const int8_t* si0 = J0.si[prev];
+#pragma unroll
+        for (int u = 0; u < kDQ; ++u) {
+          const int s = u * kGroup + gtid;
+          if (s < J0.C) {
+            const int src = ii0[s];
+            if (src >= 0 && src < J0.Ns) dq_pre |= (uint32_t)(uint8_t)__ldcg(si0 + src) << (8 * u);
+          }
+        }
+      }
       if (defer) {
         /* the grid's column units of the previous tick, this CTA's share */
-        if (gtid == 0) {
-          const unsigned int e = __ldcg(col_tail + prev);
-          s_hbeg = s_last_end[prev];
-          s_hend = e;
-          s_last_end[prev] = e;
-        }
-        group_sync(kBarB);
-        help_columns<kF64>(net, rp, net->col_ring + (size_t)prev * net->col_cap, s_hbeg, s_hend, simstep - 1, col_done,
-                           gtid, kBarB);
+        help_columns<kF64>(net, rp, net->col_ring + (size_t)prev * net->col_cap, s_last_end[prev], col_tail + prev,
+                           simstep - 1, col_done, gtid, kBarB, &s_hend, s_inp, s_proj, s_tab, n_in);
+        if (gtid == 0) s_last_end[prev] = s_hend;
       }
       PROBE(10);
       for (int q = 0; q < n_in; ++q) {
@@ -947,7 +1139,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           for (int u = 0; u < kDQ; ++u) {
             const int s = s0 + u * kGroup + gtid;
             sv[u] = 0;
-            if (s < C) {
+            if (q == 0 && s0 == 0) {
+              sv[u] = (int8_t)(dq_pre >> (8 * u));
+            } else if (s < C) {
               const int src = V.ii[s];
               if (src >= 0 && src < J.Ns) sv[u] = __ldcg(si + src);
             }
@@ -977,7 +1171,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
               if (s < C) nbits[s >> 5] = mb[u];
             }
           }
+          PROBE(1); /* B slot 17 */
           group_sync(kBarB);
+          PROBE(2); /* B slot 18 */
           /* slots in ascending order: chunk by chunk, warp by warp, lane by lane */
           int run = 0;
 #pragma unroll
@@ -1005,19 +1201,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       if (defer) {
         /* publish this tick's column units; the grid does them next tick */
         for (int i = gtid; i < nspk; i += kGroup) w_spkp[cur * M + i] = w_spkl[i];
-        int parts[kMaxIn];
+        auto parts = [&](int q) { return (Cq[q] + kColUnit - 1) / kColUnit; };
         int nunits = 0;
-#pragma unroll
-        for (int q = 0; q < kMaxIn; ++q) {
-          parts[q] = q < n_in ? (Cq[q] + kColUnit - 1) / kColUnit : 0;
-          nunits += nspk * parts[q];
-        }
+        for (int q = 0; q < n_in; ++q) nunits += nspk * parts(q);
         if (gtid == 0) {
           s_nspkp[cur] = nspk;
           if (nunits > 0) {
             s_upos = atomicAdd(col_tail + cur, (unsigned int)nunits);
             s_exp_total += (unsigned int)nunits;
-            for (int q = 0; q < n_in; ++q) atomicAdd(&net->counters[1], (unsigned long long)nspk * Cq[q]);
+            for (int q = 0; q < n_in; ++q) s_cols_acc += (unsigned long long)nspk * Cq[q];
           }
         }
         group_sync(kBarB);
@@ -1026,11 +1218,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           int4* ring = net->col_ring + (size_t)cur * net->col_cap;
           for (int u = gtid; u < nunits; u += kGroup) {
             int q = 0, uu = u;
-            while (uu >= nspk * parts[q]) {
-              uu -= nspk * parts[q];
+            while (uu >= nspk * parts(q)) {
+              uu -= nspk * parts(q);
               ++q;
             }
-            const int i = uu / parts[q], part = uu - i * parts[q];
+            const int i = uu / parts(q), part = uu - i * parts(q);
             const int C = Cq[q];
             const int rows = min(kColUnit, C - part * kColUnit);
             ring[(pos + (unsigned int)u) % cap] =
@@ -1053,8 +1245,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
           const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj, kF64);
           const float4* tab = s_tab[q].tab;
           const double2* rtab = s_tab[q].rtab;
-          const RCoef& rk = s_tab[q].rk;
-          const int tlen = s_tab[q].len;
+            const int tlen = s_tab[q].len;
           const uint32_t* cbits = V.bits + cur * V.W;
           const int* clist = V.list + cur * C;
           const int ncol = (pass == 0) ? nspk * C : V.nlist[cur] * nspk;
@@ -1117,22 +1308,26 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
                     cell_factors(k.kp, k.ke, k.kzi, k.kzj, pdt, A, B);
                   recip_part(A, B, 0, R0, R1);
                 }
-                c4 = cell_step_nl(c4, k, rk, A, B, R0, R1);
+                c4 = cell_step_nl(c4, &s_tab[q], A, B, R0, R1);
                 c4.w = c4.w + J.kftj;
               }
               J.cell[index[u]] = c4;
               J.tij[index[u]] = simstep;
             }
           }
-          if (pass == 0 && gtid == 0) atomicAdd(&net->counters[1], (unsigned long long)nspk * C);
+          if (pass == 0 && gtid == 0) s_cols_acc += (unsigned long long)nspk * C;
         }
       }
     }
     PROBE(13);
     __syncthreads();
     PROBE(8);
+    /* every write of this tick is done: arrive now, and stage the next tick's
+       first row chunk while the others arrive (cells of that chunk that the
+       grid's column units of this tick change are refreshed after the
+       column wait) */
+    if (it + 1 < it0 + n_ticks) grid_arrive(bar);
 
-    /* stage the next tick's first row chunk before the barrier */
     if (it + 1 < it0 + n_ticks && n_in > 0) {
       const ProjDev& J = s_proj[0];
       QView V = qview(sm, L, 0, M, J.C);
@@ -1148,19 +1343,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
     if (!grid_sync(bar, (unsigned int)n_ticks * gridDim.x, net->err, &s_ok)) return;
     if (!groupA) {
       const int lastp = (rp->k0 + it0 + n_ticks - 1) & 1;
-      if (gtid == 0) {
-        const unsigned int e = __ldcg(col_tail + lastp);
-        s_hbeg = s_last_end[lastp];
-        s_hend = e;
-      }
-      group_sync(kBarB);
-      help_columns<kF64>(net, rp, net->col_ring + (size_t)lastp * net->col_cap, s_hbeg, s_hend,
-                         rp->simstep0 + it0 + n_ticks - 1, col_done, gtid, kBarB);
+      help_columns<kF64>(net, rp, net->col_ring + (size_t)lastp * net->col_cap, s_last_end[lastp], col_tail + lastp,
+                         rp->simstep0 + it0 + n_ticks - 1, col_done, gtid, kBarB, &s_hend, s_inp, s_proj, s_tab,
+                         n_in);
     }
   }
 
   /* ---- write the resident state back (buffers of the last tick) --------- */
+  PROBE_FLUSH();
   __syncthreads();
+  if (tid == 0) {
+    if (s_rows_acc) atomicAdd(&net->counters[0], s_rows_acc);
+    if (s_cols_acc) atomicAdd(&net->counters[1], s_cols_acc);
+  }
   {
     const int last = (rp->k0 + it0 + n_ticks - 1) & 1;
     const int next = last ^ 1;

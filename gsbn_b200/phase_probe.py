@@ -23,10 +23,13 @@ import numpy as np
 
 from gsbn_b200 import capi, extgen, schema, workloads
 
-PHASES_A = ["barrier wait", "support", "softmax", "spikes", "j-traces", "column wait + refresh", "rows",
-            "end of rows", "join wait", "staging next chunk"]
-PHASES_B = {16: "barrier wait", 26: "column units of the grid", 27: "delay queue", 28: "spike wait",
-            29: "unit publication", 24: "join wait", 25: "staging next chunk"}
+PHASES_A = {0: "barrier wait", 1: "support", 10: "softmax: max", 11: "softmax: exp", 2: "softmax: sum",
+            12: "spikes: sampling", 3: "spikes: list, publish", 4: "j-traces", 5: "column wait + refresh",
+            6: "rows", 7: "end of rows", 8: "join wait", 9: "staging next chunk"}
+PHASES_B = {16: "barrier wait", 26: "column units of the grid", 19: "  units: ring, cell loads",
+            20: "  units: tables, decay, store", 21: "  units: group sync", 17: "delay queue: loads, ballots",
+            18: "delay queue: sync", 27: "delay queue: list", 28: "spike wait", 29: "unit publication",
+            24: "join wait", 25: "staging next chunk"}
 
 
 def main():
@@ -52,6 +55,8 @@ def main():
     net.upload_stimuli_idx(lgidx, float(np.float32(sp.gen_param.eps)), wmask)
     out, counts = {}, {}
     for name, sel in (("training", runs[1:1 + a.train]), ("recall", runs[first_recall + 1:first_recall + 1 + a.recall])):
+        if not sel:
+            continue
         # run up to the selection without the probe, then the selection with it
         net.reset()
         for r in runs[:runs.index(sel[0])]:
@@ -70,12 +75,12 @@ def main():
     for name, pt in out.items():
         print(f"== {name} segments: us per tick at {a.mhz:.0f} MHz (median CTA / slowest CTA)")
         tot = 0.0
-        for k, ph in enumerate(PHASES_A):
+        for k, ph in PHASES_A.items():
             med, mx = float(np.median(pt[:, k])), float(pt[:, k].max())
             tot += med
             print(f"  A {ph:<24} {med:7.3f} {mx:7.3f}")
         print(f"  A {'total (median)':<24} {tot:7.3f}")
-        for k, ph in sorted(PHASES_B.items()):
+        for k, ph in PHASES_B.items():
             print(f"  B {ph:<24} {float(np.median(pt[:, k])):7.3f} {float(pt[:, k].max()):7.3f}")
         slow, fast = float(counts[name][:, 14].sum()), float(counts[name][:, 15].sum())
         print(f"  decays: {fast:.0f} by the reciprocal form, {slow:.0f} by the div_rn fallback "
