@@ -543,72 +543,91 @@ def run_multi_extension(dev, steps, warmup, ring=25, cpu=True):
 
 def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
     """The batching extension: 256 independent networks of uneven size (HCUs
-    8-64, MCUs 5-50, full recurrent), 20 patterns each, advanced together under
-    the schedule the tuner picks, against the plain path (one network per
-    launch, one after the other) on the same first ticks."""
+    8-64, MCUs 5-50, full recurrent), 20 patterns each, advanced together by
+    the batch engine (one persistent kernel per run) under the launch shape its
+    tuner picks, against the plain path (one network per launch, one after the
+    other) on the same first ticks."""
     import torch
     from gsbn_b200 import batch
     members = batch.make_members(n_nets)
     runs = batch.schedule(20, train_ticks=100, recall_ticks=50)
     ticks = sum(r[1] for r in runs)
-    cache = os.path.join(tempfile.mkdtemp(prefix="gsbn_tune_"), "tune.json")
-    best, tune_times = batch.tune(members, device=dev, probe_ticks=20, cache=cache)
+    eng = batch.BatchEngine(members, device=dev, max_ticks=128)
+    t0 = time.perf_counter()
+    shape, tune_us = eng.tune(20, train_rows=(0, 0), recall_rows=(20, 1))
+    tune_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
 
-    def timed(b, rs):
-        """device time of the runs rs: events on every group's stream, from the
-        first start to the last end"""
-        torch.cuda.synchronize()
-        starts, ends = [], []
-        for g in b.groups:
-            st = torch.cuda.ExternalStream(g.net.stream(), device=dev)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            starts.append(e0)
-            ends.append((e1, st))
-        for r in rs:
-            b.run_segment(*r)
-        for e1, st in ends:
-            e1.record(st)
-        torch.cuda.synchronize()
-        return max(starts[0].elapsed_time(e1) for e1, _ in ends) * 1e-3
+    def step():
+        eng.reset()
+        for r in runs:
+            eng.run_segment(*r)
 
-    groups = batch.partition(members, best[0], best[1])
-    b = batch.Batch(members, groups, device=dev, threads=best[2])
-    b.run_segment(*runs[0])  # warm-up (graphs, tables)
-    b.sync()
-    l0, c0 = b.launches(), b.counters()
-    secs = []
+    step()  # warm-up: tables, the first catch-ups
+    eng.sync()
+    c0, l0 = eng.counters(), eng.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
     for _ in range(steps):
-        b.reset()
-        secs.append(timed(b, runs))
-    cells = (b.counters() - c0) / steps
-    launches = (b.launches() - l0) / steps
+        step()
+    e1.record(stream)
+    eng.sync()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) * 1e-3 / steps
+    c1 = eng.counters()
+    row, col, allc = [(c1[k] - c0[k]) / steps for k in range(3)]
+    cells = row + col + allc
+    launches = (eng.launches() - l0) / steps
     head = [r for r in runs if r[0] <= head_ticks]
     n_head = sum(r[1] for r in head)
-    b.reset()
-    t_head_best = timed(b, head)
-    b.close()
-    plain = batch.Batch(members, batch.partition(members, "plain"), device=dev)
-    plain.run_segment(*runs[0])
+    eng.reset()
+    torch.cuda.synchronize()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for r in head:
+        eng.run_segment(*r)
+    h1.record(stream)
+    eng.sync()
+    t_head_batch = h0.elapsed_time(h1) * 1e-3
+    eng.close()
+    plain = batch.Plain(members, device=dev)
+    plain.run_segment(1, 2, 1.0, 0.0, 0, 0)  # warm-up: tables, graphs
     plain.sync()
     plain.reset()
-    c1 = plain.counters()
-    t_head_plain = timed(plain, head)
-    plain_cells = plain.counters() - c1
+    plain.sync()
+    pc0 = plain.counters()
+    t0 = time.perf_counter()
+    for r in head:
+        for net in plain.nets:
+            net.use_stimulus(r[4], r[5])
+            net.run(*r[:4])
+            net.sync()
+    t_head_plain = time.perf_counter() - t0
+    plain_cells = plain.counters() - pc0
     plain.close()
-    sec = statistics.mean(secs)
+    pk, pk_kind = peaks()
+    # algorithmic bytes: 44 B per row cell and all-cells cell, 40 B per column
+    # cell, 8 + 25 B per MCU per tick (one projection per member)
+    mcus = sum(m.H * m.M for m in members)
+    algo = 44 * (row + allc) + 40 * col + 33 * mcus * ticks
+    achieved = algo / sec / 1e9
     out = {
         "workload": f"{n_nets} independent networks, HCUs 8-64 x MCUs 5-50 (uniform), full recurrent, "
                     f"{sum(m.cells for m in members) / 1e6:.0f}M cells, 20 patterns each: "
                     f"{ticks} ticks (20 x 100 training + 20 x 50 recall)",
         "metric": "network ticks/s", "value": n_nets * ticks / sec, "unit": "network-ticks/s",
-        "cell_updates_per_s": cells / sec, "ms_per_step": sec * 1e3, "steps": steps,
-        "schedule": batch.cand_name(best), "groups": len(groups), "gpu_launches_per_step": launches,
-        "tuner_probe_s": tune_times,
+        "cell_updates_per_s": cells / sec, "ms_per_step": sec * 1e3, "us_per_tick": sec * 1e6 / ticks,
+        "steps": steps, "gpu_launches_per_step": launches,
+        "schedule": {"threads": shape[0], "cost_weights": list(shape[1:]), "tuner_us_per_tick": tune_us,
+                     "tuner_s": tune_s},
+        "roofline": {"bound": "hbm", "kernel": "batch_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_kind": pk_kind,
+                     "algorithmic_bytes_per_step": algo},
         "plain_one_network_per_launch": {"network_ticks_per_s": n_nets * n_head / t_head_plain,
                                          "cell_updates_per_s": plain_cells / t_head_plain, "ticks_timed": n_head},
-        "batched_same_ticks": {"network_ticks_per_s": n_nets * n_head / t_head_best},
-        "speedup_vs_plain_same_ticks": t_head_plain / t_head_best,
+        "batched_same_ticks": {"network_ticks_per_s": n_nets * n_head / t_head_batch},
+        "speedup_vs_plain_same_ticks": t_head_plain / t_head_batch,
     }
     if cpu:
         try:
@@ -973,6 +992,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extensions", action="store_true")
     ap.add_argument("--only-extensions", action="store_true", help="run the extension workloads alone (profiling)")
+    ap.add_argument("--batch-nets", type=int, default=256, help="networks of the batched extension")
+    ap.add_argument("--ext", default="bf16_recall,batched,procupdmulti",
+                    help="with --only-extensions: the extensions to run (comma separated)")
     ap.add_argument("--recall-replicates", type=int, default=4096)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -991,10 +1013,16 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.only_extensions:
         if rank == 0:
-            ext = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup, args.recall_replicates,
-                                                       cpu=cpu),
-                   "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
-                   "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
+            want = args.ext.split(",")
+            ext = {}
+            if "bf16_recall" in want:
+                ext["bf16_recall"] = run_recall_extension(local_rank, args.steps, args.warmup,
+                                                          args.recall_replicates, cpu=cpu)
+            if "batched" in want:
+                ext["batched"] = run_batch_extension(local_rank, max(1, args.steps // 2), n_nets=args.batch_nets,
+                                                     cpu=cpu)
+            if "procupdmulti" in want:
+                ext["procupdmulti"] = run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)
             print(json.dumps({"extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank, cpu=cpu)
@@ -1003,7 +1031,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_extensions:
         out["extensions"] = {"bf16_recall": run_recall_extension(local_rank, args.steps, args.warmup,
                                                                  args.recall_replicates, cpu=cpu),
-                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2), cpu=cpu),
+                             "batched": run_batch_extension(local_rank, max(1, args.steps // 2),
+                                                            n_nets=args.batch_nets, cpu=cpu),
                              "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
     if rank == 0:
         print(json.dumps(out), flush=True)

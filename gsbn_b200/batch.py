@@ -1,33 +1,27 @@
-"""Batches of independent networks on one GPU.
+"""Batches of independent networks on one GPU: ctypes binding of the batch
+engine (include/bcpnn_batch.h) and the batch workload.
 
 A batch member is a complete network of its own (one population with a full
-recurrent projection, its own patterns, connectivity and Philox seed).  Members
-are packed into groups; a group is built as one multi-population network
-through the C ABI, one population and one projection per member, each
-population keyed with its member's seed as population 0
-(bcpnn_set_pop_rng), so a member draws exactly the numbers, and computes
-exactly the state, it would as a network of its own.  Several groups run side
-by side on their own CUDA streams (one CUDA-graph-captured launch per tick
-each); a lone group whose HCUs all fit on the GPU at once runs one persistent
-launch per segment.
-
-The schedule (which members go together, and the CTA size of the tick
-kernel) is chosen by `tune`: it times each candidate on the first training
-ticks and keeps the fastest, cached by the member shapes.  Candidates:
-everything in one group; k groups of similar size (sorted by slots per HCU,
-so that a group's shared memory is sized for members like it); one group per
-member run one after the other (one network per launch, the plain path);
-each with 512-thread CTAs (one per SM) or 256-thread CTAs (two per SM, for
-small HCUs).
+recurrent projection, its own patterns, connectivity and Philox seed, keyed as
+population 0 of a network of its own), so it draws exactly the numbers, and
+computes exactly the state, it would alone.  The engine advances every member
+over the same ticks in one persistent kernel per run; its launch shape (CTA
+size, the cost model of the warp schedule) is chosen by its own tuner
+(bcpnn_batch_tune, C++), which times the candidates on training and recall
+ticks.
 """
-import hashlib
-import json
-import os
-import time
+import ctypes
 
 import numpy as np
 
 from . import capi, extgen, schema, workloads
+
+BATCH_EXPORTS = (
+    "bcpnn_batch_create", "bcpnn_batch_destroy", "bcpnn_batch_set_conn", "bcpnn_batch_upload_stimuli_idx",
+    "bcpnn_batch_use_stimulus", "bcpnn_batch_run", "bcpnn_batch_reset", "bcpnn_batch_sync", "bcpnn_batch_get_stream",
+    "bcpnn_batch_state_info", "bcpnn_batch_read_state", "bcpnn_batch_get_spike_log", "bcpnn_batch_counters",
+    "bcpnn_batch_kernel_launches", "bcpnn_batch_tune", "bcpnn_batch_last_error",
+)
 
 F32 = np.float32
 
@@ -78,149 +72,180 @@ def schedule(n_patterns, train_ticks=100, recall_ticks=50):
     return runs
 
 
-class Group:
-    """Members built as one multi-population network.  per_tick forces one
-    launch per tick (no cooperative persistent launch), which is what groups
-    that run side by side on several streams use: a persistent launch relies
-    on every CTA of its grid being resident at once."""
+class MemberDesc(ctypes.Structure):
+    _fields_ = [("pop", capi.PopDesc), ("proj", capi.ProjDesc), ("seed", ctypes.c_uint32)]
 
-    def __init__(self, members, dt=0.001, eps=1e-4, device=0, max_ticks=128, per_tick=False, threads=512):
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("n_members", ctypes.c_int32), ("members", ctypes.POINTER(MemberDesc)), ("dt", ctypes.c_float),
+                ("poisson_noise_hz", ctypes.c_float), ("device", ctypes.c_int32),
+                ("max_ticks_per_run", ctypes.c_int32), ("threads", ctypes.c_int32),
+                ("lpt_weights", ctypes.c_int32 * 3)]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    lib = capi.load()
+    vp, i32, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_size_t
+    P = ctypes.POINTER
+    sig = {
+        "bcpnn_batch_create": (ctypes.c_int, [P(BatchDesc), P(vp)]),
+        "bcpnn_batch_destroy": (ctypes.c_int, [vp]),
+        "bcpnn_batch_set_conn": (ctypes.c_int, [vp, i32, vp, vp, sz]),
+        "bcpnn_batch_upload_stimuli_idx": (ctypes.c_int, [vp, i32, i32, vp, ctypes.c_float, i32, vp]),
+        "bcpnn_batch_use_stimulus": (ctypes.c_int, [vp, i32, i32]),
+        "bcpnn_batch_run": (ctypes.c_int, [vp, i32, i32, ctypes.c_float, ctypes.c_float]),
+        "bcpnn_batch_reset": (ctypes.c_int, [vp]),
+        "bcpnn_batch_sync": (ctypes.c_int, [vp]),
+        "bcpnn_batch_get_stream": (ctypes.c_int, [vp, P(vp)]),
+        "bcpnn_batch_state_info": (ctypes.c_int, [vp, i32, ctypes.c_char_p, P(i32), P(sz)]),
+        "bcpnn_batch_read_state": (ctypes.c_int, [vp, i32, ctypes.c_char_p, vp, sz]),
+        "bcpnn_batch_get_spike_log": (ctypes.c_int, [vp, i32, vp, sz]),
+        "bcpnn_batch_counters": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
+        "bcpnn_batch_kernel_launches": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
+        "bcpnn_batch_tune": (ctypes.c_int, [vp, i32, i32, i32, i32, i32, P(i32), P(ctypes.c_float)]),
+        "bcpnn_batch_last_error": (ctypes.c_char_p, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class BatchEngine:
+    """The members on one GPU, driven through the batch C ABI."""
+
+    def __init__(self, members, dt=0.001, eps=1e-4, device=0, max_ticks=128, threads=512, lpt=(0, 0, 0),
+                 poisson_hz=0.0):
+        self._lib = load()
+        self._h = ctypes.c_void_p()
         self.members = members
-        pops = [m.pop for m in members]
-        projs = [dict(m.proj, src_pop=i, dest_pop=i) for i, m in enumerate(members)]
-        old = os.environ.get("GSBN_PER_TICK")
-        os.environ["GSBN_PER_TICK"] = "1" if per_tick else "0"
-        try:
-            self.net = capi.Net(pops, projs, dt, seed=0, device=device, max_ticks=max_ticks, tick_threads=threads)
-        finally:
-            if old is None:
-                del os.environ["GSBN_PER_TICK"]
-            else:
-                os.environ["GSBN_PER_TICK"] = old
+        arr = (MemberDesc * len(members))(*[MemberDesc(capi.PopDesc(**m.pop), capi.ProjDesc(**m.proj), m.seed)
+                                            for m in members])
+        self._arr = arr
+        d = BatchDesc(len(members), arr, dt, poisson_hz, device, max_ticks, threads, (ctypes.c_int32 * 3)(*lpt))
+        rc = self._lib.bcpnn_batch_create(ctypes.byref(d), ctypes.byref(self._h))
+        if rc != 0:
+            msg = self._lib.bcpnn_batch_last_error(self._h).decode() if self._h else ""
+            if self._h:
+                self._lib.bcpnn_batch_destroy(self._h)
+                self._h = ctypes.c_void_p()
+            raise capi.BcpnnError(rc, msg or self._lib.bcpnn_status_string(rc).decode())
         for i, m in enumerate(members):
-            self.net.set_pop_rng(i, m.seed, 0)
-            self.net.set_conn(i, m.ii, m.di)
-        lg = np.concatenate([m.lgidx for m in members], axis=1)
-        wm = np.concatenate([m.wmask for m in members], axis=1)
-        self.net.upload_stimuli_idx(lg, eps, wm)
+            ii = np.ascontiguousarray(m.ii, np.int32)
+            di = np.ascontiguousarray(m.di, np.int32)
+            self._check(self._lib.bcpnn_batch_set_conn(self._h, i, _p(ii), _p(di), ii.size))
+            lg = np.ascontiguousarray(m.lgidx, np.int32)
+            wm = np.ascontiguousarray(m.wmask, np.float32)
+            self._check(self._lib.bcpnn_batch_upload_stimuli_idx(self._h, i, lg.shape[0], _p(lg), eps, wm.shape[0],
+                                                                 _p(wm)))
+        self.last_ticks = 0
 
-    def run(self, first, n, prn, old_prn, lg_row, wm_row):
-        self.net.use_stimulus(lg_row, wm_row)
-        self.net.run(first, n, prn, old_prn)
-
-    def close(self):
-        self.net.close()
-
-
-def partition(members, kind, k=1):
-    """member index groups of one candidate schedule"""
-    if kind == "one":
-        return [list(range(len(members)))]
-    if kind == "plain":
-        return [[i] for i in range(len(members))]
-    order = sorted(range(len(members)), key=lambda i: (members[i].C, members[i].H))
-    total = sum(members[i].cells for i in order)
-    groups, cur, acc = [], [], 0
-    for i in order:  # k groups of about equal cell count, similar shapes together
-        cur.append(i)
-        acc += members[i].cells
-        if acc >= total * (len(groups) + 1) / k and len(groups) < k - 1:
-            groups.append(cur)
-            cur = []
-    if cur:
-        groups.append(cur)
-    return groups
-
-
-# (partition kind, groups, tick-kernel CTA size)
-CANDIDATES = [("one", 1, 512), ("one", 1, 256), ("buckets", 4, 512), ("buckets", 4, 256), ("buckets", 8, 256),
-              ("buckets", 16, 256), ("buckets", 16, 512), ("plain", 1, 512)]
-
-
-def cand_name(c):
-    return f"{c[0]}{c[1]}/t{c[2]}"
-
-
-class Batch:
-    """The batch on the GPU under one schedule.  concurrent: groups run side by
-    side on their own streams (one launch per tick each); otherwise one group
-    after the other (a group may then use the persistent launch)."""
-
-    def __init__(self, members, groups, device=0, concurrent=None, threads=512):
-        self.members = members
-        self.groups_idx = groups
-        self.concurrent = (1 < len(groups) <= 64) if concurrent is None else concurrent
-        self.threads = threads
-        self.groups = [Group([members[i] for i in g], device=device, per_tick=self.concurrent, threads=threads)
-                       for g in groups]
+    def _check(self, rc):
+        if rc != 0:
+            raise capi.BcpnnError(rc, self._lib.bcpnn_batch_last_error(self._h).decode())
 
     def run_segment(self, first, n, prn, old_prn, lg_row, wm_row):
-        for g in self.groups:
-            g.run(first, n, prn, old_prn, lg_row, wm_row)
-            if not self.concurrent:
-                g.net.sync()
-
-    def sync(self):
-        for g in self.groups:
-            g.net.sync()
+        self._check(self._lib.bcpnn_batch_use_stimulus(self._h, lg_row, wm_row))
+        self._check(self._lib.bcpnn_batch_run(self._h, first, n, prn, old_prn))
+        self.last_ticks = n
 
     def reset(self):
-        for g in self.groups:
-            g.net.reset()
+        self._check(self._lib.bcpnn_batch_reset(self._h))
+
+    def sync(self):
+        self._check(self._lib.bcpnn_batch_sync(self._h))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self._lib.bcpnn_batch_get_stream(self._h, ctypes.byref(s)))
+        return s.value
+
+    def read(self, member, name):
+        t, n = ctypes.c_int32(), ctypes.c_size_t()
+        self._check(self._lib.bcpnn_batch_state_info(self._h, member, name.encode(), ctypes.byref(t), ctypes.byref(n)))
+        out = np.zeros(n.value, dtype={0: np.float32, 1: np.int32, 2: np.int8}[t.value])
+        self._check(self._lib.bcpnn_batch_read_state(self._h, member, name.encode(), _p(out), out.nbytes))
+        return out
+
+    def spike_log(self, member):
+        m = self.members[member]
+        words = (m.H * m.M + 31) // 32
+        out = np.zeros((self.last_ticks, words), np.uint32)
+        self._check(self._lib.bcpnn_batch_get_spike_log(self._h, member, _p(out), out.size))
+        return out
 
     def counters(self):
-        return sum(sum(g.net.counters()) for g in self.groups)
+        c = (ctypes.c_uint64 * 3)()
+        self._check(self._lib.bcpnn_batch_counters(self._h, c))
+        return [int(c[0]), int(c[1]), int(c[2])]
 
     def launches(self):
-        return sum(g.net.kernel_launches() for g in self.groups)
+        c = ctypes.c_uint64()
+        self._check(self._lib.bcpnn_batch_kernel_launches(self._h, ctypes.byref(c)))
+        return int(c.value)
 
-    def member_state(self, index, name):
-        """state vector `name` (gsbn name with the member's own index 0) of one member"""
-        for gi, g in enumerate(self.groups_idx):
-            if index in g:
-                local = g.index(index)
-                base = name.rsplit("_", 1)[0]
-                return self.groups[gi].net.read(f"{base}_{local}")
-        raise KeyError(index)
+    def tune(self, probe_ticks, train_rows=(0, 0), recall_rows=(1, 1)):
+        """the engine's tuner: ((threads, w0, w1, w2), us per tick); leaves the
+        batch reset under the chosen shape"""
+        out = (ctypes.c_int32 * 4)()
+        us = ctypes.c_float()
+        self._check(self._lib.bcpnn_batch_tune(self._h, probe_ticks, train_rows[0], train_rows[1], recall_rows[0],
+                                               recall_rows[1], out, ctypes.byref(us)))
+        return tuple(int(v) for v in out), float(us.value)
 
     def close(self):
-        for g in self.groups:
-            g.close()
+        if self._h:
+            self._lib.bcpnn_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
-def shape_key(members):
-    """cache key: the sorted (H, M) list"""
-    return hashlib.sha1(json.dumps(sorted((m.H, m.M) for m in members)).encode()).hexdigest()[:16]
+class Plain:
+    """The same members as networks of their own through the single-network C
+    ABI, one after the other (one network per launch): the comparison path."""
 
+    def __init__(self, members, dt=0.001, eps=1e-4, device=0, max_ticks=128):
+        self.members = members
+        self.nets = []
+        for m in members:
+            net = capi.Net([m.pop], [m.proj], dt, seed=m.seed, device=device, max_ticks=max_ticks)
+            net.set_conn(0, m.ii, m.di)
+            net.upload_stimuli_idx(m.lgidx, eps, m.wmask)
+            self.nets.append(net)
 
-def tune(members, device=0, probe_ticks=20, cache=None, candidates=CANDIDATES):
-    """Time every candidate schedule on the first `probe_ticks` training ticks
-    from the initial state; return (best (kind, k, threads), {name: seconds}).  With
-    `cache` (a JSON path), a result for the same member shapes is reused."""
-    key = shape_key(members)
-    if cache and os.path.exists(cache):
-        with open(cache) as f:
-            known = json.load(f)
-        if key in known:
-            return tuple(known[key]["best"]), known[key]["times"]
-    times = {}
-    for c in candidates:
-        kind, k, threads = c
-        b = Batch(members, partition(members, kind, k), device, threads=threads)
-        b.run_segment(1, 2, 1.0, 0.0, 0, 0)  # warm-up: graphs, tables, the first catch-up
-        b.sync()
-        t0 = time.perf_counter()
-        b.run_segment(3, probe_ticks, 1.0, 1.0, 0, 0)
-        b.sync()
-        times[cand_name(c)] = time.perf_counter() - t0
-        b.close()
-    best = min(candidates, key=lambda c: times[cand_name(c)])
-    if cache:
-        known = {}
-        if os.path.exists(cache):
-            with open(cache) as f:
-                known = json.load(f)
-        known[key] = {"best": list(best), "times": times}
-        with open(cache, "w") as f:
-            json.dump(known, f)
-    return tuple(best), times
+    def run_segment(self, first, n, prn, old_prn, lg_row, wm_row):
+        for net in self.nets:
+            net.use_stimulus(lg_row, wm_row)
+            net.run(first, n, prn, old_prn)
+
+    def sync(self):
+        for net in self.nets:
+            net.sync()
+
+    def reset(self):
+        for net in self.nets:
+            net.reset()
+
+    def counters(self):
+        return sum(sum(net.counters()) for net in self.nets)
+
+    def close(self):
+        for net in self.nets:
+            net.close()

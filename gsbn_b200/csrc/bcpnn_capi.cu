@@ -1705,3 +1705,6 @@ extern "C" int bcpnn_read_state_noalloc(bcpnn_net* net, const char* name, void* 
   CU(cudaStreamSynchronize(net->stream));
   return BCPNN_OK;
 }
+
+/* the batch engine (include/bcpnn_batch.h) shares this unit's device code */
+#include "bcpnn_batch.cuh"

@@ -23,13 +23,13 @@ def declared(prefix="bcpnn_"):
 
 
 def test_every_declared_entry_point_is_exported():
-    from gsbn_b200 import engine, recall
+    from gsbn_b200 import batch, engine, recall
     lib = capi.load()
     names = declared("bcpnn_") | declared("gsbn_")
     assert len(names) >= 40
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
-    bound = set(capi.EXPORTS) | set(recall.RECALL_EXPORTS) | set(engine.ENGINE_EXPORTS)
+    bound = set(capi.EXPORTS) | set(recall.RECALL_EXPORTS) | set(engine.ENGINE_EXPORTS) | set(batch.BATCH_EXPORTS)
     assert names <= bound, sorted(names - bound)
 
 
@@ -132,3 +132,19 @@ def test_non_finite_prn_is_rejected_before_any_launch(prn, old_prn):
         assert b"finite" in lib.bcpnn_last_error(h)
     finally:
         lib.bcpnn_net_destroy(h)
+
+
+def test_batch_rejects_bad_members_before_the_device():
+    """bcpnn_batch_create refuses members beyond the engine's limits (64 MCUs
+    per HCU, one recurrent projection) and non-positive rates, before any
+    device work."""
+    from gsbn_b200 import batch
+    good = batch.make_members(n=1, seed=1, hcu=(8, 8), mcu=(5, 5), n_patterns=2)[0]
+    for edit in (dict(pop=dict(good.pop, mcu_num=65)), dict(proj=dict(good.proj, src_pop=1)),
+                 dict(proj=dict(good.proj, taue=0.0)), dict(pop=dict(good.pop, taum=float("nan")))):
+        m = batch.Member.__new__(batch.Member)
+        m.__dict__.update(good.__dict__)
+        m.__dict__.update(edit)
+        with pytest.raises(capi.BcpnnError) as e:
+            batch.BatchEngine([m], max_ticks=8)
+        assert e.value.status == -1
