@@ -20,7 +20,7 @@ BATCH_EXPORTS = (
     "bcpnn_batch_create", "bcpnn_batch_destroy", "bcpnn_batch_set_conn", "bcpnn_batch_upload_stimuli_idx",
     "bcpnn_batch_use_stimulus", "bcpnn_batch_run", "bcpnn_batch_reset", "bcpnn_batch_sync", "bcpnn_batch_get_stream",
     "bcpnn_batch_state_info", "bcpnn_batch_read_state", "bcpnn_batch_get_spike_log", "bcpnn_batch_counters",
-    "bcpnn_batch_kernel_launches", "bcpnn_batch_tune", "bcpnn_batch_last_error",
+    "bcpnn_batch_kernel_launches", "bcpnn_batch_tune", "bcpnn_batch_last_error", "bcpnn_batch_phase_probe",
 )
 
 F32 = np.float32
@@ -110,6 +110,7 @@ def load():
         "bcpnn_batch_kernel_launches": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_batch_tune": (ctypes.c_int, [vp, i32, i32, i32, i32, i32, P(i32), P(ctypes.c_float)]),
         "bcpnn_batch_last_error": (ctypes.c_char_p, [vp]),
+        "bcpnn_batch_phase_probe": (ctypes.c_int, [vp, vp, i32, P(i32), i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -204,6 +205,15 @@ class BatchEngine:
         self._check(self._lib.bcpnn_batch_tune(self._h, probe_ticks, train_rows[0], train_rows[1], recall_rows[0],
                                                recall_rows[1], out, ctypes.byref(us)))
         return tuple(int(v) for v in out), float(us.value)
+
+    def phase_probe(self, reset=True):
+        """uint64 [CTAs, 32] batch-kernel phase counters (library built with
+        BCPNN_PHASE_PROBE; see bcpnn_batch_phase_probe)"""
+        n = ctypes.c_int32()
+        self._check(self._lib.bcpnn_batch_phase_probe(self._h, None, 0, ctypes.byref(n), 0))
+        out = np.zeros((n.value, 32), np.uint64)
+        self._check(self._lib.bcpnn_batch_phase_probe(self._h, _p(out), n.value, ctypes.byref(n), 1 if reset else 0))
+        return out
 
     def close(self):
         if self._h:

@@ -49,8 +49,18 @@ constexpr int kUnit = 64;     /* slots of one column unit: two per lane */
 constexpr int kListCap = 64;  /* active rows gathered per pass of a warp */
 constexpr int kCellsPerPass = 64; /* row cells decayed per pass of a warp: two per lane */
 constexpr int kCPL = kCellsPerPass / 32; /* cells per lane and pass */
-constexpr int kWarpScratch = kMaxM /* act */ + kMaxM /* pj */ + kListCap /* pi */ + kListCap /* list */ +
-                             kCellsPerPass /* w */ + kCellsPerPass / 4 /* skip bytes */;
+constexpr int kMaxW = 4;      /* arrival words per lane of an HCU: C <= 4096 slots */
+/* per-warp shared scratch, in floats: the member's and its tables'
+   descriptors, then the item's buffers */
+constexpr int kOffMember = 0;
+constexpr int kOffTab = 96;
+constexpr int kOffAct = 160;
+constexpr int kOffPj = kOffAct + kMaxM;
+constexpr int kOffPi = kOffPj + kMaxM;
+constexpr int kOffList = kOffPi + kListCap;
+constexpr int kOffW = kOffList + kListCap;
+constexpr int kOffSkip = kOffW + kCellsPerPass;
+constexpr int kWarpScratch = kOffSkip + kCellsPerPass / 4;
 constexpr unsigned long long kBarrierNs = 2000000000ull;
 
 struct Member {
@@ -175,45 +185,65 @@ __device__ __forceinline__ float warp_max(float v) {
 
 /* Active rows ros[0..nr) (ascending slots of HCU h) of member B at tick
    simstep: row traces, cells, weights, ordered epsc sum into e[2] (MCUs lane,
-   lane + 32).  kp as the tick's prn gives it. */
+   lane + 32).  kp as the tick's prn gives it.  The loads of the row traces
+   and of the first cells go out together, then their table entries. */
 __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict__ T, int h, const int* ros, int nr,
-                                          int simstep, float kp, float* ws_pi, const float* ws_pj, float* ws_w,
-                                          int8_t* ws_skip, float e[2], int lane) {
+                                       int simstep, float kp, float* ws_pi, const float* ws_pj, float* ws_w,
+                                       int8_t* ws_skip, float e[2], int lane) {
   const int M = B.M, C = B.C;
   const Coef& k = T->k;
   const int tlen = T->len;
-  /* row traces, Proj.cpp:397-416 (one lane per row) */
-  for (int r = lane; r < nr; r += 32) {
-    const int row = h * C + ros[r];
-    const int ti = B.ti[row];
-    const int pdt = simstep - ti;
-    if (pdt <= 0) {
-      B.zi[row] = B.zi[row] + B.kfti;
-      B.ti[row] = simstep;
-      ws_pi[r] = B.pi[row];
-    } else {
-      float4 A, Bt;
-      double2 R0, R1;
-      if (pdt < tlen) {
-        A = T->tab[(size_t)pdt * 4 + 2];
-        Bt = T->tab[(size_t)pdt * 4 + 3];
-        R0 = T->rtab[(size_t)pdt * 4 + 2];
-        R1 = T->rtab[(size_t)pdt * 4 + 3];
-      } else {
-        load_entry(T->tab, tlen, k, pdt, 2, A, Bt);
-        recip_part(A, Bt, 2, R0, R1);
+  const int ncell = nr * M;
+  /* row traces, Proj.cpp:397-416 (one lane per row; at most kListCap rows) */
+  {
+    int ti[2], row[2];
+    float4 tr[2];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int r = lane + 32 * v;
+      if (r < nr) {
+        row[v] = h * C + ros[r];
+        ti[v] = B.ti[row[v]];
+        tr[v] = make_float4(B.pi[row[v]], B.ei[row[v]], B.zi[row[v]], 0.0f);
       }
-      const float4 rt = row_step_in(make_float4(B.pi[row], B.ei[row], B.zi[row], 0.0f), T, A, Bt, R0, R1);
-      B.pi[row] = rt.x;
-      B.ei[row] = rt.y;
-      B.zi[row] = rt.z + B.kfti;
-      B.ti[row] = simstep;
-      ws_pi[r] = rt.x;
+    }
+    float4 A[2], Bt[2];
+    double2 R0[2], R1[2];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int pdt = simstep - ti[v];
+      if (lane + 32 * v < nr && pdt > 0 && pdt < tlen) {
+        A[v] = T->tab[(size_t)pdt * 4 + 2];
+        Bt[v] = T->tab[(size_t)pdt * 4 + 3];
+        R0[v] = T->rtab[(size_t)pdt * 4 + 2];
+        R1[v] = T->rtab[(size_t)pdt * 4 + 3];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int r = lane + 32 * v;
+      if (r >= nr) continue;
+      const int pdt = simstep - ti[v];
+      if (pdt <= 0) {
+        B.zi[row[v]] = tr[v].z + B.kfti;
+        B.ti[row[v]] = simstep;
+        ws_pi[r] = tr[v].x;
+      } else {
+        if (pdt >= tlen) {
+          load_entry(T->tab, tlen, k, pdt, 2, A[v], Bt[v]);
+          recip_part(A[v], Bt[v], 2, R0[v], R1[v]);
+        }
+        const float4 rt = row_step_in(tr[v], T, A[v], Bt[v], R0[v], R1[v]);
+        B.pi[row[v]] = rt.x;
+        B.ei[row[v]] = rt.y;
+        B.zi[row[v]] = rt.z + B.kfti;
+        B.ti[row[v]] = simstep;
+        ws_pi[r] = rt.x;
+      }
     }
   }
   __syncwarp();
   /* cells, Proj.cpp:418-478, kCellsPerPass at a time, kCPL per lane */
-  const int ncell = nr * M;
   for (int b0 = 0; b0 < ncell; b0 += kCellsPerPass) {
     int tv[kCPL];
     float4 cv[kCPL];
@@ -294,21 +324,17 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
   }
 }
 
-/* gather the active slots of HCU h's arrival word group into ascending
-   passes of at most kListCap rows; every pass runs rows_pass */
-__device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restrict__ T, int h, int kk, int simstep,
-                                         float kp, int* ws_list, float* ws_pi, const float* ws_pj, float* ws_w,
-                                         int8_t* ws_skip, float e[2], int lane) {
-  uint32_t* rw = B.ring + ((size_t)h * kRing + (unsigned)kk % kRing) * B.W;
+/* gather the active slots of HCU h (the arrival-ring words `words`, already
+   loaded: word g*32 + lane in words[g]) into ascending passes of at most
+   kListCap rows; every pass runs rows_pass.  Returns the number of rows. */
+__device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restrict__ T, int h, int simstep, float kp,
+                                         const uint32_t words[kMaxW], int* ws_list, float* ws_pi, const float* ws_pj,
+                                         float* ws_w, int8_t* ws_skip, float e[2], int lane) {
   int nl = 0, total_rows = 0;
-  /* rows of one pass: at most kListCap, and few enough that a pass of cells
-     fits the weight buffer when it is split into kCellsPerPass pieces */
-  for (int w0 = 0; w0 < B.W; w0 += 32) {
-    uint32_t word = 0;
-    if (w0 + lane < B.W) {
-      word = __ldcg(rw + w0 + lane);
-      if (word) rw[w0 + lane] = 0u;
-    }
+#pragma unroll
+  for (int g = 0; g < kMaxW; ++g) {
+    if (g * 32 >= B.W) break;
+    const uint32_t word = words[g];
     const int cnt = __popc(word);
     int incl = cnt;
 #pragma unroll
@@ -327,7 +353,7 @@ __device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restri
       while (wbits) {
         const int b = __ffs(wbits) - 1;
         wbits &= wbits - 1;
-        if (p >= done && p < done + take) ws_list[nl + p - done] = (w0 + lane) * 32 + b;
+        if (p >= done && p < done + take) ws_list[nl + p - done] = (g * 32 + lane) * 32 + b;
         ++p;
       }
       __syncwarp();
@@ -343,44 +369,75 @@ __device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restri
   return total_rows;
 }
 
-/* one tick of one (member, HCU) item, phase A, by one warp */
+/* one tick of one (member, HCU) item, phase A, by one warp.  The member's
+   and its tables' descriptors are copied to the warp's shared scratch first;
+   then every load the tick needs that depends on nothing else goes out
+   together (previous-tick state of the HCU's MCUs, stimulus, the softmax
+   seed's terms, the HCU's arrival words of this tick). */
 __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h, int it, float* ws,
-                                          unsigned long long& rows_acc, unsigned long long& cols_acc) {
-  const Member& B = D.m[n];
-  const TabRef* T = &R.tabs[n];
+                                       unsigned long long& rows_acc, unsigned long long& cols_acc) {
   const int lane = threadIdx.x & 31;
+  {
+    const uint32_t* src = (const uint32_t*)&D.m[n];
+    uint32_t* dst = (uint32_t*)(ws + kOffMember);
+    for (int k = lane; k < (int)(sizeof(Member) / 4); k += 32) dst[k] = src[k];
+    const uint32_t* tsrc = (const uint32_t*)&R.tabs[n];
+    uint32_t* tdst = (uint32_t*)(ws + kOffTab);
+    for (int k = lane; k < (int)(sizeof(TabRef) / 4); k += 32) tdst[k] = tsrc[k];
+  }
+  __syncwarp();
+  const Member& B = *(const Member*)(ws + kOffMember);
+  const TabRef* T = (const TabRef*)(ws + kOffTab);
   const int M = B.M, C = B.C, H = B.H, base = h * M;
   const int simstep = R.simstep0 + it, kk = R.k0 + it;
   const int cur = kk & 1, prev = cur ^ 1;
-  float* ws_act = ws;
-  float* ws_pj = ws + kMaxM;
-  float* ws_pi = ws + 2 * kMaxM;
-  int* ws_list = (int*)(ws + 2 * kMaxM + kListCap);
-  float* ws_w = ws + 2 * kMaxM + 2 * kListCap;
-  int8_t* ws_skip = (int8_t*)(ws + 2 * kMaxM + 2 * kListCap + kCellsPerPass);
+  float* ws_act = ws + kOffAct;
+  float* ws_pj = ws + kOffPj;
+  float* ws_pi = ws + kOffPi;
+  int* ws_list = (int*)(ws + kOffList);
+  float* ws_w = ws + kOffW;
+  int8_t* ws_skip = (int8_t*)(ws + kOffSkip);
 
-  /* 1. arrivals of the previous tick's spikes of this HCU (Proj.cpp:645-664
-     as events): a spike at T turns row h'*C + s active at T + 2 + delay */
-  for (int j0 = 0; j0 < M; j0 += 32) {
-    const int j = j0 + lane;
-    unsigned m = __ballot_sync(0xffffffffu, j < M && B.spike[base + j] > 0);
-    while (m) {
-      const int src = base + j0 + __ffs(m) - 1;
-      m &= m - 1;
-      const int e0 = B.fo_off[src], e1 = B.fo_off[src + 1];
-      for (int e = e0 + lane; e < e1; e += 32) {
-        const int row = B.fo_row[e];
-        const int hd = row / C, s = row - hd * C;
-        const unsigned slot = (unsigned)(kk + 1 + B.fo_di[e]) % kRing;
-        atomicOr(B.ring + ((size_t)hd * kRing + slot) * B.W + (s >> 5), 1u << (s & 31));
-      }
-    }
-  }
-
-  /* 2. population update, Pop.cpp:229-323 */
+  /* every independent load of the tick at once */
   const int lgrow = min(R.lg_row, B.lg_rows - 1), wmrow = min(R.wm_row, B.wm_rows - 1);
   const int want = B.lgidx[(size_t)lgrow * H + h];
   const float wm = B.wmask[(size_t)wmrow * H + h];
+  float dsp[2], bjp[2], esp[2], pjv[2], ejv[2], zjv[2];
+#pragma unroll
+  for (int jj = 0; jj < 2; ++jj) {
+    const int j = lane + 32 * jj;
+    if (j < M) {
+      const int idx = base + j;
+      dsp[jj] = B.dsup[prev][idx];
+      bjp[jj] = B.bj[prev][idx];
+      esp[jj] = B.epsc[prev][idx];
+      pjv[jj] = B.pj[idx];
+      ejv[jj] = B.ej[idx];
+      zjv[jj] = B.zj[idx];
+    }
+  }
+  float sd = 0.0f, sb = 0.0f, se = 0.0f, sw = 0.0f;
+  int sl = 0;
+  if (h != 0 && lane == 0) {
+    /* HCU 0's item wrote these in the previous tick, on another SM */
+    sd = __ldcg(B.dsup[prev]);
+    sb = __ldcg(B.bj[prev]);
+    se = __ldcg(B.epsc[prev]);
+    sl = B.lgidx[(size_t)lgrow * H];
+    sw = B.wmask[(size_t)wmrow * H];
+  }
+  uint32_t words[kMaxW];
+  uint32_t* rw = B.ring + ((size_t)h * kRing + (unsigned)kk % kRing) * B.W;
+#pragma unroll
+  for (int g = 0; g < kMaxW; ++g) {
+    words[g] = 0u;
+    if (g * 32 + lane < B.W) words[g] = __ldcg(rw + g * 32 + lane);
+  }
+#pragma unroll
+  for (int g = 0; g < kMaxW; ++g)
+    if (words[g]) rw[g * 32 + lane] = 0u;
+
+  /* population update, Pop.cpp:229-323 */
   float dn[2];
 #pragma unroll
   for (int jj = 0; jj < 2; ++jj) {
@@ -389,13 +446,12 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
     if (j < M) {
       const int idx = base + j;
       float wsup = 0.0f;
-      wsup += B.bj[prev][idx] + B.epsc[prev][idx];
+      wsup += bjp[jj] + esp[jj];
       float noise = 0.0f;
       if (B.snoise != 0.0f) noise = B.snoise * dev_normal01(B.rng_seed, 0u, (uint32_t)simstep, (uint32_t)idx);
       float sup = B.lgbias + B.igain * (want == j ? B.lg_hit : B.lg_miss) + noise;
       sup += (B.wgain * wm) * wsup;
-      const float d = B.dsup[prev][idx];
-      dn[jj] = d + (sup - d) * B.taumdt;
+      dn[jj] = dsp[jj] + (sup - dsp[jj]) * B.taumdt;
     }
   }
   /* the softmax maximum is seeded with the member's MCU 0 (Pop.cpp:270) */
@@ -405,15 +461,13 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
   } else {
     float s0 = 0.0f;
     if (lane == 0) {
-      /* HCU 0's item wrote these in the previous tick, on another SM */
       float wsup = 0.0f;
-      wsup += __ldcg(B.bj[prev]) + __ldcg(B.epsc[prev]);
+      wsup += sb + se;
       float noise = 0.0f;
       if (B.snoise != 0.0f) noise = B.snoise * dev_normal01(B.rng_seed, 0u, (uint32_t)simstep, 0u);
-      float sup = B.lgbias + B.igain * (B.lgidx[(size_t)lgrow * H] == 0 ? B.lg_hit : B.lg_miss) + noise;
-      sup += (B.wgain * B.wmask[(size_t)wmrow * H]) * wsup;
-      const float d = __ldcg(B.dsup[prev]);
-      s0 = d + (sup - d) * B.taumdt;
+      float sup = B.lgbias + B.igain * (sl == 0 ? B.lg_hit : B.lg_miss) + noise;
+      sup += (B.wgain * sw) * wsup;
+      s0 = sd + (sup - sd) * B.taumdt;
     }
     seed0 = __shfl_sync(0xffffffffu, s0, 0);
   }
@@ -468,7 +522,7 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
     }
   }
 
-  /* 3. j-traces and bias, Proj.cpp:310-363 */
+  /* j-traces and bias, Proj.cpp:310-363 */
   const float kp = B.taupdt * R.prn;
   float e[2];
 #pragma unroll
@@ -477,14 +531,14 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
     e[jj] = 0.0f;
     if (j < M) {
       const int idx = base + j;
-      float pj = B.pj[idx], ej = B.ej[idx], zj = B.zj[idx];
-      float ev = B.epsc[prev][idx];
+      float pj = pjv[jj], ej = ejv[jj], zj = zjv[jj];
+      float ev = esp[jj];
       ev *= (1 - B.kepsc);
       pj += (ej - pj) * kp;
       ej += (zj - ej) * B.ke;
       zj *= (1 - B.kzj);
       if (spk[jj] > 0) zj += B.kftj;
-      B.bj[cur][idx] = (kp != 0.0f) ? B.bgain * dev_logf(pj + B.eps) : B.bj[prev][idx];
+      B.bj[cur][idx] = (kp != 0.0f) ? B.bgain * dev_logf(pj + B.eps) : bjp[jj];
       B.pj[idx] = pj;
       B.ej[idx] = ej;
       B.zj[idx] = zj;
@@ -494,36 +548,46 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
   }
   __syncwarp();
 
-  /* 4. the active rows of this tick, ascending (Proj.cpp:365-479, 667-720) */
-  const int nrows = item_rows(B, T, h, kk, simstep, kp, ws_list, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
+  /* the active rows of this tick, ascending (Proj.cpp:365-479, 667-720) */
+  const int nrows = item_rows(B, T, h, simstep, kp, words, ws_list, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
 #pragma unroll
   for (int jj = 0; jj < 2; ++jj) {
     const int j = lane + 32 * jj;
     if (j < M) B.epsc[cur][base + j] = e[jj];
   }
 
-  /* 5. column units of this tick's spikes (done in phase B) */
-  const int parts = (C + kUnit - 1) / kUnit;
-  unsigned int* cnt = D.unit_cnt + cur;
-  int4* units = D.units + (size_t)cur * D.unit_cap;
-  int nspk = 0;
-#pragma unroll
-  for (int jj = 0; jj < 2; ++jj) {
-    unsigned m = __ballot_sync(0xffffffffu, spk[jj] > 0);
-    while (m) {
-      const int j = 32 * jj + __ffs(m) - 1;
-      m &= m - 1;
-      ++nspk;
-      unsigned int pos = 0;
-      if (lane == 0) pos = atomicAdd(cnt, (unsigned int)parts);
-      pos = __shfl_sync(0xffffffffu, pos, 0);
-      if (pos + (unsigned)parts > (unsigned)D.unit_cap) {
-        if (lane == 0) atomicOr(D.err, kErrIndex);
-        continue;
-      }
-      for (int p = lane; p < parts; p += 32) {
-        const int rows = min(kUnit, C - p * kUnit);
-        units[pos + p] = make_int4(n, h * C + p * kUnit, j | (rows << 16), 0);
+  /* units of phase B for this tick's spikes: per spike, its column in
+     slot pieces (Proj.cpp:481-536) and its fan-out (the delay queue of the
+     next tick, as arrivals); one counter add for all of them */
+  const unsigned m0 = __ballot_sync(0xffffffffu, spk[0] > 0), m1 = __ballot_sync(0xffffffffu, spk[1] > 0);
+  const int nspk = __popc(m0) + __popc(m1);
+  if (nspk > 0) {
+    const int parts = (C + kUnit - 1) / kUnit + 1;
+    unsigned int pos = 0;
+    if (lane == 0) pos = atomicAdd(D.unit_cnt + cur, (unsigned int)(parts * nspk));
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+    if (pos + (unsigned)(parts * nspk) > (unsigned)D.unit_cap) {
+      if (lane == 0) atomicOr(D.err, kErrIndex);
+    } else {
+      int4* units = D.units + (size_t)cur * D.unit_cap;
+      for (int k = lane; k < parts * nspk; k += 32) {
+        const int i = k / parts, p = k - i * parts;
+        /* the i-th spiking MCU, in MCU order */
+        unsigned mm = m0;
+        int j = 0, left = i;
+        if (left >= __popc(m0)) {
+          left -= __popc(m0);
+          mm = m1;
+          j = 32;
+        }
+        for (; left > 0; --left) mm &= mm - 1;
+        j += __ffs(mm) - 1;
+        if (p < parts - 1) {
+          const int rows = min(kUnit, C - p * kUnit);
+          units[pos + k] = make_int4(n, h * C + p * kUnit, j | (rows << 16), 0);
+        } else {
+          units[pos + k] = make_int4(n, base + j, 0, 1); /* fan-out of MCU base + j */
+        }
       }
     }
   }
@@ -533,13 +597,26 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
   }
 }
 
-/* one column unit, phase B: slots [row0, row0 + rows) of member n's column j
-   (Proj.cpp:481-536); every cell of the tick's active rows already has
-   tij = simstep (rows ran in phase A), so it only gains kftj */
-__device__ __noinline__ void column_unit(const Dev& D, const Run& R, int4 u, int simstep) {
+/* a unit of phase B.  w == 0: column unit, slots [row0, row0 + rows) of
+   member n's column j (Proj.cpp:481-536); every cell of the tick's active
+   rows already has tij = simstep (rows ran in phase A), so it only gains
+   kftj.  w == 1: the fan-out of source MCU y, whose spike of this tick turns
+   each slot it feeds active at kk + 2 + delay (the delay queue, as events). */
+__device__ __noinline__ void column_unit(const Dev& D, const Run& R, int4 u, int simstep, int kk) {
   const Member& B = D.m[u.x];
-  const TabRef* T = &R.tabs[u.x];
   const int lane = threadIdx.x & 31;
+  if (u.w == 1) {
+    const int src = u.y, C = B.C;
+    const int e0 = B.fo_off[src], e1 = B.fo_off[src + 1];
+    for (int e = e0 + lane; e < e1; e += 32) {
+      const int row = B.fo_row[e];
+      const int hd = row / C, s = row - hd * C;
+      const unsigned slot = (unsigned)(kk + 2 + B.fo_di[e]) % kRing;
+      atomicOr(B.ring + ((size_t)hd * kRing + slot) * B.W + (s >> 5), 1u << (s & 31));
+    }
+    return;
+  }
+  const TabRef* T = &R.tabs[u.x];
   const int row0 = u.y, j = u.z & 0xffff, rows = u.z >> 16, M = B.M;
   const int tlen = T->len;
   size_t index[kUnit / 32];
@@ -617,25 +694,74 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const Dev* __restric
   unsigned int arrivals = 0;
   const int i0 = gwarp < D.n_warps ? D.warp_off[gwarp] : 0;
   const int i1 = gwarp < D.n_warps ? D.warp_off[gwarp + 1] : 0;
+#ifdef BCPNN_PHASE_PROBE
+  /* per CTA: [0] phase A cycles summed over warps and ticks, [1] the slowest
+     warp's, summed over ticks, [2], [3] the same for phase B, [4], [5] the
+     waits of the two barriers (thread 0), [6] ticks, [7] units done, [8]
+     items done */
+  if (threadIdx.x < kProbeSlots) g_probe_smem[threadIdx.x] = 0;
+  __shared__ unsigned long long s_pmax[2];
+  __syncthreads();
+#endif
   for (int it = 0; it < R.n_ticks; ++it) {
     const int simstep = R.simstep0 + it, kk = R.k0 + it;
+#ifdef BCPNN_PHASE_PROBE
+    long long pt0 = clock64();
+    if (threadIdx.x == 0) s_pmax[0] = s_pmax[1] = 0;
+    __syncthreads();
+#endif
     for (int e = i0; e < i1; ++e) {
       const int2 item = D.items[D.warp_items[e]];
       item_tick(D, R, item.x, item.y, it, ws, rows_acc, cols_acc);
     }
+#ifdef BCPNN_PHASE_PROBE
+    if (lane == 0) {
+      const unsigned long long d = (unsigned long long)(clock64() - pt0);
+      atomicAdd(&g_probe_smem[0], d);
+      atomicMax(&s_pmax[0], d);
+      atomicAdd(&g_probe_smem[8], (unsigned long long)(i1 - i0));
+    }
+    long long pt1 = clock64();
+#endif
     arrivals += gridDim.x;
     if (!grid_sync(bar, arrivals, D.err, &s_ok)) return;
+#ifdef BCPNN_PHASE_PROBE
+    if (threadIdx.x == 0) g_probe_smem[4] += (unsigned long long)(clock64() - pt1);
+    long long pt2 = clock64();
+#endif
     /* phase B: the tick's column units over every warp of the grid */
     /* a counter past the ring's capacity (reported in phase A) is clamped */
     const unsigned int nu = min(__ldcg(D.unit_cnt + (kk & 1)), (unsigned int)D.unit_cap);
     const int4* units = D.units + (size_t)(kk & 1) * D.unit_cap;
-    for (unsigned int u = gwarp; u < nu; u += nw) column_unit(D, R, __ldcg(units + u), simstep);
+    for (unsigned int u = gwarp; u < nu; u += nw) column_unit(D, R, __ldcg(units + u), simstep, kk);
+#ifdef BCPNN_PHASE_PROBE
+    if (lane == 0) {
+      const unsigned long long d = (unsigned long long)(clock64() - pt2);
+      atomicAdd(&g_probe_smem[2], d);
+      atomicMax(&s_pmax[1], d);
+      if (gwarp < (int)nu) atomicAdd(&g_probe_smem[7], (unsigned long long)((nu - gwarp + nw - 1) / nw));
+    }
+    long long pt3 = clock64();
+#endif
     /* the other parity's counter is free again (its units were done in the
        previous tick's phase B); the next tick appends to it */
     if (blockIdx.x == 0 && threadIdx.x == 0) D.unit_cnt[(kk + 1) & 1] = 0u;
     arrivals += gridDim.x;
     if (!grid_sync(bar, arrivals, D.err, &s_ok)) return;
+#ifdef BCPNN_PHASE_PROBE
+    if (threadIdx.x == 0) {
+      g_probe_smem[5] += (unsigned long long)(clock64() - pt3);
+      g_probe_smem[1] += s_pmax[0];
+      g_probe_smem[3] += s_pmax[1];
+      g_probe_smem[6] += 1;
+    }
+#endif
   }
+#ifdef BCPNN_PHASE_PROBE
+  __syncthreads();
+  if (threadIdx.x < kProbeSlots && blockIdx.x < kProbeCtas)
+    atomicAdd(&g_phase_probe[blockIdx.x * kProbeSlots + threadIdx.x], g_probe_smem[threadIdx.x]);
+#endif
   if (lane == 0) {
     if (rows_acc) atomicAdd(&D.counters[0], rows_acc);
     if (cols_acc) atomicAdd(&D.counters[1], cols_acc);
@@ -1044,7 +1170,7 @@ int bcpnn_batch_create(const bcpnn_batch_desc* desc, bcpnn_batch** out) {
     if ((rc = reset_member(b, i))) return rc;
     row_off[i + 1] = row_off[i] + R;
     cell_off[i + 1] = cell_off[i] + cells;
-    unit_cap += (size_t)B.n * ((B.C + kUnit - 1) / kUnit);
+    unit_cap += (size_t)B.n * ((B.C + kUnit - 1) / kUnit + 1); /* column pieces + the fan-out */
     for (int hh = 0; hh < B.H; ++hh) b->items.push_back(make_int2(i, hh));
   }
   b->total_rows = row_off[N];
@@ -1367,11 +1493,17 @@ int bcpnn_batch_read_state(bcpnn_batch* b, int32_t member, const char* name, voi
     } else {
       /* gsbn's delay queue from the arrival ring: at the end of executed tick
          K, qi bit k of a slot is its row turning active at K + 2 + k, .siq its
-         row turning active at K + 1 (rows of the spikes of K are queued at
-         K + 1, as ProcExchangeSpike -> update_que does) */
+         row turning active at K + 1.  The ring already holds the arrivals of
+         the spikes of K (phase B of K), which gsbn queues only at K + 1 (they
+         are in si): a slot's bit at K + 2 + k comes from its source's spike at
+         K + k - delay, so bit k = delay is left out when the source spiked at
+         K. */
       const size_t words = (size_t)B.H * kRing * B.W;
       std::vector<uint32_t> ring(words);
+      std::vector<int8_t> last_spk(B.n);
       BCU(cudaMemcpy(ring.data(), B.ring, words * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+      BCU(cudaMemcpy(last_spk.data(), B.spike, (size_t)B.n, cudaMemcpyDeviceToHost));
+      const MemberHost& Mh = b->mh[member];
       const int64_t K = b->k_total - 1;
       for (int h = 0; h < B.H; ++h)
         for (int s = 0; s < B.C; ++s) {
@@ -1382,8 +1514,11 @@ int bcpnn_batch_read_state(bcpnn_batch* b, int32_t member, const char* name, voi
           const size_t r = (size_t)h * B.C + s;
           if (v.kind == 2) {
             int32_t q = 0;
-            if (b->k_total > 0)
+            if (b->k_total > 0) {
               for (int k = 0; k < 31; ++k) q |= (int32_t)(bit(K + 2 + k) << k);
+              const int src = Mh.ii[r];
+              if (src >= 0 && last_spk[src] > 0 && Mh.di[r] <= 30) q &= ~(int32_t)(1u << Mh.di[r]);
+            }
             ((int32_t*)host)[r] = q;
           } else {
             ((int8_t*)host)[r] = b->k_total > 0 ? (int8_t)bit(K + 1) : 0;
@@ -1492,5 +1627,26 @@ int bcpnn_batch_tune(bcpnn_batch* b, int32_t probe_ticks, int32_t lgidx_train, i
 }
 
 const char* bcpnn_batch_last_error(const bcpnn_batch* b) { return b ? b->err.c_str() : "null handle"; }
+
+int bcpnn_batch_phase_probe(bcpnn_batch* b, uint64_t* out, int32_t max_ctas, int32_t* n_ctas, int32_t reset) {
+  if (!b) return BCPNN_ERR_INVALID;
+#ifdef BCPNN_PHASE_PROBE
+  if (!n_ctas || (max_ctas > 0 && !out)) return bfail(b, BCPNN_ERR_INVALID, "bcpnn_batch_phase_probe: null buffer");
+  const int n = std::min(b->grid, kProbeCtas);
+  *n_ctas = n;
+  BCU(cudaSetDevice(b->device));
+  BCU(cudaStreamSynchronize(b->stream));
+  if (max_ctas > 0) BCU(cudaMemcpyFromSymbol(out, g_phase_probe, (size_t)std::min(n, (int)max_ctas) * kProbeSlots * 8));
+  if (reset) {
+    static const uint64_t zeros[kProbeCtas * kProbeSlots] = {};
+    BCU(cudaMemcpyToSymbol(g_phase_probe, zeros, sizeof(zeros)));
+  }
+  return BCPNN_OK;
+#else
+  (void)out; (void)max_ctas; (void)reset;
+  if (n_ctas) *n_ctas = 0;
+  return bfail(b, BCPNN_ERR_STATE, "bcpnn_batch_phase_probe: this library was built without BCPNN_PHASE_PROBE");
+#endif
+}
 
 }  // extern "C"

@@ -24,10 +24,10 @@
  * Execution: a cooperative launch of as many CTAs as fit on the GPU at once.
  * Per tick, phase A gives every (member, HCU) item to one warp (items are
  * assigned to warps by a longest-processing-time schedule over estimated
- * costs): delay-queue arrivals of the previous tick's spikes, population
- * update, j-traces and the HCU's active rows with the ordered epsc sum; then a
- * grid barrier; phase B spreads the column updates of the tick's spikes over
- * all warps in units of 256 slots; then a grid barrier.  The delay queue is
+ * costs): population update, j-traces and the HCU's active rows with the
+ * ordered epsc sum; then a grid barrier; phase B spreads over all warps the
+ * column updates of the tick's spikes, in units of 64 slots, and their
+ * fan-out into the delay queue; then a grid barrier.  The delay queue is
  * event driven: a spike sets one bit per fan-out slot in the destination
  * HCU's arrival ring at the tick the row becomes active, instead of every
  * slot's shift register being stepped every tick; bcpnn_batch_read_state
@@ -115,6 +115,14 @@ int bcpnn_batch_tune(bcpnn_batch* b, int32_t probe_ticks, int32_t lgidx_train, i
                      int32_t lgidx_recall, int32_t wmask_recall, int32_t out[4], float* us_per_tick);
 
 const char* bcpnn_batch_last_error(const bcpnn_batch* b);
+
+/* Phase probe of the batch kernel, as bcpnn_phase_probe: in a library built
+   with -DBCPNN_PHASE_PROBE, per CTA 32 counters -- [0] phase A SM cycles
+   summed over warps and ticks, [1] the slowest warp's phase A summed over
+   ticks, [2], [3] the same for phase B, [4], [5] the waits of the two grid
+   barriers, [6] ticks, [7] units, [8] items; the default build returns
+   BCPNN_ERR_STATE. */
+int bcpnn_batch_phase_probe(bcpnn_batch* b, uint64_t* out, int32_t max_ctas, int32_t* n_ctas, int32_t reset);
 
 #ifdef __cplusplus
 }
