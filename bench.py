@@ -47,6 +47,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# nominal FP32 FFMA rate of one B200: 148 SMs x 128 FP32 lanes x 2 flops at
+# the 1965 MHz maximum SM clock (no measured figure exists for the SIMT pipes)
+FP32_SIMT_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def peaks():
@@ -329,118 +332,209 @@ RECALL_STATE = ("pij_0", "eij_0", "zi2_0", "zj2_0", "tij_0", "wij_0", "pi_0", "e
                 ".counter_0")
 
 
-def profile_value(name, key):
-    """a `key: value` line of a committed summary under profiles/"""
+def _recall_engine(tr, W, st, R, lg, wm, seed_base, hz, dev, contraction):
+    from gsbn_b200 import recall
+    eng = recall.Recall(tr.H, tr.M, R, tr.pops[0], tr.dt, recall.kepsc_of(tr.projs[0], tr.dt), seed_base, hz, dev,
+                        contraction=contraction)
+    eng.set_cues(lg[:R], tr.eps, wm[:R])
+    eng.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
+    eng.clear_counts()
+    return eng
+
+
+def time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, contraction, steps, warmup):
+    """One form of the replicate engine on the recall workload: the counted
+    run first (ProcCheck's counters over the ticks strictly inside the
+    segment), then `warmup` untimed and `steps` timed runs of T ticks, each
+    from the trained state (the state load is outside the timed region).
+    Returns (ms per run, counts, kernel launches per run)."""
+    import torch
+    eng = _recall_engine(tr, W, st, R, lg, wm, seed_base, tr.poisson_hz, dev, contraction)
     try:
-        with open(os.path.join(ROOT, "profiles", name)) as f:
-            for line in f:
-                if line.startswith(key + ":"):
-                    return json.loads(line.split(":", 1)[1])
-    except (OSError, ValueError):
-        pass
-    return None
+        stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
+
+        def load():
+            eng.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
+            eng.clear_counts()
+
+        eng.run(tr.t0, T, tr.t0, tr.t0 + T - 2)
+        counts = eng.read("counts")
+        for _ in range(max(0, warmup - 1)):
+            load()
+            eng.run(tr.t0, T)
+        times, launches = [], 0
+        for _ in range(steps):
+            load()
+            l0 = eng.launches()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            eng.run(tr.t0, T)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            launches += eng.launches() - l0
+    finally:
+        eng.close()
+    return statistics.mean(times), counts, launches / max(1, steps)
 
 
-def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_sample=8, cpu=True):
+def recall_counts(tr, W, st, R, T, lg, wm, seed_base, hz, dev, contraction):
+    """ProcCheck's counters of R replicates after one T-tick recall segment"""
+    eng = _recall_engine(tr, W, st, R, lg, wm, seed_base, hz, dev, contraction)
+    try:
+        eng.run(tr.t0, T, tr.t0, tr.t0 + T - 2)
+        return eng.read("counts")
+    finally:
+        eng.close()
+
+
+def plain_recall(tr, trained, T, lg, wm, expected, seed_base, hz, dev, n, timed):
+    """The plain FP32 path (one ProcUpdLazy network per replicate, every
+    trace carried) on replicates 0..n-1: ProcCheck decisions, per-HCU
+    accuracy and, when timed, the device time of each replicate's run."""
+    import torch
+    from gsbn_b200 import capi, recall
+    N = tr.H * tr.M
+    ms, ok, acc, cells = [], [], [], 0
+    for r in range(n):
+        net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=hz, device=dev, max_ticks=T)
+        try:
+            for name, a in trained.items():
+                net.write(name, a)
+            net.set_stimulus_idx(lg[r], tr.eps, wm[r])
+            ps = torch.cuda.ExternalStream(net.stream(), device=dev)
+            c0 = sum(net.counters())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(ps)
+            net.run(tr.t0, T, 0.0, tr.old_prn)
+            e1.record(ps)
+            net.sync()
+            torch.cuda.synchronize()
+            if timed:
+                ms.append(e0.elapsed_time(e1))
+                cells += sum(net.counters()) - c0
+            bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
+        finally:
+            net.close()
+        counts = bits[: T - 1].sum(axis=0)[None, :]
+        ok.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
+        acc.append(float(recall.hcu_accuracy(counts, tr.H, tr.M, expected[r:r + 1])[0]))
+    return ms, ok, acc, cells
+
+
+def recall_fp64_errors(tr, trained, W, st, T, lg, wm, expected, seed_base, hz, dev, K):
+    """Error of both engine forms against the FP64 oracle of the same
+    simulation (oracle/recall_fp64.py, pinned to the oracle in double), on
+    replicates 0..K-1 of the workload -- the same Philox keys and cues as in
+    the timed runs.  Each engine runs the segment tick by tick and its dsup
+    and spike rows of the sample are read after every tick; the FP64 oracle
+    runs the same K replicates.  Per replicate: the support error before the
+    spike trains first differ, the first tick where they differ, the spike
+    Jaccard over the run, and ProcCheck's decision."""
+    from gsbn_b200 import recall
+    from oracle import recall_fp64
+    H, M = tr.H, tr.M
+    R = max(128, -(-K // 128) * 128)
+    lg_r = recall_fp64.lginp_rows(lg[:1], H, M, tr.eps)[0]
+    W64, bj0, bj1, pos = recall_fp64.catchup_weights(tr.pops, tr.projs, tr.dt, hz, trained, tr.t0, tr.old_prn, lg_r,
+                                                     wm[0])
+    rs = recall_fp64.RecallFP64(tr.pops[0], tr.dt, recall_fp64.kepsc_tau(tr.projs[0]), hz, W64, bj0, bj1, pos,
+                                st["epsc"], st["dsup"], (st["s_tm3"], st["s_tm2"], st["s_tm1"]), lg, wm, tr.eps,
+                                seed_base, list(range(K)))
+    d64, s64 = [], []
+    for k in range(T):
+        d, s = rs.step(tr.t0 + k)
+        d64.append(d)
+        s64.append(s)
+    counts64 = np.sum(np.stack(s64[:T - 1]) != 0, axis=0)
+    ok64 = recall.recall_decisions(counts64, H, M, expected[:K])
+    out = {"replicates_compared": K, "ticks": T, "poisson_hz": hz,
+           "method": "engine rows 0..K-1 read every tick vs the FP64 restatement of the same replicates "
+                     "(oracle/recall_fp64.py, spike-identical to OracleNet(real_bits=64))",
+           "recall_fp64": f"{int(ok64.sum())}/{K}"}
+    for form in ("bf16", "fp32"):
+        eng = _recall_engine(tr, W, st, R, lg, wm, seed_base, hz, dev, form)
+        try:
+            ds, ss = [], []
+            for k in range(T):
+                eng.run(tr.t0 + k, 1, tr.t0, tr.t0 + T - 2)
+                ds.append(eng.read("dsup", 0, K))
+                ss.append(eng.read("spike", 0, K))
+            ok = recall.recall_decisions(eng.read("counts", 0, K), H, M, expected[:K])
+        finally:
+            eng.close()
+        ms = [recall_fp64.error_metrics([ds[k][i] for k in range(T)], [ss[k][i] for k in range(T)],
+                                        [d64[k][i] for k in range(T)], [s64[k][i] for k in range(T)])
+              for i in range(K)]
+        err = [m["support_rel_err"] for m in ms]
+        div = [m["first_divergence_tick"] for m in ms]
+        jac = [m["spike_jaccard"] for m in ms]
+        out["bf16_engine" if form == "bf16" else "fp32_engine"] = {
+            "support_rel_err_max": max(err), "support_rel_err_median": float(np.median(err)),
+            "first_divergence_tick_min": min(div), "first_divergence_tick_median": float(np.median(div)),
+            "replicates_identical_over_run": sum(int(d == T) for d in div),
+            "spike_jaccard_min": min(jac), "spike_jaccard_mean": float(np.mean(jac)),
+            "recall": f"{int(ok.sum())}/{K}",
+            "recall_agree_with_fp64": f"{int(np.sum(ok == ok64))}/{K}"}
+    return out
+
+
+def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_sample=8, fp64_sample=32, cpu=True):
     """The precision extension: recall of a trained 64x64 network (4096 x 4096
     weights) by 4096 noise replicates (25% cue, 20 Hz Poisson noise, 200
-    ticks) with the support as a BF16 tcgen05 contraction, against the plain
-    FP32 path running the same replicates one network per launch."""
-    import torch
-    from gsbn_b200 import capi, recall, workloads
+    ticks) with the support as a BF16 tcgen05 contraction; against the same
+    engine with an FP32 SIMT contraction (W in FP32), against the plain FP32
+    path running replicates one network per launch, and against the FP64
+    oracle of the same simulation on a sample of replicates."""
+    from gsbn_b200 import recall, workloads
     work = workloads.config4()
     tr = recall.Trained(work, tempfile.mkdtemp(prefix="gsbn_recall_"), device=dev)
     trained = tr.snapshot(RECALL_STATE)
     W, st = tr.recall_inputs()
-    R, T, seed_base = replicates, ticks, 1
+    R, T, seed_base, H, M = replicates, ticks, 1, tr.H, tr.M
+    N = H * M
     lg, wm, expected = tr.cues(R)
-    eng = recall.Recall(tr.H, tr.M, R, tr.pops[0], tr.dt, recall.kepsc_of(tr.projs[0], tr.dt), seed_base,
-                        tr.poisson_hz, dev)
-    eng.set_cues(lg, tr.eps, wm)
-    stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
-    count = (tr.t0, tr.t0 + T - 2)  # ProcCheck counts ticks strictly inside a T-tick segment
-
-    def load():
-        eng.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
-        eng.clear_counts()
-
-    load()
-    eng.run(tr.t0, T, *count)
-    counts_all = eng.read("counts")
-    ok = recall.recall_decisions(counts_all, tr.H, tr.M, expected)
-    acc = recall.hcu_accuracy(counts_all, tr.H, tr.M, expected)
-    for _ in range(max(0, warmup - 1)):
-        load()
-        eng.run(tr.t0, T)
-    l0 = eng.launches()
-    times = []
-    for _ in range(steps):
-        load()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        eng.run(tr.t0, T)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
-    launches = eng.launches() - l0 - 5 * steps  # the per-load broadcast kernels are not in the timed region
-    eng.close()
-    ms = statistics.mean(times)
-    N = tr.H * tr.M
+    ms, counts, launches = time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, "bf16", steps, warmup)
+    ms32, counts32, launches32 = time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, "fp32", steps, warmup)
     flops = 2.0 * R * N * N * T
-    tflops = flops / (ms * 1e-3) / 1e12
+    tflops, tflops32 = flops / (ms * 1e-3) / 1e12, flops / (ms32 * 1e-3) / 1e12
     pk, pk_kind = peaks()
+    value, value32 = R * T / (ms * 1e-3), R * T / (ms32 * 1e-3)
 
-    # the plain FP32 path, one network per replicate
-    plain_ms, plain_ok, plain_acc, plain_cells = [], [], [], 0
-    for r in range(plain_sample):
-        net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=tr.poisson_hz, device=dev,
-                       max_ticks=T)
-        for n, a in trained.items():
-            net.write(n, a)
-        net.set_stimulus_idx(lg[r], tr.eps, wm[r])
-        ps = torch.cuda.ExternalStream(net.stream(), device=dev)
-        c0 = sum(net.counters())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(ps)
-        net.run(tr.t0, T, 0.0, tr.old_prn)
-        e1.record(ps)
-        net.sync()
-        torch.cuda.synchronize()
-        plain_ms.append(e0.elapsed_time(e1))
-        plain_cells += sum(net.counters()) - c0
-        bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
-        counts = bits[: T - 1].sum(axis=0)[None, :]
-        plain_ok.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
-        plain_acc.append(float(recall.hcu_accuracy(counts, tr.H, tr.M, expected[r:r + 1])[0]))
-        net.close()
+    def decisions(c):
+        return recall.recall_decisions(c, H, M, expected), recall.hcu_accuracy(c, H, M, expected)
+
+    ok, acc = decisions(counts)
+    ok32, acc32 = decisions(counts32)
+    plain_ms, plain_ok, plain_acc, plain_cells = plain_recall(tr, trained, T, lg, wm, expected, seed_base,
+                                                              tr.poisson_hz, dev, plain_sample, True)
     plain_rate = T / (statistics.mean(plain_ms) * 1e-3)
-    value = R * T / (ms * 1e-3)
+    # the same trained weights recalled without the input noise
+    ok_q, acc_q = decisions(recall_counts(tr, W, st, R, T, lg, wm, seed_base, 0.0, dev, "bf16"))
+    ok32_q, acc32_q = decisions(recall_counts(tr, W, st, R, T, lg, wm, seed_base, 0.0, dev, "fp32"))
+    _, plain_q, plain_q_acc, _ = plain_recall(tr, trained, T, lg, wm, expected, seed_base, 0.0, dev, plain_sample,
+                                              False)
+    fp64 = {"with_noise": recall_fp64_errors(tr, trained, W, st, T, lg, wm, expected, seed_base, tr.poisson_hz, dev,
+                                             fp64_sample),
+            "without_noise": recall_fp64_errors(tr, trained, W, st, T, lg, wm, expected, seed_base, 0.0, dev,
+                                                fp64_sample)}
 
-    # the same trained weights recalled without input noise, where recall is
-    # not drowned (noise spikes reach the recurrent projection like any spike)
-    quiet = recall.Recall(tr.H, tr.M, R, tr.pops[0], tr.dt, recall.kepsc_of(tr.projs[0], tr.dt), seed_base, 0.0, dev)
-    quiet.set_cues(lg, tr.eps, wm)
-    quiet.load_state(W, st["bj"], st["epsc"], st["dsup"], st["s_tm3"], st["s_tm2"], st["s_tm1"])
-    quiet.run(tr.t0, T, *count)
-    counts_q = quiet.read("counts")
-    ok_q = recall.recall_decisions(counts_q, tr.H, tr.M, expected)
-    acc_q = recall.hcu_accuracy(counts_q, tr.H, tr.M, expected)
-    quiet.close()
-    plain_q, plain_q_acc = [], []
-    for r in range(plain_sample):
-        net = capi.Net(tr.pops, tr.projs, tr.dt, seed=seed_base + r, poisson_hz=0.0, device=dev, max_ticks=T)
-        for n, a in trained.items():
-            net.write(n, a)
-        net.set_stimulus_idx(lg[r], tr.eps, wm[r])
-        net.run(tr.t0, T, 0.0, tr.old_prn)
-        bits = np.unpackbits(net.spike_log(0).view(np.uint8), axis=1, bitorder="little")[:, :N]
-        counts = bits[: T - 1].sum(axis=0)[None, :]
-        plain_q.append(bool(recall.recall_decisions(counts, tr.H, tr.M, expected[r:r + 1])[0]))
-        plain_q_acc.append(float(recall.hcu_accuracy(counts, tr.H, tr.M, expected[r:r + 1])[0]))
-        net.close()
-    fp64 = profile_value("recall_precision_64x64.md", "fp64_error")
+    def frac(x):
+        return f"{int(np.sum(x))}/{len(x)}"
+
+    def agree(a, b):
+        return f"{int(np.sum(np.asarray(a) == np.asarray(b)))}/{len(a)}"
+
+    def rec(o, a, o32, a32, po, pa):
+        return {"bf16_all": frac(o), "fp32_engine_all": frac(o32), "decisions_agree_bf16_fp32_all": agree(o, o32),
+                "bf16_sample": frac(o[:plain_sample]), "plain_fp32_sample": frac(po),
+                "decisions_agree_bf16_plain_sample": agree(o[:plain_sample], po),
+                "hcu_accuracy_bf16_all": float(a.mean()), "hcu_accuracy_fp32_engine_all": float(a32.mean()),
+                "hcu_accuracy_plain_fp32_sample": float(np.mean(pa)),
+                "hcu_accuracy_bf16_sample": float(a[:plain_sample].mean())}
+
     if cpu:
         try:
             v, sample = cpu_recall_sample(tr.pops, tr.projs, tr.dt, tr.poisson_hz, trained, lg[0], wm[0], tr.eps,
@@ -452,34 +546,28 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     else:
         cpu_base = None
     return {
-        "workload": f"64x64 HCU/MCU full recurrent (4096 x 4096 weights), {work.meta['patterns']} trained patterns, "
-                    f"{R} noise replicates, 25% cue, 20 Hz Poisson noise, {T} recall ticks",
+        "workload": f"64x64 HCU/MCU full recurrent (4096 x 4096 weights), {work.meta['patterns']} patterns trained "
+                    f"300 ticks each, {R} noise replicates, 25% cue, 20 Hz Poisson noise, {T} recall ticks",
         "metric": "replicate ticks/s", "value": value, "unit": "replicate-ticks/s", "steps": steps,
-        "ms_per_step": ms, "us_per_tick": ms * 1e3 / T, "gpu_launches_per_step": launches / max(1, steps),
+        "ms_per_step": ms, "us_per_tick": ms * 1e3 / T, "gpu_launches_per_step": launches,
         "dtype": "bf16 weights x exact 0/1 spikes, fp32 accumulate; fp32 state",
         "roofline": {"bound": "tensor", "kernel": "recall_tick_kernel", "achieved": tflops, "peak": pk["bf16_tflops"],
                      "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"], "peak_kind": pk_kind + " (burst)",
                      "flops_per_tick": 2.0 * R * N * N},
+        "fp32_engine": {"value": value32, "unit": "replicate-ticks/s", "ms_per_step": ms32,
+                        "us_per_tick": ms32 * 1e3 / T, "tflops": tflops32, "gpu_launches_per_step": launches32,
+                        "kernel": "recall_fp32_kernel (SIMT FFMA, W in fp32)",
+                        "fp32_simt_peak_tflops": FP32_SIMT_PEAK_TFLOPS,
+                        "frac_of_fp32_simt_peak": tflops32 / FP32_SIMT_PEAK_TFLOPS},
+        "speedup_bf16_vs_fp32_engine": value / value32,
         "plain_fp32": {"value": plain_rate, "unit": "replicate-ticks/s", "replicates_timed": plain_sample,
                        "ms_per_replicate": statistics.mean(plain_ms),
                        "cell_updates_per_s": plain_cells / (sum(plain_ms) * 1e-3)},
         "speedup_vs_plain_fp32": value / plain_rate,
-        "recall": {"bf16_all": f"{int(ok.sum())}/{R}", "bf16_sample": f"{int(ok[:plain_sample].sum())}/{plain_sample}",
-                   "plain_fp32_sample": f"{sum(plain_ok)}/{plain_sample}",
-                   "decisions_agree_sample": f"{sum(int(a == b) for a, b in zip(ok[:plain_sample], plain_ok))}"
-                                             f"/{plain_sample}",
-                   "hcu_accuracy_bf16_all": float(acc.mean()),
-                   "hcu_accuracy_bf16_sample": float(acc[:plain_sample].mean()),
-                   "hcu_accuracy_plain_fp32_sample": float(np.mean(plain_acc)),
-                   "without_noise": {"bf16_all": f"{int(ok_q.sum())}/{R}",
-                                     "bf16_sample": f"{int(ok_q[:plain_sample].sum())}/{plain_sample}",
-                                     "plain_fp32_sample": f"{sum(plain_q)}/{plain_sample}",
-                                     "decisions_agree_sample":
-                                         f"{sum(int(a == b) for a, b in zip(ok_q[:plain_sample], plain_q))}"
-                                         f"/{plain_sample}",
-                                     "hcu_accuracy_bf16_all": float(acc_q.mean()),
-                                     "hcu_accuracy_bf16_sample": float(acc_q[:plain_sample].mean()),
-                                     "hcu_accuracy_plain_fp32_sample": float(np.mean(plain_q_acc))}},
+        "recall": dict(rec(ok, acc, ok32, acc32, plain_ok, plain_acc),
+                       fp64_sample=fp64["with_noise"]["recall_fp64"],
+                       without_noise=dict(rec(ok_q, acc_q, ok32_q, acc32_q, plain_q, plain_q_acc),
+                                          fp64_sample=fp64["without_noise"]["recall_fp64"])),
         "fp64_error": fp64,
         "cpu_baseline": cpu_base,
     }
@@ -983,6 +1071,48 @@ def cpu_model():
     return "unknown"
 
 
+def extensions_summary(ext):
+    """The headline figures of each extension, short enough to sit near the
+    front of the JSON line (the full objects follow under "extensions")."""
+    out = {}
+    r = ext.get("bf16_recall")
+    if r:
+        f = r.get("fp64_error", {}).get("with_noise", {})
+        out["bf16_recall"] = {
+            "replicate_ticks_per_s": r["value"], "tflops": r["roofline"]["achieved"],
+            "frac_bf16_peak": r["roofline"]["frac"],
+            "speedup_bf16_vs_fp32_engine": r.get("speedup_bf16_vs_fp32_engine"),
+            "speedup_vs_plain_fp32": r.get("speedup_vs_plain_fp32"),
+            "recall_bf16_fp32engine_fp64sample": [r["recall"]["bf16_all"], r["recall"]["fp32_engine_all"],
+                                                 r["recall"].get("fp64_sample")],
+            "recall_without_noise": [r["recall"]["without_noise"]["bf16_all"],
+                                     r["recall"]["without_noise"]["fp32_engine_all"],
+                                     r["recall"]["without_noise"].get("fp64_sample")],
+            "fp64_support_rel_err_max_bf16_fp32": [f.get("bf16_engine", {}).get("support_rel_err_max"),
+                                                   f.get("fp32_engine", {}).get("support_rel_err_max")],
+            "fp64_replicates": f.get("replicates_compared")}
+    b = ext.get("batched")
+    if b:
+        out["batched"] = {"network_ticks_per_s": b["value"], "speedup_vs_plain": b.get("speedup_vs_plain_same_ticks"),
+                          "frac_hbm": b.get("roofline", {}).get("frac"), "cell_updates_per_s": b.get("cell_updates_per_s")}
+    m = ext.get("procupdmulti")
+    if m:
+        out["procupdmulti"] = {"cell_updates_per_s": m["value"]}
+    return out
+
+
+def front(out, key, value, after="dtype"):
+    """out with `key` inserted right after `after`"""
+    res = {}
+    for k, v in out.items():
+        res[k] = v
+        if k == after:
+            res[key] = value
+    if key not in res:
+        res[key] = value
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1023,7 +1153,7 @@ def main():
                                                      cpu=cpu)
             if "procupdmulti" in want:
                 ext["procupdmulti"] = run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)
-            print(json.dumps({"extensions": ext}), flush=True)
+            print(json.dumps({"extensions_summary": extensions_summary(ext), "extensions": ext}), flush=True)
         return
     out = run_ours(args, rank, world, local_rank, cpu=cpu)
     # the extensions are single-GPU measurements: under torchrun the other
@@ -1034,6 +1164,7 @@ def main():
                              "batched": run_batch_extension(local_rank, max(1, args.steps // 2),
                                                             n_nets=args.batch_nets, cpu=cpu),
                              "procupdmulti": run_multi_extension(local_rank, max(1, args.steps // 2), 1, cpu=cpu)}
+        out = front(out, "extensions_summary", extensions_summary(out["extensions"]))
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

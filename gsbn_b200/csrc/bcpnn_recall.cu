@@ -1,23 +1,30 @@
 /*
  * bcpnn_recall.cu -- replicate recall engine (include/bcpnn_recall.h).
  *
- * One launch per tick.  CTA tile = 128 replicates x 256 destination MCUs
- * (four HCUs of 64, or more of fewer MCUs); the K loop runs over the N source
- * MCUs in stages of 64.
+ * Two launches per tick on two streams, side by side: the population update
+ * of tick t (recall_pop_kernel: support from epsc(t-1), softmax/WTA, Philox
+ * spikes, writing dsup(t), the BF16 spike row S(t) and the recall counters)
+ * and the contraction with its epilogue epsc(t) = epsc(t-1) * (1 - kepsc) +
+ * S(t-3) . W.  The contraction comes in two forms, chosen at create time:
  *
+ * BF16 (recall_tick_kernel), persistent, CTA tile = 128 replicates x 256
+ * destination MCUs, the K loop over the N source MCUs in stages of 64:
  *   warp 0      TMA producer: S(t-3) tile [128 x 64] and W^T tile [256 x 64]
  *               (BF16, 128-byte swizzle) into a 4-stage shared-memory ring,
  *               one mbarrier per stage with the transaction byte count;
- *   warp 1      allocates 256 TMEM columns; one elected thread issues
- *               tcgen05.mma.cta_group::1.kind::f16 (M=128, N=256, K=16, FP32
- *               accumulate) per 16-wide K step and tcgen05.commit to free each
- *               stage and, at the end, to signal the accumulator;
+ *   warp 1      allocates 512 TMEM columns (two accumulators); one elected
+ *               thread issues tcgen05.mma.cta_group::1.kind::f16 (M=128,
+ *               N=256, K=16, FP32 accumulate) per 16-wide K step and
+ *               tcgen05.commit to free each stage and, at the end, to signal
+ *               the accumulator;
  *   warps 2..5  epilogue, one replicate row per thread (TMEM lane = row):
- *               while the contraction runs, the population update of tick t
- *               from epsc(t-1) (support, softmax/WTA, Philox spikes) for the
- *               tile's HCUs, writing dsup(t), the BF16 spike row S(t) and the
- *               recall counters; then tcgen05.ld of the accumulator and
- *               epsc(t) = epsc(t-1) * (1 - kepsc) + acc.
+ *               tcgen05.ld of the accumulator and the epsc update.
+ *
+ * FP32 (recall_fp32_kernel): the same contraction on the FP32 pipes with W
+ * kept in FP32 -- a register-tiled SIMT product (CTA tile 128 x 128, 8 x 8
+ * outputs per thread, K stages of 16 double-buffered in shared memory) with
+ * the same epilogue expression.  It exists to measure the tensor-core form
+ * against the same engine at full precision.
  *
  * Every mbarrier wait is bounded (1 s of %globaltimer); a wait that runs out
  * sets an error bit and the CTA leaves its loops, waits (bounded) for its own
@@ -454,6 +461,110 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+constexpr int kF32BM = 128, kF32BN = 128, kF32BK = 16, kF32Threads = 256;
+
+/* FP32 SIMT contraction with the epsc epilogue of recall_tick_kernel:
+   epsc(t)[r][j] = epsc(t-1)[r][j] * (1 - kepsc) + sum_i S(t-3)[r][i] * W[i][j]
+   with W in FP32 ([source i][destination j], row-major) and S the BF16 0/1
+   spike ring (its value is exact: the bits shifted into an FP32 word).
+
+   One CTA per 128 x 128 output tile (blockIdx.x = M-tile * (N/128) + N-tile);
+   thread (ty, tx) = (tid / 16, tid % 16) owns rows {ty*4 .. +3, 64 + ty*4 ..
+   +3} and columns {tx*4 .. +3, 64 + tx*4 .. +3} of the tile, 64 FP32
+   accumulators.  K stages of 16: S as [k][row] and W as [k][col] in shared
+   memory, two buffers, the next stage's global loads held in registers while
+   the current one is multiplied, one barrier per stage. */
+__global__ void __launch_bounds__(kF32Threads, 2)
+    recall_fp32_kernel(const uint16_t* __restrict__ s, const float* __restrict__ w, Params p) {
+  __shared__ __align__(16) float As[2][kF32BK][kF32BM];
+  __shared__ __align__(16) float Bs[2][kF32BK][kF32BN];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int nN = p.N / kF32BN, nM = p.R / kF32BM;
+  const int m0 = ((int)blockIdx.x / nN) * kF32BM, n0 = ((int)blockIdx.x % nN) * kF32BN;
+  /* self-check: whole tiles, the tile inside the arrays, 16-byte alignment of
+     every vector access */
+  {
+    const bool bad = p.N % kF32BN != 0 || p.R % kF32BM != 0 || (int)blockIdx.x >= nN * nM ||
+                     (reinterpret_cast<uintptr_t>(s) & 15) || (reinterpret_cast<uintptr_t>(w) & 15) ||
+                     (reinterpret_cast<uintptr_t>(p.epsc_prev) & 15) ||
+                     (reinterpret_cast<uintptr_t>(p.epsc_cur) & 15);
+    if (bad) {
+      if (tid == 0 && atomicOr(p.err, kErrAlign) == 0) p.err[1] = -1 - (int)blockIdx.x;
+      return;
+    }
+  }
+  /* S stage: row a_row, eight BF16 at a_k (one 16-byte load); W stage: row
+     b_k, eight floats at b_n (two 16-byte loads) */
+  const int a_row = tid & 127, a_k = (tid >> 7) * 8;
+  const int b_k = tid >> 4, b_n = (tid & 15) * 8;
+  const uint16_t* ag = s + (size_t)(m0 + a_row) * p.N + a_k;
+  const float* bg = w + (size_t)b_k * p.N + n0 + b_n;
+  const size_t b_step = (size_t)kF32BK * p.N;
+  uint4 ra = __ldg(reinterpret_cast<const uint4*>(ag));
+  float4 rb0 = __ldg(reinterpret_cast<const float4*>(bg));
+  float4 rb1 = __ldg(reinterpret_cast<const float4*>(bg + 4));
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+
+  auto stage = [&](int buf) {
+    const uint32_t u[4] = {ra.x, ra.y, ra.z, ra.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      As[buf][a_k + 2 * j][a_row] = __uint_as_float(u[j] << 16);
+      As[buf][a_k + 2 * j + 1][a_row] = __uint_as_float(u[j] & 0xFFFF0000u);
+    }
+    *reinterpret_cast<float4*>(&Bs[buf][b_k][b_n]) = rb0;
+    *reinterpret_cast<float4*>(&Bs[buf][b_k][b_n + 4]) = rb1;
+  };
+  stage(0);
+  __syncthreads();
+  const int kTiles = p.N / kF32BK;
+  for (int kt = 0; kt < kTiles; kt++) {
+    const int buf = kt & 1;
+    if (kt + 1 < kTiles) {
+      ra = __ldg(reinterpret_cast<const uint4*>(ag + (size_t)(kt + 1) * kF32BK));
+      const float* b = bg + (size_t)(kt + 1) * b_step;
+      rb0 = __ldg(reinterpret_cast<const float4*>(b));
+      rb1 = __ldg(reinterpret_cast<const float4*>(b + 4));
+    }
+#pragma unroll
+    for (int k = 0; k < kF32BK; k++) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][k][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][k][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][k][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][k][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    /* the other buffer was last read in stage kt-1, before the barrier
+       that ended it */
+    if (kt + 1 < kTiles) stage(buf ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int row = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const size_t o = (size_t)row * p.N + n0 + h * 64 + tx * 4;
+      const float4 e = *reinterpret_cast<const float4*>(p.epsc_prev + o);
+      float4 v;
+      v.x = e.x * p.one_m_kepsc + acc[i][h * 4 + 0];
+      v.y = e.y * p.one_m_kepsc + acc[i][h * 4 + 1];
+      v.z = e.z * p.one_m_kepsc + acc[i][h * 4 + 2];
+      v.w = e.w * p.one_m_kepsc + acc[i][h * 4 + 3];
+      *reinterpret_cast<float4*>(p.epsc_cur + o) = v;
+    }
+  }
+}
+
 __global__ void broadcast_spikes_kernel(uint16_t* s, int R, int N, const int8_t* row) {
   size_t n = (size_t)R * N;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -479,7 +590,8 @@ struct bcpnn_recall {
   float* dsup[2] = {nullptr, nullptr};
   float* epsc[2] = {nullptr, nullptr};
   uint16_t* s[4] = {nullptr, nullptr, nullptr, nullptr}; /* spike ring, by tick mod 4 */
-  uint16_t* wt = nullptr; /* W^T BF16 [N][N] */
+  uint16_t* wt = nullptr; /* W^T BF16 [N][N] (BF16 contraction) */
+  float* wf = nullptr;    /* W FP32 [N][N], [source][destination] (FP32 contraction) */
   uint8_t* counts = nullptr;
   float* bj = nullptr;
   int32_t* lgidx = nullptr;
@@ -579,6 +691,8 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
   const long long N = (long long)H * M;
   if (N % kTileN || kTileN % M || (M != 16 && M != 32 && M != 64) || N > 65536) return BCPNN_ERR_INVALID;
   if (!(d->dt > 0.f) || !(d->pop.taum > 0.f) || d->poisson_noise_hz < 0.f) return BCPNN_ERR_INVALID;
+  if (d->contraction != BCPNN_RECALL_BF16 && d->contraction != BCPNN_RECALL_FP32) return BCPNN_ERR_INVALID;
+  const bool fp32 = d->contraction == BCPNN_RECALL_FP32;
   bcpnn_recall* r = new bcpnn_recall();
   r->d = *d;
   r->N = (int)N;
@@ -599,7 +713,8 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
   for (int i = 0; i < 2 && !rc; i++) rc = dalloc(r, &r->dsup[i], RN);
   for (int i = 0; i < 2 && !rc; i++) rc = dalloc(r, &r->epsc[i], RN);
   for (int i = 0; i < 4 && !rc; i++) rc = dalloc(r, &r->s[i], RN);
-  if (!rc) rc = dalloc(r, &r->wt, (size_t)N * N);
+  if (!rc && !fp32) rc = dalloc(r, &r->wt, (size_t)N * N);
+  if (!rc && fp32) rc = dalloc(r, &r->wf, (size_t)N * N);
   if (!rc) rc = dalloc(r, &r->counts, RN);
   if (!rc) rc = dalloc(r, &r->bj, (size_t)N);
   if (!rc) rc = dalloc(r, &r->lgidx, (size_t)R * H);
@@ -608,12 +723,14 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
   if (rc) return bad(rc);
   if (cudaMemset(r->err, 0, 2 * sizeof(int)) != cudaSuccess || cudaMemset(r->counts, 0, RN) != cudaSuccess)
     return bad(BCPNN_ERR_CUDA);
-  for (int i = 0; i < 4 && !rc; i++) rc = encode_map(r, &r->map_s[i], r->s[i], R, (int)N, kTileM);
-  if (!rc) rc = encode_map(r, &r->map_w, r->wt, (int)N, (int)N, kTileN);
-  if (rc) return bad(rc);
-  cudaError_t e = cudaSuccess;
-  e = cudaFuncSetAttribute(recall_tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-  if (e != cudaSuccess) return bad(BCPNN_ERR_CUDA);
+  if (!fp32) {
+    for (int i = 0; i < 4 && !rc; i++) rc = encode_map(r, &r->map_s[i], r->s[i], R, (int)N, kTileM);
+    if (!rc) rc = encode_map(r, &r->map_w, r->wt, (int)N, (int)N, kTileN);
+    if (rc) return bad(rc);
+    if (cudaFuncSetAttribute(recall_tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) !=
+        cudaSuccess)
+      return bad(BCPNN_ERR_CUDA);
+  }
   if (cudaStreamCreateWithFlags(&r->pop_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->ev_pop, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->ev_gemm, cudaEventDisableTiming) != cudaSuccess)
@@ -643,11 +760,16 @@ int bcpnn_recall_load(bcpnn_recall* r, const float* w, const float* bj, const fl
     return fail(r, BCPNN_ERR_INVALID, "null buffer");
   const int N = r->N, R = r->d.replicates;
   RCU(cudaSetDevice(r->d.device));
-  /* W^T in BF16: row j = destination MCU, K-contiguous over source MCUs */
-  std::vector<uint16_t> wt((size_t)N * N);
-  for (int i = 0; i < N; i++)
-    for (int j = 0; j < N; j++) wt[(size_t)j * N + i] = to_bf16(w[(size_t)i * N + j]);
-  RCU(cudaMemcpy(r->wt, wt.data(), wt.size() * 2, cudaMemcpyHostToDevice));
+  if (r->wf) {
+    /* FP32 contraction: W as given, [source][destination] */
+    RCU(cudaMemcpy(r->wf, w, (size_t)N * N * 4, cudaMemcpyHostToDevice));
+  } else {
+    /* W^T in BF16: row j = destination MCU, K-contiguous over source MCUs */
+    std::vector<uint16_t> wt((size_t)N * N);
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < N; j++) wt[(size_t)j * N + i] = to_bf16(w[(size_t)i * N + j]);
+    RCU(cudaMemcpy(r->wt, wt.data(), wt.size() * 2, cudaMemcpyHostToDevice));
+  }
   RCU(cudaMemcpy(r->bj, bj, (size_t)N * 4, cudaMemcpyHostToDevice));
   float* row_f = nullptr;
   int8_t* row_s = nullptr;
@@ -742,6 +864,7 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
   p.err = r->err;
   const int n_tiles = (r->N / kTileN) * (d.replicates / kTileM);
   const int grid = n_tiles < r->sms ? n_tiles : r->sms;
+  const int f32_tiles = (r->N / kF32BN) * (d.replicates / kF32BM);
   const int pop_blocks = (int)((size_t)d.replicates * d.hcu_num * 4 / 256);
   /* Tick kk: the population update needs epsc(kk-1) and dsup(kk-1); the
      contraction needs S(kk-3) and epsc(kk-1).  So both wait only for tick
@@ -760,12 +883,14 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
     p.s_out = r->s[mod4(kk)];
     p.simstep = first + i;
     p.count_on = (first + i >= count_first && first + i <= count_last) ? 1 : 0;
-    const CUtensorMap& ms = r->map_s[mod4(kk - 3)];
     if (d.mcu_num == 16) recall_pop_kernel<16><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
     if (d.mcu_num == 32) recall_pop_kernel<32><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
     if (d.mcu_num == 64) recall_pop_kernel<64><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
     RCU(cudaGetLastError());
-    recall_tick_kernel<<<grid, kThreads, kSmemBytes, r->stream>>>(ms, r->map_w, p);
+    if (r->wf)
+      recall_fp32_kernel<<<f32_tiles, kF32Threads, 0, r->stream>>>(r->s[mod4(kk - 3)], r->wf, p);
+    else
+      recall_tick_kernel<<<grid, kThreads, kSmemBytes, r->stream>>>(r->map_s[mod4(kk - 3)], r->map_w, p);
     RCU(cudaGetLastError());
     /* both kernels of tick kk are queued: each stream waits for the other's
        kernel of this tick before its kernel of tick kk+1 */

@@ -19,7 +19,11 @@ RECALL_EXPORTS = (
 class RecallDesc(ctypes.Structure):
     _fields_ = [("hcu_num", ctypes.c_int32), ("mcu_num", ctypes.c_int32), ("replicates", ctypes.c_int32),
                 ("pop", capi.PopDesc), ("dt", ctypes.c_float), ("kepsc", ctypes.c_float),
-                ("seed_base", ctypes.c_uint32), ("poisson_noise_hz", ctypes.c_float), ("device", ctypes.c_int32)]
+                ("seed_base", ctypes.c_uint32), ("poisson_noise_hz", ctypes.c_float), ("device", ctypes.c_int32),
+                ("contraction", ctypes.c_int32)]
+
+
+CONTRACTIONS = {"bf16": 0, "fp32": 1}
 
 
 _lib = None
@@ -58,13 +62,17 @@ def _p(a):
 
 
 class Recall:
-    """R replicates of one trained population on one GPU."""
+    """R replicates of one trained population on one GPU; `contraction` is
+    "bf16" (tensor cores, W rounded to BF16) or "fp32" (SIMT, W in FP32)."""
 
-    def __init__(self, hcu, mcu, replicates, pop, dt, kepsc, seed_base=0, poisson_hz=0.0, device=0):
+    def __init__(self, hcu, mcu, replicates, pop, dt, kepsc, seed_base=0, poisson_hz=0.0, device=0,
+                 contraction="bf16"):
         self._lib = load()
         self._h = ctypes.c_void_p()
         self.H, self.M, self.R, self.N = hcu, mcu, replicates, hcu * mcu
-        d = RecallDesc(hcu, mcu, replicates, capi.PopDesc(**pop), dt, kepsc, seed_base, poisson_hz, device)
+        self.contraction = contraction
+        d = RecallDesc(hcu, mcu, replicates, capi.PopDesc(**pop), dt, kepsc, seed_base, poisson_hz, device,
+                       CONTRACTIONS[contraction])
         rc = self._lib.bcpnn_recall_create(ctypes.byref(d), ctypes.byref(self._h))
         if rc != 0:
             raise capi.BcpnnError(rc, self._lib.bcpnn_status_string(rc).decode())

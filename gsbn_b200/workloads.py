@@ -215,12 +215,15 @@ def config1(seed=0, record=True, check=True, n_patterns=100, train_ticks=100, re
                       record=record, check=check)
 
 
-def config4(seed=0, hcu=64, mcu=64, n_patterns=16, train_ticks=100, rest_ticks=20, recall_ticks=200,
+def config4(seed=0, hcu=64, mcu=64, n_patterns=16, train_ticks=300, rest_ticks=20, recall_ticks=200,
             cue_frac=0.25, poisson_hz=20.0, record=False, check=False):
     """The network of the replicate recall workload: 64x64 HCU/MCU, full
-    recurrent projection (C = 4096, 4096 x 4096 weights), patterns trained
-    100 ticks each with rests, 20 Hz Poisson input noise; the recall segments
-    (25% of HCUs cued, 200 ticks) are what the replicates run."""
+    recurrent projection (C = 4096, 4096 x 4096 weights), 16 patterns trained
+    300 ticks each with 20-tick rests, 20 Hz Poisson input noise; the recall
+    segments (25% of HCUs cued, 200 ticks) are what the replicates run.  At
+    300 training ticks per pattern ProcCheck's all-HCU recall is non-zero
+    (the last-trained patterns are recalled, with and without the input
+    noise); at 100 it is zero for every replicate."""
     return single_pop(f"{hcu}x{mcu} full recurrent", hcu, mcu, n_patterns, train_ticks, rest_ticks, recall_ticks,
                       cue_frac, hcu, seed=seed, record=record, check=check, poisson_hz=poisson_hz)
 

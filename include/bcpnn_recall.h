@@ -27,6 +27,8 @@
  *
  * Limits: N = H*M a multiple of 256, M dividing 256 (HCUs never straddle a
  * 256-column tile), R a multiple of 128, one population.  sm_100a only.
+ * desc.contraction selects an FP32 form of the contraction (W kept in FP32,
+ * SIMT multiply-adds) with everything else unchanged.
  */
 #ifndef BCPNN_RECALL_H
 #define BCPNN_RECALL_H
@@ -51,13 +53,24 @@ typedef struct bcpnn_recall_desc {
   uint32_t seed_base;        /* replicate r uses Philox key seed_base + r */
   float poisson_noise_hz;
   int32_t device;
+  int32_t contraction;       /* BCPNN_RECALL_BF16 (0) or BCPNN_RECALL_FP32 (1) */
 } bcpnn_recall_desc;
+
+/* The form of the support contraction S(t-3) . W:
+   BCPNN_RECALL_BF16  W rounded once to BF16, tcgen05 tensor-core MMA with
+                      FP32 accumulation in tensor memory;
+   BCPNN_RECALL_FP32  W kept in FP32, FP32 fused multiply-adds on the SIMT
+                      pipes (the same engine at full precision, for measuring
+                      the BF16 form against).
+   Both accumulate in FP32 in an order of their own, not gsbn's row order, and
+   share the population kernel and the epsc epilogue. */
+enum { BCPNN_RECALL_BF16 = 0, BCPNN_RECALL_FP32 = 1 };
 
 int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out);
 int bcpnn_recall_destroy(bcpnn_recall* r);
 
 /* Trained state, shared by every replicate: W[i*N + j] = w_ij from source MCU
-   i to destination MCU j (float, rounded to BF16 here), bj[N], and the
+   i to destination MCU j (float; rounded to BF16 here in the BF16 form), bj[N], and the
    population state at the end of tick first-1: epsc[N], dsup[N], the spikes
    of ticks first-3, first-2 and first-1 (int8 [N] each; in a gsbn network
    these are .siq, bit 0 of qi and si of the slots, by source MCU). */
