@@ -346,8 +346,10 @@ def time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, contraction, ste
     """One form of the replicate engine on the recall workload: the counted
     run first (ProcCheck's counters over the ticks strictly inside the
     segment), then `warmup` untimed and `steps` timed runs of T ticks, each
-    from the trained state (the state load is outside the timed region).
-    Returns (ms per run, counts, kernel launches per run)."""
+    from the trained state (the state load is outside the timed region).  In
+    the timed runs the engine also times every contraction launch in place
+    (a CUDA event pair on its stream around each launch).  Returns (ms per
+    run, counts, kernel launches per run, ms per contraction launch)."""
     import torch
     eng = _recall_engine(tr, W, st, R, lg, wm, seed_base, tr.poisson_hz, dev, contraction)
     try:
@@ -363,6 +365,7 @@ def time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, contraction, ste
             load()
             eng.run(tr.t0, T)
         times, launches = [], 0
+        eng.timing(True)
         for _ in range(steps):
             load()
             l0 = eng.launches()
@@ -374,9 +377,10 @@ def time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, contraction, ste
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
             launches += eng.launches() - l0
+        c_ms, c_n = eng.contraction_time()
     finally:
         eng.close()
-    return statistics.mean(times), counts, launches / max(1, steps)
+    return statistics.mean(times), counts, launches / max(1, steps), c_ms / max(1, c_n)
 
 
 def recall_counts(tr, W, st, R, T, lg, wm, seed_base, hz, dev, contraction):
@@ -496,10 +500,12 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
     R, T, seed_base, H, M = replicates, ticks, 1, tr.H, tr.M
     N = H * M
     lg, wm, expected = tr.cues(R)
-    ms, counts, launches = time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, "bf16", steps, warmup)
-    ms32, counts32, launches32 = time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, "fp32", steps, warmup)
+    ms, counts, launches, k_ms = time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, "bf16", steps, warmup)
+    ms32, counts32, launches32, k_ms32 = time_recall_engine(tr, W, st, R, T, lg, wm, seed_base, dev, "fp32", steps,
+                                                            warmup)
     flops = 2.0 * R * N * N * T
     tflops, tflops32 = flops / (ms * 1e-3) / 1e12, flops / (ms32 * 1e-3) / 1e12
+    k_tflops, k_tflops32 = flops / T / (k_ms * 1e-3) / 1e12, flops / T / (k_ms32 * 1e-3) / 1e12
     pk, pk_kind = peaks()
     value, value32 = R * T / (ms * 1e-3), R * T / (ms32 * 1e-3)
 
@@ -551,14 +557,19 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
         "metric": "replicate ticks/s", "value": value, "unit": "replicate-ticks/s", "steps": steps,
         "ms_per_step": ms, "us_per_tick": ms * 1e3 / T, "gpu_launches_per_step": launches,
         "dtype": "bf16 weights x exact 0/1 spikes, fp32 accumulate; fp32 state",
-        "roofline": {"bound": "tensor", "kernel": "recall_tick_kernel", "achieved": tflops, "peak": pk["bf16_tflops"],
-                     "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"], "peak_kind": pk_kind + " (burst)",
-                     "flops_per_tick": 2.0 * R * N * N},
+        "roofline": {"bound": "tensor", "kernel": "recall_tick_kernel", "achieved": k_tflops,
+                     "peak": pk["bf16_tflops"], "unit": "TFLOP/s", "frac": k_tflops / pk["bf16_tflops"],
+                     "peak_kind": pk_kind + " (burst)", "flops_per_launch": 2.0 * R * N * N,
+                     "us_per_launch": k_ms * 1e3,
+                     "timing": "CUDA event pair around every contraction launch on its stream, in place beside the "
+                               "population kernel of the same tick",
+                     "tick_tflops": tflops, "tick_frac": tflops / pk["bf16_tflops"]},
         "fp32_engine": {"value": value32, "unit": "replicate-ticks/s", "ms_per_step": ms32,
                         "us_per_tick": ms32 * 1e3 / T, "tflops": tflops32, "gpu_launches_per_step": launches32,
+                        "contraction_us_per_launch": k_ms32 * 1e3, "contraction_tflops": k_tflops32,
                         "kernel": "recall_fp32_kernel (SIMT FFMA, W in fp32)",
                         "fp32_simt_peak_tflops": FP32_SIMT_PEAK_TFLOPS,
-                        "frac_of_fp32_simt_peak": tflops32 / FP32_SIMT_PEAK_TFLOPS},
+                        "frac_of_fp32_simt_peak": k_tflops32 / FP32_SIMT_PEAK_TFLOPS},
         "speedup_bf16_vs_fp32_engine": value / value32,
         "plain_fp32": {"value": plain_rate, "unit": "replicate-ticks/s", "replicates_timed": plain_sample,
                        "ms_per_replicate": statistics.mean(plain_ms),
@@ -1079,8 +1090,8 @@ def extensions_summary(ext):
     if r:
         f = r.get("fp64_error", {}).get("with_noise", {})
         out["bf16_recall"] = {
-            "replicate_ticks_per_s": r["value"], "tflops": r["roofline"]["achieved"],
-            "frac_bf16_peak": r["roofline"]["frac"],
+            "replicate_ticks_per_s": r["value"], "contraction_tflops": r["roofline"]["achieved"],
+            "contraction_frac_bf16_peak": r["roofline"]["frac"], "tick_frac_bf16_peak": r["roofline"]["tick_frac"],
             "speedup_bf16_vs_fp32_engine": r.get("speedup_bf16_vs_fp32_engine"),
             "speedup_vs_plain_fp32": r.get("speedup_vs_plain_fp32"),
             "recall_bf16_fp32engine_fp64sample": [r["recall"]["bf16_all"], r["recall"]["fp32_engine_all"],

@@ -191,10 +191,13 @@ __device__ __forceinline__ float dsup_mcu0(const Params& p, int row, uint32_t se
 }
 
 /* Population update of tick `simstep` (Pop.cpp:229-323) for one quarter of
-   one HCU of one replicate: four consecutive lanes hold the four quarters of
-   an HCU (Q = M/4 MCUs each).  The HCU maximum is a shuffle max (exact); the
+   one HCU of one replicate: thread tid = (replicate * H + HCU) * 4 + q holds
+   MCUs q*Q .. q*Q+Q-1 of the HCU (Q = M/4), so four consecutive lanes hold
+   the four quarters of an HCU.  The HCU maximum is a shuffle max (exact); the
    activity sum keeps gsbn's serial MCU order by passing the running sum from
-   lane to lane; one Philox call per four MCUs and stream. */
+   lane to lane; one Philox call per four MCUs and stream.  Its own kernel,
+   run beside the contraction on a second stream: a CTA of the contraction
+   leaves room on its SM for three of its CTAs. */
 template <int M>
 __global__ void __launch_bounds__(256) recall_pop_kernel(Params p) {
   constexpr int Q = M / 4;
@@ -212,8 +215,9 @@ __global__ void __launch_bounds__(256) recall_pop_kernel(Params p) {
                      (reinterpret_cast<uintptr_t>(p.dsup_prev) & 15) || (reinterpret_cast<uintptr_t>(p.dsup_cur) & 15) ||
                      (reinterpret_cast<uintptr_t>(p.epsc_prev) & 15) || (reinterpret_cast<uintptr_t>(p.bj) & 15) ||
                      (reinterpret_cast<uintptr_t>(p.s_out) & 15) || (reinterpret_cast<uintptr_t>(p.counts) & 15);
-    if (bad) {
-      if (atomicOr(p.err, kErrAlign) == 0) p.err[1] = tid;
+    /* the warp leaves together: the shuffles below take all 32 lanes */
+    if (__any_sync(0xffffffffu, bad)) {
+      if (bad && atomicOr(p.err, kErrAlign) == 0) p.err[1] = tid;
       return;
     }
   }
@@ -605,6 +609,11 @@ struct bcpnn_recall {
   CUtensorMap map_w;
   uint64_t launches = 0;
   int sms = 148;
+  /* in-place timing of the contraction launches (bcpnn_recall_timing) */
+  bool timing = false;
+  std::vector<cudaEvent_t> tev;
+  double contraction_ms = 0.0;
+  uint64_t contraction_launches = 0;
   std::string last_error;
   std::vector<void*> allocs;
 };
@@ -707,7 +716,12 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
   if (major != 10 || minor != 0) return bad(BCPNN_ERR_DEVICE);
   cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, d->device);
   if (r->sms < 1) r->sms = 1;
-  if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(BCPNN_ERR_CUDA);
+  /* the contraction's stream first in the block scheduler's order: its CTAs
+     (one per SM) take their SMs before the population update fills the rest */
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  if (cudaStreamCreateWithPriority(&r->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess)
+    return bad(BCPNN_ERR_CUDA);
   size_t RN = (size_t)R * N;
   int rc = BCPNN_OK;
   for (int i = 0; i < 2 && !rc; i++) rc = dalloc(r, &r->dsup[i], RN);
@@ -731,7 +745,7 @@ int bcpnn_recall_create(const bcpnn_recall_desc* d, bcpnn_recall** out) {
         cudaSuccess)
       return bad(BCPNN_ERR_CUDA);
   }
-  if (cudaStreamCreateWithFlags(&r->pop_stream, cudaStreamNonBlocking) != cudaSuccess ||
+  if (cudaStreamCreateWithPriority(&r->pop_stream, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->ev_pop, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->ev_gemm, cudaEventDisableTiming) != cudaSuccess)
     return bad(BCPNN_ERR_CUDA);
@@ -745,6 +759,7 @@ int bcpnn_recall_destroy(bcpnn_recall* r) {
   if (r->stream) cudaStreamSynchronize(r->stream);
   if (r->pop_stream) cudaStreamSynchronize(r->pop_stream);
   for (void* p : r->allocs) cudaFree(p);
+  for (cudaEvent_t e : r->tev) cudaEventDestroy(e);
   if (r->ev_pop) cudaEventDestroy(r->ev_pop);
   if (r->ev_gemm) cudaEventDestroy(r->ev_gemm);
   if (r->pop_stream) cudaStreamDestroy(r->pop_stream);
@@ -871,6 +886,13 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
      kk-1 and run side by side: pop(kk) after gemm(kk-1) (it also must not
      overwrite S(kk) = S(kk-4) while gemm(kk-1) reads it), gemm(kk) after
      pop(kk-1) (which last read the epsc buffer gemm(kk) writes). */
+  if (r->timing) {
+    while (r->tev.size() < 2 * (size_t)n_ticks) {
+      cudaEvent_t e;
+      RCU(cudaEventCreate(&e));
+      r->tev.push_back(e);
+    }
+  }
   RCU(cudaEventRecord(r->ev_gemm, r->stream));
   RCU(cudaStreamWaitEvent(r->pop_stream, r->ev_gemm, 0));
   for (int i = 0; i < n_ticks; i++) {
@@ -887,11 +909,13 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
     if (d.mcu_num == 32) recall_pop_kernel<32><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
     if (d.mcu_num == 64) recall_pop_kernel<64><<<pop_blocks, 256, 0, r->pop_stream>>>(p);
     RCU(cudaGetLastError());
+    if (r->timing) RCU(cudaEventRecord(r->tev[2 * i], r->stream));
     if (r->wf)
       recall_fp32_kernel<<<f32_tiles, kF32Threads, 0, r->stream>>>(r->s[mod4(kk - 3)], r->wf, p);
     else
       recall_tick_kernel<<<grid, kThreads, kSmemBytes, r->stream>>>(r->map_s[mod4(kk - 3)], r->map_w, p);
     RCU(cudaGetLastError());
+    if (r->timing) RCU(cudaEventRecord(r->tev[2 * i + 1], r->stream));
     /* both kernels of tick kk are queued: each stream waits for the other's
        kernel of this tick before its kernel of tick kk+1 */
     RCU(cudaEventRecord(r->ev_pop, r->pop_stream));
@@ -902,7 +926,16 @@ int bcpnn_recall_run(bcpnn_recall* r, int32_t first, int32_t n_ticks, int32_t co
   r->kk += n_ticks;
   r->counted += counted;
   r->launches += 2 * (uint64_t)n_ticks;
-  return check_err(r);
+  int rc = check_err(r); /* synchronises the stream: every timing event has completed */
+  if (rc == BCPNN_OK && r->timing) {
+    for (int i = 0; i < n_ticks; i++) {
+      float ms = 0.f;
+      RCU(cudaEventElapsedTime(&ms, r->tev[2 * i], r->tev[2 * i + 1]));
+      r->contraction_ms += ms;
+    }
+    r->contraction_launches += (uint64_t)n_ticks;
+  }
+  return rc;
 }
 
 static int resolve_rows(bcpnn_recall* r, const char* name, int32_t row0, int32_t n_rows, size_t bytes, void** base,
@@ -997,6 +1030,21 @@ int bcpnn_recall_get_stream(const bcpnn_recall* r, void** stream) {
 int bcpnn_recall_launches(const bcpnn_recall* r, uint64_t* out) {
   if (!r || !out) return BCPNN_ERR_INVALID;
   *out = r->launches;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_timing(bcpnn_recall* r, int32_t on) {
+  if (!r) return BCPNN_ERR_INVALID;
+  r->timing = on != 0;
+  r->contraction_ms = 0.0;
+  r->contraction_launches = 0;
+  return BCPNN_OK;
+}
+
+int bcpnn_recall_contraction_time(const bcpnn_recall* r, double* total_ms, uint64_t* n_launches) {
+  if (!r || !total_ms || !n_launches) return BCPNN_ERR_INVALID;
+  *total_ms = r->contraction_ms;
+  *n_launches = r->contraction_launches;
   return BCPNN_OK;
 }
 

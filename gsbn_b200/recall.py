@@ -12,7 +12,7 @@ from . import capi
 RECALL_EXPORTS = (
     "bcpnn_recall_create", "bcpnn_recall_destroy", "bcpnn_recall_load", "bcpnn_recall_set_cues", "bcpnn_recall_run",
     "bcpnn_recall_clear_counts", "bcpnn_recall_read", "bcpnn_recall_write", "bcpnn_recall_get_stream",
-    "bcpnn_recall_launches", "bcpnn_recall_last_error",
+    "bcpnn_recall_launches", "bcpnn_recall_last_error", "bcpnn_recall_timing", "bcpnn_recall_contraction_time",
 )
 
 
@@ -48,6 +48,8 @@ def load():
         "bcpnn_recall_get_stream": (ctypes.c_int, [vp, P(vp)]),
         "bcpnn_recall_launches": (ctypes.c_int, [vp, P(ctypes.c_uint64)]),
         "bcpnn_recall_last_error": (ctypes.c_char_p, [vp]),
+        "bcpnn_recall_timing": (ctypes.c_int, [vp, i32]),
+        "bcpnn_recall_contraction_time": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -120,6 +122,16 @@ class Recall:
         v = ctypes.c_uint64()
         self._check(self._lib.bcpnn_recall_launches(self._h, ctypes.byref(v)))
         return v.value
+
+    def timing(self, on=True):
+        """switch the in-place timing of the contraction launches (clears the sums)"""
+        self._check(self._lib.bcpnn_recall_timing(self._h, 1 if on else 0))
+
+    def contraction_time(self):
+        """(summed milliseconds, launches) of the timed contraction launches"""
+        ms, n = ctypes.c_double(), ctypes.c_uint64()
+        self._check(self._lib.bcpnn_recall_contraction_time(self._h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
 
     def close(self):
         if self._h:

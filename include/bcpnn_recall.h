@@ -102,6 +102,15 @@ int bcpnn_recall_write(bcpnn_recall* r, const char* name, int32_t row0, int32_t 
                        size_t bytes);
 
 int bcpnn_recall_get_stream(const bcpnn_recall* r, void** stream);
+
+/* In-place timing of the contraction kernel: with timing on, bcpnn_recall_run
+   records a CUDA event pair around every contraction launch on the engine's
+   stream -- each launch timed where it runs, beside the population update of
+   the same tick -- and adds the elapsed times up when the run synchronises.
+   bcpnn_recall_timing(r, on) switches it and clears the sums;
+   bcpnn_recall_contraction_time reads the summed milliseconds and launches. */
+int bcpnn_recall_timing(bcpnn_recall* r, int32_t on);
+int bcpnn_recall_contraction_time(const bcpnn_recall* r, double* total_ms, uint64_t* n_launches);
 int bcpnn_recall_launches(const bcpnn_recall* r, uint64_t* out);
 const char* bcpnn_recall_last_error(const bcpnn_recall* r);
 

@@ -99,6 +99,7 @@ def test_synthetic_ticks(H, M, R, contraction):
     # the BF16 form multiplies W rounded once to BF16, the FP32 form W itself
     Wb = (bf16(W) if contraction == "bf16" else W).astype(np.float64)
 
+    eng.timing(True)  # the contraction launches timed in place; results unchanged
     dsup = np.tile(dsup0, (R, 1))
     epsc = np.tile(epsc0, (R, 1))
     spikes = [np.tile(h, (R, 1)) for h in hist]
@@ -121,6 +122,8 @@ def test_synthetic_ticks(H, M, R, contraction):
         spikes.append(got_s)
     assert np.array_equal(eng.read("counts").astype(np.int64), counted)
     assert eng.launches() >= 6
+    ms, n = eng.contraction_time()
+    assert n == 6 and ms > 0
     # history rows written back are read back
     eng.write("spike_tm1", spikes[-1])
     assert np.array_equal(eng.read("spike_tm1"), spikes[-1])
