@@ -640,6 +640,10 @@ def run_multi_extension(dev, steps, warmup, ring=25, cpu=True):
     return out
 
 
+BATCH_PARITY = ("dsup_0", "act_0", "epsc_0", "bj_0", "spike_0", ".counter_0", "pj_0", "ej_0", "zj_0", "pi_0", "ei_0",
+                "zi_0", "ti_0")
+
+
 def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
     """The batching extension: 256 independent networks of uneven size (HCUs
     8-64, MCUs 5-50, full recurrent), 20 patterns each, advanced together by
@@ -689,7 +693,6 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
     h1.record(stream)
     eng.sync()
     t_head_batch = h0.elapsed_time(h1) * 1e-3
-    eng.close()
     plain = batch.Plain(members, device=dev)
     plain.run_segment(1, 2, 1.0, 0.0, 0, 0)  # warm-up: tables, graphs
     plain.sync()
@@ -704,6 +707,13 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
             net.sync()
     t_head_plain = time.perf_counter() - t0
     plain_cells = plain.counters() - pc0
+    # every member against the same network run alone on the plain path, after
+    # the same ticks: population and row-trace vectors by bit pattern
+    same = 0
+    for k, net in enumerate(plain.nets):
+        same += all(np.array_equal(np.asarray(eng.read(k, n)).view(np.uint8), np.asarray(net.read(n)).view(np.uint8))
+                    for n in BATCH_PARITY)
+    eng.close()
     plain.close()
     pk, pk_kind = peaks()
     # algorithmic bytes: 44 B per row cell and all-cells cell, 40 B per column
@@ -727,6 +737,8 @@ def run_batch_extension(dev, steps, n_nets=256, head_ticks=500, cpu=True):
                                          "cell_updates_per_s": plain_cells / t_head_plain, "ticks_timed": n_head},
         "batched_same_ticks": {"network_ticks_per_s": n_nets * n_head / t_head_batch},
         "speedup_vs_plain_same_ticks": t_head_plain / t_head_batch,
+        "parity_vs_plain": {"members_identical": f"{same}/{len(members)}", "ticks": n_head,
+                            "arrays": list(BATCH_PARITY)},
     }
     if cpu:
         try:
@@ -1105,6 +1117,7 @@ def extensions_summary(ext):
     b = ext.get("batched")
     if b:
         out["batched"] = {"network_ticks_per_s": b["value"], "speedup_vs_plain": b.get("speedup_vs_plain_same_ticks"),
+                          "members_identical_to_plain": b.get("parity_vs_plain", {}).get("members_identical"),
                           "frac_hbm": b.get("roofline", {}).get("frac"), "cell_updates_per_s": b.get("cell_updates_per_s")}
     m = ext.get("procupdmulti")
     if m:

@@ -671,8 +671,9 @@ __device__ __noinline__ void column_unit(const Dev& D, const Run& R, int4 u, int
 }
 
 /* kThreads 512: 16 warps per SM, 128 registers a thread (the column decays
-   then keep some values in local memory); 256: 8 warps per SM with room for
-   every value in registers.  The tuner times both. */
+   then keep some values in local memory); 384: 12 warps with 168 registers;
+   256: 8 warps per SM with room for every value in registers.  The tuner
+   times them all. */
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const Dev* __restrict__ dg, const Run* __restrict__ rg,
                                                            unsigned int* bar) {
@@ -1004,12 +1005,24 @@ int table_for(bcpnn_batch* b, float kp, float ke, float kzi, float kzj, int need
   return BCPNN_OK;
 }
 
+/* the batch kernel instance of a CTA size (256, 384 or 512 threads) */
+const void* kernel_for(int threads) {
+  switch (threads) {
+    case 256:
+      return (const void*)batch_kernel<256>;
+    case 384:
+      return (const void*)batch_kernel<384>;
+    default:
+      return (const void*)batch_kernel<512>;
+  }
+}
+
 /* longest-processing-time assignment of the items to the warps of the grid */
 int schedule_items(bcpnn_batch* b) {
   const int wpc = b->threads / 32;
   const size_t smem = (size_t)wpc * kWarpScratch * sizeof(float);
   int per_sm = 0;
-  const void* fn = b->threads == 256 ? (const void*)batch_kernel<256> : (const void*)batch_kernel<512>;
+  const void* fn = kernel_for(b->threads);
   BCU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, b->threads, smem));
   int sms = 0;
@@ -1079,7 +1092,7 @@ int bcpnn_batch_create(const bcpnn_batch_desc* desc, bcpnn_batch** out) {
   if (!out) return BCPNN_ERR_INVALID;
   *out = nullptr;
   if (!desc || desc->n_members <= 0 || !desc->members || !finite_pos(desc->dt) || desc->max_ticks_per_run <= 0 ||
-      (desc->threads != 0 && desc->threads != 256 && desc->threads != 512) ||
+      (desc->threads != 0 && desc->threads != 256 && desc->threads != 384 && desc->threads != 512) ||
       !(desc->poisson_noise_hz >= 0.0f && desc->poisson_noise_hz <= 3.4028234663852886e38f))
     return BCPNN_ERR_INVALID;
   for (int i = 0; i < desc->n_members; ++i) {
@@ -1365,7 +1378,7 @@ int bcpnn_batch_run(bcpnn_batch* b, int32_t first_simstep, int32_t n_ticks, floa
     b->all_cells += b->total_cells; /* Proj.cpp:538-588 visits every cell */
   }
   void* args[] = {(void*)&b->d_dev, (void*)&b->d_run, (void*)&b->bar};
-  const void* fn = b->threads == 256 ? (const void*)batch_kernel<256> : (const void*)batch_kernel<512>;
+  const void* fn = kernel_for(b->threads);
   BCU(cudaLaunchCooperativeKernel(fn, dim3(b->grid), dim3(b->threads), args, b->smem, b->stream));
   b->launches++;
   b->k_total += n_ticks;
@@ -1570,10 +1583,11 @@ int bcpnn_batch_tune(bcpnn_batch* b, int32_t probe_ticks, int32_t lgidx_train, i
   struct Cand {
     int threads, w0, w1, w2;
   };
-  /* launch shapes: CTA size (512: one CTA of 16 warps per SM; 256: 8-warp
-     CTAs) and the cost model of the warp schedule (per item: a fixed part,
-     per MCU, per 32 slots) */
+  /* launch shapes: CTA size (512, 384: one CTA of 16 or 12 warps per SM; 256:
+     8-warp CTAs) and the cost model of the warp schedule (per item: a fixed
+     part, per MCU, per 32 slots) */
   const Cand cands[] = {{512, 64, 4, 1}, {512, 16, 4, 4}, {512, 128, 2, 1}, {512, 32, 8, 2},
+                        {384, 64, 4, 1}, {384, 16, 4, 4}, {384, 128, 2, 1}, {384, 32, 8, 2},
                         {256, 64, 4, 1}, {256, 16, 4, 4}, {256, 128, 2, 1}, {256, 32, 8, 2}};
   const int old_threads = b->threads;
   int old_w[3] = {b->lpt[0], b->lpt[1], b->lpt[2]};

@@ -63,7 +63,7 @@ typedef struct bcpnn_batch_desc {
   float poisson_noise_hz;   /* project-defined input noise, as bcpnn_net_desc */
   int32_t device;
   int32_t max_ticks_per_run;
-  int32_t threads;          /* CTA size of the batch kernel: 256 or 512 (0: 512) */
+  int32_t threads;          /* CTA size of the batch kernel: 256, 384 or 512 (0: 512) */
   int32_t lpt_weights[3];   /* item cost model of the warp schedule: cost = w0 + w1*M + w2*C/32
                                ({0,0,0}: the default 64, 4, 1) */
 } bcpnn_batch_desc;
@@ -105,8 +105,8 @@ int bcpnn_batch_get_spike_log(bcpnn_batch* b, int32_t member, uint32_t* out, siz
 int bcpnn_batch_counters(bcpnn_batch* b, uint64_t out[3]);
 int bcpnn_batch_kernel_launches(const bcpnn_batch* b, uint64_t* out);
 
-/* The schedule tuner: times candidate launch shapes -- CTA size 256 or 512
-   and item cost models of the warp schedule -- on probe_ticks training ticks
+/* The schedule tuner: times candidate launch shapes -- CTA size 256, 384 or
+   512 and item cost models of the warp schedule -- on probe_ticks training ticks
    followed by probe_ticks recall ticks (the catch-up at the switch included),
    from the current state, restoring nothing (call it on a fresh or reset
    batch; reset afterwards).  The fastest becomes the batch's shape;
