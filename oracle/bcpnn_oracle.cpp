@@ -979,5 +979,7 @@ float oracle_logf(int math, float x) { return Fn<float>::log(math, x); }
 /* 1 when this build carries gsbn's own kernels (math mode MATH_REF). */
 int oracle_has_ref(void) { return kHaveRef ? 1 : 0; }
 double oracle_log_double(int math, double x) { return log_double(math, x); }
+/* cos(2 pi u) of the Box-Muller draws (the library's bx_cos2pi_d) */
+double oracle_cos2pi_double(double u) { return bx_cos2pi_d(u); }
 
 }  // extern "C"

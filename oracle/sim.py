@@ -26,6 +26,7 @@ The restatement is pinned against MATH_REF, on the reference's fixtures and on
 the published Philox known-answer vectors.
 """
 import ctypes
+import math
 import os
 import subprocess
 
@@ -99,6 +100,8 @@ def _bind(lib):
     lib.oracle_logf.argtypes = [i32, fl]
     lib.oracle_log_double.restype = ctypes.c_double
     lib.oracle_log_double.argtypes = [i32, ctypes.c_double]
+    lib.oracle_cos2pi_double.restype = ctypes.c_double
+    lib.oracle_cos2pi_double.argtypes = [ctypes.c_double]
     lib.oracle_expf_array.argtypes = [i32, ctypes.c_longlong, vp, vp]
     lib.oracle_logf_array.argtypes = [i32, ctypes.c_longlong, vp, vp]
     lib.oracle_philox.argtypes = [vp, vp, vp]
@@ -285,6 +288,11 @@ def dim_conn(pops, q):
     """Proj.cpp:22-26."""
     c = pops[q["src_pop"]]["hcu_num"] * pops[q["src_pop"]]["mcu_num"]
     return min(c, int(q["slot_num"]))
+
+
+def log_double(x):
+    """the library's double log (bx_log_d), as the oracle computes it"""
+    return load().oracle_log_double(MATH_SHARED, x)
 
 
 def proc_args(sp, name):
@@ -561,7 +569,12 @@ class SpkRec:
 # random_device draws replaced by the seeded Philox stream the product uses:
 # draw i = philox((i, i >> 32, 0x53505241, 0), (seed, 0x5350))[0], uniform
 # (x >> 8) * 2^-24; Fisher-Yates from the back with j = floor(u * (i + 1)).
-# enable-geometry (random delays) is not restated here.
+# enable-geometry: a grown row's delay is ceil(tij * 0.001 / dt) ticks with
+# tij ~ normal(mean, 0.1 mean), mean = d_norm * distance / v_cond + 1 in float
+# over the HCUs' grid coordinates (delay_cycle, ProcStructuralPlasitcity.cpp:
+# 597-627; Pop::hcu_coor, ProcStructuralPlasticity/Pop.cpp:64-88); gsbn's
+# normal draw is restated as Box-Muller in double from two uniforms of the
+# stream, z = sqrt(-2 log(1 - u1)) cos(2 pi u2).
 # ---------------------------------------------------------------------------
 
 class StructuralPlasticity:
@@ -572,8 +585,14 @@ class StructuralPlasticity:
         self.period = argi.get("period", 100) if argi.get("period", 100) > 0 else 100
         pp = argi.get("pruning-period", 1000)
         self.pruning_period = pp if pp > 0 else 1000
-        if argi.get("enable-geometry", 0):
-            raise NotImplementedError("enable-geometry is not restated in the oracle")
+        self.geometry = argi.get("enable-geometry", 0) != 0
+        self.d_norm = f32(argf.get("d-norm", 0.75))
+        if "d-norm" in argf and self.d_norm < 0:
+            self.d_norm = f32(0)
+        self.v_cond = f32(argf.get("v-cond", 0.2))
+        if "v-cond" in argf and self.v_cond <= 0:
+            self.v_cond = f32(1)
+        self.geo = [(list(pp.shape), list(pp.position)) for pp in sp.net_param.pop_param for _ in range(pp.pop_num)]
         self.wp, self.wn = f32(argf.get("wp", 0.5)), f32(argf.get("wn", -0.5))
         self.seed = argi.get("seed", 0) & 0xFFFFFFFF
         self.draws = 0
@@ -588,6 +607,41 @@ class StructuralPlasticity:
         self.draws += 1
         x = philox([i & 0xFFFFFFFF, (i >> 32) & 0xFFFFFFFF, 0x53505241, 0], [self.seed, 0x5350])[0]
         return f32(int(x) >> 8) * f32(2.0 ** -24)
+
+    def hcu_coor(self, pop, hcu):
+        """Pop::hcu_coor (ProcStructuralPlasticity/Pop.cpp:64-88)"""
+        shape, position = self.geo[pop]
+        coor, index = [], hcu
+        for d in shape:
+            if d <= 0:
+                raise ValueError("population shape entries must be > 0")
+            coor.append(index % d)
+            index //= d
+        for i, p in enumerate(position):
+            if i < len(coor):
+                coor[i] += p
+            else:
+                coor.append(p)
+        return coor
+
+    def delay_cycle(self, k, src_mcu, dest_hcu):
+        """ProcStructuralPlasticity::delay_cycle (ProcStructuralPlasitcity.cpp:597-627)"""
+        q = self.projs[k]
+        a = self.hcu_coor(q["src_pop"], src_mcu // self.pops[q["src_pop"]]["mcu_num"])
+        b = self.hcu_coor(q["dest_pop"], dest_hcu)
+        n = max(len(a), len(b))
+        a, b = a + [0] * (n - len(a)), b + [0] * (n - len(b))
+        d2 = f32(0)
+        for x, y in zip(a, b):
+            d2 = f32(d2 + f32((x - y) * (x - y)))
+        distance = f32(math.sqrt(float(d2)))
+        mean = f32(f32(f32(self.d_norm * distance) / self.v_cond) + f32(1))
+        u1 = 1.0 - float(self.uniform())
+        u2 = float(self.uniform())
+        z = math.sqrt(-2.0 * log_double(u1)) * load().oracle_cos2pi_double(u2)
+        m = float(mean)
+        tij = f32(m + 0.1 * m * z)
+        return int(math.ceil(float(tij) * 0.001 / float(self.dt)))
 
     def shuffle(self, a):
         for i in range(len(a) - 1, 0, -1):
@@ -689,7 +743,7 @@ class StructuralPlasticity:
                     free = np.nonzero(ii[h * C:(h + 1) * C] < 0)[0]
                     f = h * C + int(free[0])
                     ii[f] = local[k][idx]
-                    di[f] = 1
+                    di[f] = self.delay_cycle(k, int(local[k][idx]), h) if self.geometry else 1
             self.net.write(f"ii_{k}", ii)
             self.net.write(f"di_{k}", di)
 

@@ -234,15 +234,24 @@ def test_gsbn_sim_command(tmp_path):
     assert bad.returncode == 1 and "no CPU path" in bad.stderr
 
 
-def test_structural_plasticity_matches_oracle(tmp_path):
+@pytest.mark.parametrize("geometry", [False, True])
+def test_structural_plasticity_matches_oracle(tmp_path, geometry):
     """ProcStructuralPlasticity (device pruning + host growth, seeded stream)
     against the oracle's restatement: same records, same final connectivity
-    and traces."""
+    and traces.  With enable-geometry the grown rows get delays drawn from the
+    HCUs' grid distance (the population laid out as a 5 x 2 grid at offset
+    (1, 0, 3))."""
     def edit(text):
         text = text.replace("prn: 1.0\n    plasticity: 0", "prn: 1.0\n    plasticity: 1")
+        geo = ('  argi { key: "enable-geometry" val: 1 }\n  argf { key: "d-norm" val: 0.9 }\n'
+               '  argf { key: "v-cond" val: 0.25 }\n') if geometry else ""
         sp_block = ('proc_param {\n  name: "ProcStructuralPlasticity"\n  argi { key: "period" val: 50 }\n'
                     '  argi { key: "pruning-period" val: 100 }\n  argi { key: "t-th" val: 60 }\n'
-                    '  argi { key: "seed" val: 7 }\n  argf { key: "wp" val: 1.5 }\n  argf { key: "wn" val: -1.5 }\n}\n')
+                    '  argi { key: "seed" val: 7 }\n  argf { key: "wp" val: 1.5 }\n  argf { key: "wn" val: -1.5 }\n'
+                    + geo + '}\n')
+        if geometry:
+            text = text.replace("    snoise: 0\n  }", "    snoise: 0\n    shape: 5\n    shape: 2\n    position: 1\n"
+                                "    position: 0\n    position: 3\n  }", 1)
         return text.replace('proc_param {\n  name: "ProcSpkRec"', sp_block + 'proc_param {\n  name: "ProcSpkRec"')
 
     path, sp = write(workloads.config0(), tmp_path, edit)
@@ -261,3 +270,6 @@ def test_structural_plasticity_matches_oracle(tmp_path):
         assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), n
     # pruning and regrowth both happened
     assert (got["ii_0"] < 0).any() or (got["ii_0"] != np.tile(np.arange(100), 10)).any()
+    if geometry:
+        assert "shape: 5" in open(path).read()
+        assert (got["di_0"] > 1).any(), "grown rows carry geometric delays"
