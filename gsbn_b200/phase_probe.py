@@ -38,6 +38,8 @@ def main():
     ap.add_argument("--recall", type=int, default=20)
     ap.add_argument("--mhz", type=float, default=1965.0)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--critical", type=int, default=0,
+                    help="also print the N CTAs with the least barrier wait (the ones that arrive last most often)")
     a = ap.parse_args()
     if "probe" not in capi.LIB_PATH:
         sys.exit("set GSBN_B200_LIB to the phase-probe build (gsbn_b200/libgsbn_b200_probe.so)")
@@ -82,6 +84,13 @@ def main():
         print(f"  A {'total (median)':<24} {tot:7.3f}")
         for k, ph in PHASES_B.items():
             print(f"  B {ph:<24} {float(np.median(pt[:, k])):7.3f} {float(pt[:, k].max()):7.3f}")
+        if a.critical:
+            order = np.argsort(pt[:, 0])[:a.critical]
+            keys = list(PHASES_A)
+            print(f"  CTAs with the least A barrier wait (HCU: {', '.join(PHASES_A[k] for k in keys)}):")
+            for c in order:
+                print(f"    {int(c):4d}: " + " ".join(f"{pt[c, k]:.2f}" for k in keys))
+            print(f"  A barrier wait min {float(pt[:, 0].min()):.3f}, B barrier wait min {float(pt[:, 16].min()):.3f}")
         slow, fast = float(counts[name][:, 14].sum()), float(counts[name][:, 15].sum())
         print(f"  decays: {fast:.0f} by the reciprocal form, {slow:.0f} by the div_rn fallback "
               f"({100.0 * slow / max(1.0, slow + fast):.3f} %)")
