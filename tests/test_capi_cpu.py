@@ -41,6 +41,14 @@ def test_recall_rejects_bad_shapes_before_the_device():
         with pytest.raises(capi.BcpnnError) as e:
             recall.Recall(H, M, R, dict(pop, hcu_num=H, mcu_num=M), 0.001, 0.1)
         assert e.value.status == -1
+    # a contraction form other than BF16 (0) or FP32 (1)
+    recall.CONTRACTIONS["unknown"] = 7
+    try:
+        with pytest.raises(capi.BcpnnError) as e:
+            recall.Recall(8, 32, 128, pop, 0.001, 0.1, contraction="unknown")
+        assert e.value.status == -1
+    finally:
+        del recall.CONTRACTIONS["unknown"]
 
 
 def test_status_strings():
@@ -147,4 +155,9 @@ def test_batch_rejects_bad_members_before_the_device():
         m.__dict__.update(edit)
         with pytest.raises(capi.BcpnnError) as e:
             batch.BatchEngine([m], max_ticks=8)
+        assert e.value.status == -1
+    # CTA sizes other than 256, 384 and 512 threads
+    for threads in (128, 300, 448, 1024):
+        with pytest.raises(capi.BcpnnError) as e:
+            batch.BatchEngine([good], max_ticks=8, threads=threads)
         assert e.value.status == -1
