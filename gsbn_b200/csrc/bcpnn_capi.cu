@@ -631,8 +631,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   if ((rc = dalloc(net, &errw, 1))) return bail(rc);
   H.err = errw;
   unsigned long long* seeds = nullptr;
-  if ((rc = dalloc(net, &seeds, (size_t)desc->n_pops))) return bail(rc);
-  if (cudaMemsetAsync(seeds, 0, (size_t)desc->n_pops * sizeof(unsigned long long), net->stream) != cudaSuccess) {
+  if ((rc = dalloc(net, &seeds, 2 * (size_t)desc->n_pops))) return bail(rc);
+  if (cudaMemsetAsync(seeds, 0, 2 * (size_t)desc->n_pops * sizeof(unsigned long long), net->stream) != cudaSuccess) {
     net->err = "memset failed";
     return bail(BCPNN_ERR_CUDA);
   }

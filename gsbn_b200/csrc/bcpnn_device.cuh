@@ -133,11 +133,15 @@ struct NetDev {
      MCU | rows << 16).  Two ring halves by tick parity, col_cap units each. */
   int4* col_ring;
   int col_cap;
-  /* [n_pops] the softmax seed of the next tick (dsup of the population's MCU
-     0, Pop.cpp:270), published by the population's HCU-0 CTA at the end of a
-     tick of the persistent launch: (tick tag << 32) | float bits.  The other
-     CTAs' barrier threads load it while they poll, so it costs no round trip
-     after the barrier; the tag (RunParams::serial0 + tick) certifies it. */
+  /* [n_pops][2] the softmax seed of the next tick (dsup of the population's
+     MCU 0, Pop.cpp:270), published by the population's HCU-0 CTA at the end
+     of a tick of the persistent launch, before its barrier arrival: (tick
+     tag << 32) | float bits, in slot [tag & 1].  The other CTAs' barrier
+     threads load it while they poll, so it costs no round trip after the
+     barrier; the tag (RunParams::serial0 + tick) certifies it.  Two slots:
+     the publisher can be a tick ahead of a reader that has not yet seen the
+     barrier complete (it publishes tick t+1's seed before every CTA has read
+     tick t's), never two. */
   unsigned long long* seed64;
 };
 

@@ -717,7 +717,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
     if (it > it0) {
       /* this CTA arrived at the end of the previous tick (grid_arrive) */
       if (!grid_wait(bar, (unsigned int)(it - it0) * gridDim.x, net->err, &s_ok,
-                     (defer && h != 0) ? net->seed64 + P : nullptr, rp->serial0 + (unsigned int)(it - it0),
+                     (defer && h != 0) ? net->seed64 + 2 * P + ((rp->serial0 + (unsigned int)(it - it0)) & 1u) : nullptr,
+                     rp->serial0 + (unsigned int)(it - it0),
                      &s_dsup0))
         return;
     } else {
@@ -1088,8 +1089,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         sup += (pop.wgain * s_wm) * wsup;
         const float d = st_dsup[0];
         const float next = d + (sup - d) * pop.taumdt;
-        store_relaxed_u64(net->seed64 + P, ((unsigned long long)(rp->serial0 + (unsigned int)(it + 1 - it0)) << 32) |
-                                               __float_as_uint(next));
+        const unsigned int tag = rp->serial0 + (unsigned int)(it + 1 - it0);
+        store_relaxed_u64(net->seed64 + 2 * P + (tag & 1u), ((unsigned long long)tag << 32) | __float_as_uint(next));
       }
       /* rows done: group B may now update column cells of active rows */
       if (!defer) asm volatile("bar.arrive %0, %1;" ::"r"(kBarRows), "r"(kBlock) : "memory");
