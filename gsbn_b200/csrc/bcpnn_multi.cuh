@@ -164,12 +164,45 @@ __global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __re
   pop_hcu(net, rp, it, net->cta_pop[blockIdx.x], net->cta_hcu[blockIdx.x], sm, &s_vsum);
 }
 
+/* One closed-form decay of a cell over pdt ticks.  With the run's TabRef of
+   this kp (T non-null: the tick path, whose kp the TabRef's coefficients
+   and reciprocal table were made for) the divisions are multiplications by
+   the tabulated double reciprocals with the exact fallback (cell_step_nl,
+   bit-identical to cell_decay); without it (the catch-up at a change of prn,
+   with the old kp) cell_decay itself. */
+__device__ __forceinline__ void decay_cell(float& pij, float& eij, float& zi2, float& zj2, const Coef& k,
+                                           const float4* tab, int tlen, const TabRef* T, int pdt) {
+  float4 A, Bv;
+  if (T) {
+    double2 R0, R1;
+    if (pdt < tlen) {
+      A = tab[(size_t)pdt * 4];
+      Bv = tab[(size_t)pdt * 4 + 1];
+      R0 = T->rtab[(size_t)pdt * 4];
+      R1 = T->rtab[(size_t)pdt * 4 + 1];
+    } else {
+      table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 0, A, Bv, k.fp64);
+      recip_part(A, Bv, 0, R0, R1);
+    }
+    const float4 c = cell_step_nl(make_float4(pij, eij, zi2, zj2), T, A, Bv, R0, R1);
+    pij = c.x;
+    eij = c.y;
+    zi2 = c.z;
+    zj2 = c.w;
+    return;
+  }
+  entry(tab, tlen, k, pdt, 0, A, Bv);
+  cell_decay(pij, eij, zi2, zj2, k, A, Bv);
+}
+
 /* One cell of an active row (update_row_kernel_cpu, Proj.cpp:409-488, after
    the row traces): replay of the postsynaptic spikes in the ring, decay to
-   simstep, kftj for a spike now.  tij/zi2 start from the row's ti/zi. */
+   simstep, kftj for a spike now.  tij/zi2 start from the row's ti/zi.  T as
+   for decay_cell. */
 __device__ __forceinline__ void replay_cell(float4& c4, int tij, float zi2, int simstep, int last_exclusive,
                                             const int8_t* __restrict__ ring, int B, int n, int mcu, const Coef& k,
-                                            const float4* tab, int tlen, float kftj, bool final_decay_always) {
+                                            const float4* tab, int tlen, const TabRef* T, float kftj,
+                                            bool final_decay_always) {
   float pij = c4.x, eij = c4.y, zj2 = c4.w;
   int now = tij;
   if (simstep - now >= B) now = simstep - B + 1;
@@ -178,9 +211,7 @@ __device__ __forceinline__ void replay_cell(float4& c4, int tij, float zi2, int 
     if ((!last_exclusive || now < simstep) && ring[(size_t)(now % B) * n + mcu] > 0) {
       const int pdt = now - tij;
       if (pdt > 0) {
-        float4 A, Bv;
-        entry(tab, tlen, k, pdt, 0, A, Bv);
-        cell_decay(pij, eij, zi2, zj2, k, A, Bv);
+        decay_cell(pij, eij, zi2, zj2, k, tab, tlen, T, pdt);
         zj2 = zj2 + kftj;
         tij = now;
       }
@@ -188,10 +219,8 @@ __device__ __forceinline__ void replay_cell(float4& c4, int tij, float zi2, int 
   }
   const int pdt = simstep - tij;
   if (final_decay_always || pdt > 0) {
-    float4 A, Bv;
-    entry(tab, tlen, k, pdt, 0, A, Bv);
     float zi2_unused = zi2;
-    cell_decay(pij, eij, zi2_unused, zj2, k, A, Bv);
+    decay_cell(pij, eij, zi2_unused, zj2, k, tab, tlen, T, pdt);
   }
   c4 = make_float4(pij, eij, zi2, zj2);
 }
@@ -216,6 +245,7 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
   const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
   const float4* tab = rp->tabs[p].tab;
   const int tlen = rp->tabs[p].len;
+  const TabRef* T = &rp->tabs[p]; /* coefficients and reciprocals of this kp */
   const size_t eoff = (size_t)J.proj_in_pop * n;
   const int8_t* sj = pop.ring + (size_t)(simstep % B) * n;
   const int rch = row_chunk(M);
@@ -267,8 +297,21 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
       if (pdt > 0) {
         float ei = J.ei[r], zi = s_zi[t];
         float4 A, Bv;
-        entry(tab, tlen, k, pdt, 2, A, Bv);
-        row_decay(pi, ei, zi, k, A, Bv); /* zi becomes zi*exp(-kzi*pdt) */
+        double2 R0, R1;
+        if (pdt < tlen) {
+          A = tab[(size_t)pdt * 4 + 2];
+          Bv = tab[(size_t)pdt * 4 + 3];
+          R0 = T->rtab[(size_t)pdt * 4 + 2];
+          R1 = T->rtab[(size_t)pdt * 4 + 3];
+        } else {
+          table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
+          recip_part(A, Bv, 2, R0, R1);
+        }
+        /* zi becomes zi*exp(-kzi*pdt) */
+        const float4 rv = row_step_nl(make_float4(pi, ei, zi, 0.0f), T, A, Bv, R0, R1);
+        pi = rv.x;
+        ei = rv.y;
+        zi = rv.z;
         J.pi[r] = pi;
         J.ei[r] = ei;
         J.zi[r] = zi + J.kfti;
@@ -280,7 +323,7 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
       const int rr = c / M, j = c - rr * M;
       const size_t index = (size_t)s_list[base + rr] * M + j;
       float4 c4 = J.cell[index];
-      replay_cell(c4, s_ti[rr], s_zi[rr], simstep, 1, pop.ring, B, n, h * M + j, k, tab, tlen, J.kftj, true);
+      replay_cell(c4, s_ti[rr], s_zi[rr], simstep, 1, pop.ring, B, n, h * M + j, k, tab, tlen, T, J.kftj, true);
       if (sj[h * M + j] > 0) c4.w += J.kftj;
       J.cell[index] = c4;
       s_w[c] = c4.x;
@@ -411,7 +454,7 @@ __global__ void all_kernel(const NetDev* __restrict__ net, const RunParams* __re
     for (int j = lane; j < M; j += 32) {
       const size_t index = (size_t)r * M + j;
       float4 c4 = J.cell[index];
-      replay_cell(c4, ti, zi, simstep, 0, pop.ring, B, n, h * M + j, k, tab, tlen, J.kftj, false);
+      replay_cell(c4, ti, zi, simstep, 0, pop.ring, B, n, h * M + j, k, tab, tlen, nullptr, J.kftj, false);
       J.cell[index] = c4;
       if (kp != 0.0f)
         J.wij[index] = J.wgain * bx_logf((c4.x + J.eps2) / ((pi_new + J.eps) * (J.pj[h * M + j] + J.eps)));
