@@ -1233,22 +1233,33 @@ int bcpnn_get_spike_log_async(bcpnn_net* net, int32_t pop, uint32_t* out, size_t
   return BCPNN_OK;
 }
 
-/* ProcCheck/Pop.cpp:36-44: count the spikes of ticks k0..k1-1 of a spike log */
+/* ProcCheck/Pop.cpp:36-44: count the spikes of ticks k0..k1-1 of a spike
+   log.  Thread (i, s) counts MCU i over the ticks k0 + s, k0 + s + S, ...
+   (S = gridDim.y slices, so that a whole window's loads are spread over the
+   GPU) and adds its count to counts[i]; integer sums, so the order does not
+   matter. */
 __global__ void check_count_kernel(const uint32_t* __restrict__ log, int words, int k0, int k1, int n,
                                    int32_t* __restrict__ counts) {
+  const int S = gridDim.y, s = blockIdx.y;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int c = 0;
-    for (int t = k0; t < k1; ++t) c += (int)((log[(size_t)t * words + (i >> 5)] >> (i & 31)) & 1u);
-    counts[i] += c;
+    for (int t = k0 + s; t < k1; t += S) c += (int)((__ldcg(log + (size_t)t * words + (i >> 5)) >> (i & 31)) & 1u);
+    if (c) atomicAdd(counts + i, c);
   }
 }
 
 /* ProcCheck/Pop.cpp:46-60: per HCU the first MCU with the largest count (-1
-   when none counted) and that count; counters cleared */
+   when none counted) and that count; counters cleared.  One warp per HCU:
+   each lane keeps the first of its MCUs with its largest positive count,
+   then the warp keeps the largest count and, among equal counts, the
+   smallest MCU index -- the MCU gsbn's scan in index order with a strict >
+   picks. */
 __global__ void check_result_kernel(int32_t* __restrict__ counts, int H, int M, int32_t* __restrict__ out) {
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int h = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); h < H; h += nw) {
     int best = -1, most = 0;
-    for (int j = 0; j < M; ++j) {
+    for (int j = lane; j < M; j += 32) {
       const int c = counts[(size_t)h * M + j];
       if (c > most) {
         best = j;
@@ -1256,8 +1267,18 @@ __global__ void check_result_kernel(int32_t* __restrict__ counts, int H, int M, 
       }
       counts[(size_t)h * M + j] = 0;
     }
-    out[h] = best;
-    out[H + h] = most;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int ob = __shfl_xor_sync(0xffffffffu, best, o), om = __shfl_xor_sync(0xffffffffu, most, o);
+      if (om > most || (om == most && om > 0 && ob < best)) {
+        best = ob;
+        most = om;
+      }
+    }
+    if (lane == 0) {
+      out[h] = best;
+      out[H + h] = most;
+    }
   }
 }
 
@@ -1287,8 +1308,9 @@ int bcpnn_check_count(bcpnn_net* net, int32_t pop, int32_t k0, int32_t k1) {
   if (k1 == k0) return BCPNN_OK;
   const PopHost& P = net->pops[pop];
   const int n = P.H * P.M;
-  check_count_kernel<<<(n + 255) / 256, 256, 0, net->stream>>>(net->log_buf + P.log_offset, P.log_words, k0, k1, n,
-                                                               net->check_cnt[pop]);
+  const int slices = (k1 - k0) < 16 ? (k1 - k0) : 16;
+  check_count_kernel<<<dim3((n + 255) / 256, slices), 256, 0, net->stream>>>(net->log_buf + P.log_offset, P.log_words,
+                                                                            k0, k1, n, net->check_cnt[pop]);
   CU(cudaGetLastError());
   net->launches += 1;
   return BCPNN_OK;
@@ -1303,7 +1325,7 @@ int bcpnn_check_result_async(bcpnn_net* net, int32_t pop, int32_t* idx, int32_t*
   CU(cudaSetDevice(net->device));
   int rc = check_buffers(net, pop);
   if (rc) return rc;
-  check_result_kernel<<<(P.H + 127) / 128, 128, 0, net->stream>>>(net->check_cnt[pop], P.H, P.M, net->check_out[pop]);
+  check_result_kernel<<<(P.H + 7) / 8, 256, 0, net->stream>>>(net->check_cnt[pop], P.H, P.M, net->check_out[pop]);
   CU(cudaGetLastError());
   net->launches += 1;
   CU(cudaMemcpyAsync(idx, net->check_out[pop], n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost, net->stream));
