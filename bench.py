@@ -268,11 +268,17 @@ def run_ours(args, rank, world, local_rank, cpu=False):
     net.sync()
     e0 = sum(net.counters())
     barrier()
-    t0 = time.perf_counter()
+    # timed on the device (CUDA events on the library stream), like the rest;
+    # each step ends with the host's synchronisation, so the gaps where the
+    # device waits for the host's next calls are inside the interval
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
     for _ in range(args.steps):
         recall = e2e_step()
+    ev1.record(stream)
     net.sync()
-    e_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    e_s = ev0.elapsed_time(ev1) * 1e-3
     e_cells = sum(net.counters()) - e0
     e_s, e_cells = combine_over_ranks(e_s, e_cells, f"cuda:{dev}")
     # every e2e step is the same pass from the initial state: its spike logs
