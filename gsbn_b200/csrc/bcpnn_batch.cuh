@@ -602,6 +602,7 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
    rows already has tij = simstep (rows ran in phase A), so it only gains
    kftj.  w == 1: the fan-out of source MCU y, whose spike of this tick turns
    each slot it feeds active at kk + 2 + delay (the delay queue, as events). */
+template <int kV>
 __device__ __noinline__ void column_unit(const Dev& D, const Run& R, int4 u, int simstep, int kk) {
   const Member& B = D.m[u.x];
   const int lane = threadIdx.x & 31;
@@ -619,54 +620,58 @@ __device__ __noinline__ void column_unit(const Dev& D, const Run& R, int4 u, int
   const TabRef* T = &R.tabs[u.x];
   const int row0 = u.y, j = u.z & 0xffff, rows = u.z >> 16, M = B.M;
   const int tlen = T->len;
-  size_t index[kUnit / 32];
-  int tv[kUnit / 32];
-  float4 cv[kUnit / 32];
-  bool ok[kUnit / 32];
+  /* kV of the lane's kUnit/32 cells at a time: their loads issued together */
+#pragma unroll 1
+  for (int v0 = 0; v0 < kUnit / 32; v0 += kV) {
+    size_t index[kV];
+    int tv[kV];
+    float4 cv[kV];
+    bool ok[kV];
 #pragma unroll
-  for (int v = 0; v < kUnit / 32; ++v) {
-    const int s = v * 32 + lane;
-    ok[v] = false;
-    if (s < rows) {
-      const int row = row0 + s;
-      index[v] = (size_t)row * M + j;
-      ok[v] = B.ii[row] >= 0;
-      /* the owner's rows of this tick (phase A, another SM) wrote these */
-      tv[v] = __ldcg(B.tij + index[v]);
-      cv[v] = __ldcg(B.cell + index[v]);
-    }
-  }
-  float4 tA[kUnit / 32], tB[kUnit / 32];
-  double2 tR0[kUnit / 32], tR1[kUnit / 32];
-#pragma unroll
-  for (int v = 0; v < kUnit / 32; ++v) {
-    const int pdt = simstep - tv[v];
-    if (ok[v] && pdt > 0 && pdt < tlen) {
-      tA[v] = T->tab[(size_t)pdt * 4 + 0];
-      tB[v] = T->tab[(size_t)pdt * 4 + 1];
-      tR0[v] = T->rtab[(size_t)pdt * 4 + 0];
-      tR1[v] = T->rtab[(size_t)pdt * 4 + 1];
-    }
-  }
-#pragma unroll
-  for (int v = 0; v < kUnit / 32; ++v) {
-    if (!ok[v]) continue;
-    const int pdt = simstep - tv[v];
-    float4 q = cv[v];
-    if (pdt <= 0) {
-      q.w += B.kftj;
-    } else {
-      float4 A = tA[v], Bt = tB[v];
-      double2 R0 = tR0[v], R1 = tR1[v];
-      if (pdt >= tlen) {
-        load_entry(T->tab, tlen, T->k, pdt, 0, A, Bt);
-        recip_part(A, Bt, 0, R0, R1);
+    for (int v = 0; v < kV; ++v) {
+      const int s = (v0 + v) * 32 + lane;
+      ok[v] = false;
+      if (s < rows) {
+        const int row = row0 + s;
+        index[v] = (size_t)row * M + j;
+        ok[v] = B.ii[row] >= 0;
+        /* the owner's rows of this tick (phase A, another SM) wrote these */
+        tv[v] = __ldcg(B.tij + index[v]);
+        cv[v] = __ldcg(B.cell + index[v]);
       }
-      q = cell_step_in(q, T, A, Bt, R0, R1);
-      q.w = q.w + B.kftj;
     }
-    B.cell[index[v]] = q;
-    B.tij[index[v]] = simstep;
+    float4 tA[kV], tB[kV];
+    double2 tR0[kV], tR1[kV];
+#pragma unroll
+    for (int v = 0; v < kV; ++v) {
+      const int pdt = simstep - tv[v];
+      if (ok[v] && pdt > 0 && pdt < tlen) {
+        tA[v] = T->tab[(size_t)pdt * 4 + 0];
+        tB[v] = T->tab[(size_t)pdt * 4 + 1];
+        tR0[v] = T->rtab[(size_t)pdt * 4 + 0];
+        tR1[v] = T->rtab[(size_t)pdt * 4 + 1];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < kV; ++v) {
+      if (!ok[v]) continue;
+      const int pdt = simstep - tv[v];
+      float4 q = cv[v];
+      if (pdt <= 0) {
+        q.w += B.kftj;
+      } else {
+        float4 A = tA[v], Bt = tB[v];
+        double2 R0 = tR0[v], R1 = tR1[v];
+        if (pdt >= tlen) {
+          load_entry(T->tab, tlen, T->k, pdt, 0, A, Bt);
+          recip_part(A, Bt, 0, R0, R1);
+        }
+        q = cell_step_in(q, T, A, Bt, R0, R1);
+        q.w = q.w + B.kftj;
+      }
+      B.cell[index[v]] = q;
+      B.tij[index[v]] = simstep;
+    }
   }
 }
 
@@ -734,7 +739,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const Dev* __restric
     /* a counter past the ring's capacity (reported in phase A) is clamped */
     const unsigned int nu = min(__ldcg(D.unit_cnt + (kk & 1)), (unsigned int)D.unit_cap);
     const int4* units = D.units + (size_t)(kk & 1) * D.unit_cap;
-    for (unsigned int u = gwarp; u < nu; u += nw) column_unit(D, R, __ldcg(units + u), simstep, kk);
+    for (unsigned int u = gwarp; u < nu; u += nw)
+      column_unit<(kThreads >= 384) ? 1 : kUnit / 32>(D, R, __ldcg(units + u), simstep, kk);
 #ifdef BCPNN_PHASE_PROBE
     if (lane == 0) {
       const unsigned long long d = (unsigned long long)(clock64() - pt2);
