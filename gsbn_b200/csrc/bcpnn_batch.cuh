@@ -187,32 +187,36 @@ __device__ __forceinline__ float warp_max(float v) {
    simstep: row traces, cells, weights, ordered epsc sum into e[2] (MCUs lane,
    lane + 32).  kp as the tick's prn gives it.  The loads of the row traces
    and of the first cells go out together, then their table entries. */
+template <int kCP>
 __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict__ T, int h, const int* ros, int nr,
                                        int simstep, float kp, float* ws_pi, const float* ws_pj, float* ws_w,
                                        int8_t* ws_skip, float e[2], int lane) {
+  static_assert(kCP == 1 || kCP == kCPL, "one or kCPL cells per lane and pass");
   const int M = B.M, C = B.C;
   const Coef& k = T->k;
   const int tlen = T->len;
   const int ncell = nr * M;
-  /* row traces, Proj.cpp:397-416 (one lane per row; at most kListCap rows) */
-  {
-    int ti[2], row[2];
-    float4 tr[2];
+  /* row traces, Proj.cpp:397-416 (one lane per row; at most kListCap rows),
+     kCP rows of a lane at a time */
+#pragma unroll 1
+  for (int v0 = 0; v0 < 2; v0 += kCP) {
+    int ti[kCP], row[kCP];
+    float4 tr[kCP];
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const int r = lane + 32 * v;
+    for (int v = 0; v < kCP; ++v) {
+      const int r = lane + 32 * (v0 + v);
       if (r < nr) {
         row[v] = h * C + ros[r];
         ti[v] = B.ti[row[v]];
         tr[v] = make_float4(B.pi[row[v]], B.ei[row[v]], B.zi[row[v]], 0.0f);
       }
     }
-    float4 A[2], Bt[2];
-    double2 R0[2], R1[2];
+    float4 A[kCP], Bt[kCP];
+    double2 R0[kCP], R1[kCP];
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
+    for (int v = 0; v < kCP; ++v) {
       const int pdt = simstep - ti[v];
-      if (lane + 32 * v < nr && pdt > 0 && pdt < tlen) {
+      if (lane + 32 * (v0 + v) < nr && pdt > 0 && pdt < tlen) {
         A[v] = T->tab[(size_t)pdt * 4 + 2];
         Bt[v] = T->tab[(size_t)pdt * 4 + 3];
         R0[v] = T->rtab[(size_t)pdt * 4 + 2];
@@ -220,8 +224,8 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
       }
     }
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const int r = lane + 32 * v;
+    for (int v = 0; v < kCP; ++v) {
+      const int r = lane + 32 * (v0 + v);
       if (r >= nr) continue;
       const int pdt = simstep - ti[v];
       if (pdt <= 0) {
@@ -243,15 +247,16 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
     }
   }
   __syncwarp();
-  /* cells, Proj.cpp:418-478, kCellsPerPass at a time, kCPL per lane */
-  for (int b0 = 0; b0 < ncell; b0 += kCellsPerPass) {
-    int tv[kCPL];
-    float4 cv[kCPL];
-    float wv[kCPL];
-    size_t index[kCPL];
-    bool ok[kCPL];
+  /* cells, Proj.cpp:418-478, 32*kCP at a time, kCP per lane */
+  constexpr int kPass = 32 * kCP;
+  for (int b0 = 0; b0 < ncell; b0 += kPass) {
+    int tv[kCP];
+    float4 cv[kCP];
+    float wv[kCP];
+    size_t index[kCP];
+    bool ok[kCP];
 #pragma unroll
-    for (int u = 0; u < kCPL; ++u) {
+    for (int u = 0; u < kCP; ++u) {
       const int c = b0 + u * 32 + lane;
       ok[u] = c < ncell;
       if (ok[u]) {
@@ -263,10 +268,10 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
         wv[u] = B.wij[index[u]];
       }
     }
-    float4 tA[kCPL], tB[kCPL];
-    double2 tR0[kCPL], tR1[kCPL];
+    float4 tA[kCP], tB[kCP];
+    double2 tR0[kCP], tR1[kCP];
 #pragma unroll
-    for (int u = 0; u < kCPL; ++u) {
+    for (int u = 0; u < kCP; ++u) {
       const int pdt = simstep - tv[u];
       if (ok[u] && pdt > 0 && pdt < tlen) {
         tA[u] = T->tab[(size_t)pdt * 4 + 0];
@@ -276,7 +281,7 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
       }
     }
 #pragma unroll
-    for (int u = 0; u < kCPL; ++u) {
+    for (int u = 0; u < kCP; ++u) {
       if (!ok[u]) continue;
       const int c = b0 + u * 32 + lane;
       const int r = c / M, j = c - r * M;
@@ -315,7 +320,7 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
     for (int jj = 0; jj < 2; ++jj) {
       const int j = lane + 32 * jj;
       if (j >= M) continue;
-      for (int c = (b0 / M) * M + j; c < min(ncell, b0 + kCellsPerPass); c += M) {
+      for (int c = (b0 / M) * M + j; c < min(ncell, b0 + kPass); c += M) {
         if (c < b0) continue;
         if (!ws_skip[c - b0]) e[jj] += ws_w[c - b0];
       }
@@ -327,6 +332,7 @@ __device__ __noinline__ void rows_pass(const Member& B, const TabRef* __restrict
 /* gather the active slots of HCU h (the arrival-ring words `words`, already
    loaded: word g*32 + lane in words[g]) into ascending passes of at most
    kListCap rows; every pass runs rows_pass.  Returns the number of rows. */
+template <int kCP>
 __device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restrict__ T, int h, int simstep, float kp,
                                          const uint32_t words[kMaxW], int* ws_list, float* ws_pi, const float* ws_pj,
                                          float* ws_w, int8_t* ws_skip, float e[2], int lane) {
@@ -360,12 +366,12 @@ __device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restri
       nl += take;
       done += take;
       if (nl == kListCap) {
-        rows_pass(B, T, h, ws_list, nl, simstep, kp, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
+        rows_pass<kCP>(B, T, h, ws_list, nl, simstep, kp, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
         nl = 0;
       }
     }
   }
-  if (nl) rows_pass(B, T, h, ws_list, nl, simstep, kp, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
+  if (nl) rows_pass<kCP>(B, T, h, ws_list, nl, simstep, kp, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
   return total_rows;
 }
 
@@ -374,6 +380,7 @@ __device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restri
    then every load the tick needs that depends on nothing else goes out
    together (previous-tick state of the HCU's MCUs, stimulus, the softmax
    seed's terms, the HCU's arrival words of this tick). */
+template <int kCP>
 __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h, int it, float* ws,
                                        unsigned long long& rows_acc, unsigned long long& cols_acc) {
   const int lane = threadIdx.x & 31;
@@ -549,7 +556,7 @@ __device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h,
   __syncwarp();
 
   /* the active rows of this tick, ascending (Proj.cpp:365-479, 667-720) */
-  const int nrows = item_rows(B, T, h, simstep, kp, words, ws_list, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
+  const int nrows = item_rows<kCP>(B, T, h, simstep, kp, words, ws_list, ws_pi, ws_pj, ws_w, ws_skip, e, lane);
 #pragma unroll
   for (int jj = 0; jj < 2; ++jj) {
     const int j = lane + 32 * jj;
@@ -718,7 +725,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const Dev* __restric
 #endif
     for (int e = i0; e < i1; ++e) {
       const int2 item = D.items[D.warp_items[e]];
-      item_tick(D, R, item.x, item.y, it, ws, rows_acc, cols_acc);
+      item_tick<(kThreads >= 384) ? 1 : kCPL>(D, R, item.x, item.y, it, ws, rows_acc, cols_acc);
     }
 #ifdef BCPNN_PHASE_PROBE
     if (lane == 0) {
