@@ -381,7 +381,7 @@ __device__ __forceinline__ int item_rows(const Member& B, const TabRef* __restri
    together (previous-tick state of the HCU's MCUs, stimulus, the softmax
    seed's terms, the HCU's arrival words of this tick). */
 template <int kCP>
-__device__ __noinline__ void item_tick(const Dev& D, const Run& R, int n, int h, int it, float* ws,
+__device__ __forceinline__ void item_tick(const Dev& D, const Run& R, int n, int h, int it, float* ws,
                                        unsigned long long& rows_acc, unsigned long long& cols_acc) {
   const int lane = threadIdx.x & 31;
   {
