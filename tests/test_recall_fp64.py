@@ -100,3 +100,28 @@ def test_error_metrics():
     assert m["first_divergence_tick"] == 2
     assert abs(m["support_rel_err"] - np.float64(np.float32(2.4) - 2.5).__abs__() / 2.5) < 1e-7
     assert m["spike_jaccard"] == 3 / 4
+
+
+def test_rows_follow_each_hcus_slot_order():
+    """epsc += w over the active sources in the slot order of every
+    destination HCU, also when the HCUs order their slots differently"""
+    rng = np.random.default_rng(3)
+    H, M = 3, 4
+    N = H * M
+    # magnitudes spread over 16 decades across rows: the sums depend on the order
+    W = rng.standard_normal((N, N)) * (10.0 ** rng.uniform(-8, 8, N))[:, None]
+    pos = np.stack([rng.permutation(N) for _ in range(H)])
+    pop = dict(hcu_num=H, mcu_num=M, taum=0.005, wtagain=1.0, maxfq=100.0, igain=1.0, wgain=1.0, lgbias=0.0,
+               snoise=0.0)
+    z = np.zeros(N, np.float32)
+    rs = recall_fp64.RecallFP64(pop, 0.001, 0.005, 0.0, W, z, z, pos, z, z, (z, z, z),
+                                np.zeros((1, H), np.int32), np.ones((1, H), np.float32), 1e-4, 0, [0])
+    active = rng.random(N) < 0.6
+    rs._rows(0, active)
+    for h in range(H):
+        src = [i for i in np.argsort(pos[h]) if active[i]]  # slot order of HCU h
+        for m in range(M):
+            want = 0.0
+            for i in src:
+                want += W[i, h * M + m]
+            assert rs.epsc[0, h * M + m] == want
