@@ -36,6 +36,24 @@ constexpr int kRowCells = 1024;      /* cells of one row chunk in shared memory 
 
 __host__ __device__ inline int row_chunk(int M) { return M >= kRowCells ? 1 : kRowCells / M; }
 
+/* phase probe of the persistent launch (BCPNN_PHASE_PROBE): thread 0 adds
+   the cycles since its previous mark to slot `slot` of its CTA's counters:
+   0 barrier wait, 1 support, 2 softmax maximum and exponentials, 3 softmax
+   sum, 4 spikes, 5 j-traces and row list, 6 row traces and cell replays,
+   7 weights, 8 epsc sums, 9 delay queue; kProbeTicks counts the ticks */
+#ifdef BCPNN_PHASE_PROBE
+#define MPROBE(slot)                                                   \
+  do {                                                                 \
+    if (threadIdx.x == 0) {                                            \
+      const long long t_ = clock64();                                  \
+      g_probe_smem[slot] += (unsigned long long)(t_ - *probe_t);       \
+      *probe_t = t_;                                                   \
+    }                                                                  \
+  } while (0)
+#else
+#define MPROBE(slot) do {} while (0)
+#endif
+
 /* dynamic shared memory of proj_kernel, in bytes */
 __host__ __device__ inline size_t proj_smem_bytes(int M, int C) {
   return (size_t)(M + C + kRowCells + 3 * row_chunk(M)) * 4;
@@ -51,7 +69,8 @@ __device__ __forceinline__ void entry(const float4* tab, int len, const Coef& k,
 /* Population update, ProcUpdMulti/Pop.cpp:222-311 and fill_spike 403-421.
    dynamic shared memory: 2*M floats. */
 __device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it, int P,
-                                        int h, float* sm, float* s_vsum_p) {
+                                        int h, float* sm, float* s_vsum_p, long long* probe_t) {
+  (void)probe_t;
   float& s_vsum = *s_vsum_p;
   __shared__ float s_red[32];
   const PopDev& pop = net->pops[P];
@@ -86,6 +105,7 @@ __device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const Ru
     s_dsup[j] = nd;
   }
   __syncthreads();
+  MPROBE(1);
   /* update_sup_kernel_2_cpu, Pop.cpp:255-286: the maximum (order does not
      matter) and the exponentials in parallel, the sum serial in MCU order */
   {
@@ -107,12 +127,14 @@ __device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const Ru
       s_act[m] = a;
     }
     __syncthreads();
+    MPROBE(2);
     if (threadIdx.x == 0) {
       float vsum = 0.0f;
       for (int m = 0; m < M; ++m) vsum += s_act[m];
       s_vsum = vsum;
     }
     __syncthreads();
+    MPROBE(3);
   }
   /* update_sup_kernel_3_cpu, Pop.cpp:288-311 */
   const float vsum = s_vsum;
@@ -156,12 +178,14 @@ __device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const Ru
     if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
     for (int q = 0; q < pop.n_out; ++q) net->projs[pop.out_proj[q]].si[cur][idx] = sv;
   }
+  MPROBE(4);
 }
 
 __global__ void pop_kernel(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it) {
   extern __shared__ __align__(16) float sm[];
   __shared__ float s_vsum;
-  pop_hcu(net, rp, it, net->cta_pop[blockIdx.x], net->cta_hcu[blockIdx.x], sm, &s_vsum);
+  long long probe_t = 0;
+  pop_hcu(net, rp, it, net->cta_pop[blockIdx.x], net->cta_hcu[blockIdx.x], sm, &s_vsum, &probe_t);
 }
 
 /* One closed-form decay of a cell over pdt ticks.  With the run's TabRef of
@@ -232,7 +256,8 @@ struct ProjShared {
 };
 
 __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it,
-                                         int p, int h, float* sm, ProjShared* ps) {
+                                         int p, int h, float* sm, ProjShared* ps, long long* probe_t) {
+  (void)probe_t;
   int* s_warp = ps->warp;
   int& s_total = ps->total;
   int& s_flag9 = ps->flag9;
@@ -278,6 +303,7 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
   for (int i = tid; i < nrow; i += blockDim.x) s_list[i] = J.list[h * C + i];
   if (tid == 0) s_flag9 = 0;
   __syncthreads();
+  MPROBE(5);
 
   /* update_row_cpu, Proj.cpp:638-706 */
   for (int base = 0; base < nrow; base += rch) {
@@ -329,6 +355,7 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
       s_w[c] = c4.x;
     }
     __syncthreads();
+    MPROBE(6);
     for (int c = tid; c < nr * M; c += blockDim.x) {
       const int rr = c / M, j = c - rr * M;
       const size_t index = (size_t)s_list[base + rr] * M + j;
@@ -342,12 +369,14 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
       s_w[c] = w;
     }
     __syncthreads();
+    MPROBE(7);
     for (int j = tid; j < M; j += blockDim.x) {
       float e = s_epsc[j];
       for (int rr = 0; rr < nr; ++rr) e += s_w[rr * M + j];
       s_epsc[j] = e;
     }
     __syncthreads();
+    MPROBE(8);
   }
   for (int j = tid; j < M; j += blockDim.x) pop.epsc[cur][eoff + h * M + j] = s_epsc[j];
 
@@ -386,13 +415,15 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
     if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + p], f);
     atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
   }
+  MPROBE(9);
 }
 
 __global__ void __launch_bounds__(kProjThreads, 1) proj_kernel(const NetDev* __restrict__ net,
                                                               const RunParams* __restrict__ rp, int it, int p) {
   extern __shared__ __align__(16) float sm[];
   __shared__ ProjShared ps;
-  proj_hcu(net, rp, it, p, blockIdx.x, sm, &ps);
+  long long probe_t = 0;
+  proj_hcu(net, rp, it, p, blockIdx.x, sm, &ps, &probe_t);
 }
 
 /* Persistent form: one cooperative launch per run, one CTA per (population,
@@ -410,15 +441,34 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
   const int P = net->cta_pop[blockIdx.x];
   const int h = net->cta_hcu[blockIdx.x];
   const PopDev& pop = net->pops[P];
+#ifdef BCPNN_PHASE_PROBE
+  if (threadIdx.x < kProbeSlots) g_probe_smem[threadIdx.x] = 0;
+  __syncthreads();
+#endif
+#ifdef BCPNN_PHASE_PROBE
+  long long probe_clock = clock64();
+#else
+  long long probe_clock = 0;
+#endif
+  long long* probe_t = &probe_clock;
   for (int it = it0; it < it0 + n_ticks; ++it) {
-    if (it > it0 && !sync(it - it0)) return;
-    pop_hcu(net, rp, it, P, h, sm, &s_vsum);
+    if (it > it0 && !sync(it - it0)) break;
+    MPROBE(0);
+#ifdef BCPNN_PHASE_PROBE
+    if (threadIdx.x == 0) g_probe_smem[kProbeTicks] += 1;
+#endif
+    pop_hcu(net, rp, it, P, h, sm, &s_vsum, probe_t);
     __syncthreads();
     for (int q = 0; q < pop.n_in; ++q) {
-      proj_hcu(net, rp, it, pop.in_proj[q], h, sm, &ps);
+      proj_hcu(net, rp, it, pop.in_proj[q], h, sm, &ps, probe_t);
       __syncthreads();
     }
   }
+#ifdef BCPNN_PHASE_PROBE
+  __syncthreads();
+  if (threadIdx.x < kProbeSlots && blockIdx.x < kProbeCtas)
+    atomicAdd(&g_phase_probe[blockIdx.x * kProbeSlots + threadIdx.x], g_probe_smem[threadIdx.x]);
+#endif
 }
 
 /* update_all_cpu (Proj.cpp:490-555) for projection p at a change of prn:

@@ -13,6 +13,10 @@ clock given by --mhz (the counters are SM clock cycles).  The probe adds a
 clock read and a store per phase boundary, so the total is a little above
 the default build's time per tick.  Slots 14 and 15 count the cell and row
 decays done by the div_rn fallback and by the reciprocal form.
+
+`--variant multi` probes the ProcUpdMulti launch on the same workload
+(adaptation taua 0.05, adgain 1; a spike ring of `--ring` ticks): one
+thread per CTA marks the phases of its HCU's tick in order.
 """
 import argparse
 import os
@@ -30,6 +34,9 @@ PHASES_B = {16: "barrier wait", 26: "column units of the grid", 19: "  units: ri
             20: "  units: tables, decay, store", 21: "  units: group sync", 17: "delay queue: loads, ballots",
             18: "delay queue: sync", 27: "delay queue: list", 28: "spike wait", 29: "unit publication",
             24: "join wait", 25: "staging next chunk"}
+PHASES_MULTI = {0: "barrier wait", 1: "support", 2: "softmax: max, exp", 3: "softmax: sum", 4: "spikes",
+                5: "j-traces, row list", 6: "row traces, cell replays", 7: "weights", 8: "epsc sums",
+                9: "delay queue"}
 
 
 def main():
@@ -38,6 +45,8 @@ def main():
     ap.add_argument("--recall", type=int, default=20)
     ap.add_argument("--mhz", type=float, default=1965.0)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--variant", choices=("lazy", "multi"), default="lazy")
+    ap.add_argument("--ring", type=int, default=25)
     ap.add_argument("--critical", type=int, default=0,
                     help="also print the N CTAs with the least barrier wait (the ones that arrive last most often)")
     a = ap.parse_args()
@@ -50,8 +59,11 @@ def main():
     lgidx, wmask = extgen.stim_tables(schema.read_stim(sp.gen_param.stim_file))
     runs = extgen.segments(sp)
     first_recall = next(i for i, r in enumerate(runs) if r.prn == 0.0)
-    net = capi.Net(pops, projs, float(np.float32(sp.gen_param.dt)), seed=w.meta["seed"], max_ticks=128,
-                   tick_threads=a.threads)
+    kw = dict(tick_threads=a.threads)
+    if a.variant == "multi":
+        pops = [dict(p, taua=0.05, adgain=1.0) for p in pops]
+        kw = dict(variant=1, spike_buffer=a.ring)
+    net = capi.Net(pops, projs, float(np.float32(sp.gen_param.dt)), seed=w.meta["seed"], max_ticks=128, **kw)
     for k, (ii, di) in enumerate(conn):
         net.set_conn(k, ii, di)
     net.upload_stimuli_idx(lgidx, float(np.float32(sp.gen_param.eps)), wmask)
@@ -74,6 +86,16 @@ def main():
         per_tick = c / np.maximum(ticks, 1) / a.mhz  # us per tick
         out[name] = per_tick
     net.close()
+    if a.variant == "multi":
+        for name, pt in out.items():
+            print(f"== {name} segments, ProcUpdMulti: us per tick at {a.mhz:.0f} MHz (median CTA / slowest CTA)")
+            tot = 0.0
+            for k, ph in PHASES_MULTI.items():
+                med, mx = float(np.median(pt[:, k])), float(pt[:, k].max())
+                tot += med
+                print(f"  {ph:<26} {med:7.3f} {mx:7.3f}")
+            print(f"  {'total (median)':<26} {tot:7.3f}")
+        return
     for name, pt in out.items():
         print(f"== {name} segments: us per tick at {a.mhz:.0f} MHz (median CTA / slowest CTA)")
         tot = 0.0
