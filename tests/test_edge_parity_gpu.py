@@ -17,6 +17,9 @@ The cases:
   - widest: 2x512, the most MCUs a 512-thread CTA takes, full recurrent
     (C = 1024, 10^6 cells).
 
+The time constants of a projection stay distinct (tauzi, tauzj != taue):
+gsbn's closed-form decays divide by their differences.
+
 Each case runs training segments and then recall segments (prn changes, so
 the all-cells catch-up runs), compares the spikes of every tick and, at the
 end, every state vector by bit pattern and the cell-update counters with the
@@ -62,7 +65,7 @@ def sparse_case(rng):
 
 def tiny_case(rng):
     pops = [pop(3, 1), pop(1, 7)]
-    projs = [proj(0, 1, 3), proj(1, 0, 7, tau=0.005), proj(1, 1, 7, tau=0.02)]
+    projs = [proj(0, 1, 3), proj(1, 0, 7, tau=0.005), proj(1, 1, 7, tau=0.03)]
     conn = [(np.arange(3, dtype=np.int32), np.array([1, 2, 3], np.int32)),
             (np.full(3 * 7, -1, np.int32), np.zeros(3 * 7, np.int32)),
             (np.arange(7, dtype=np.int32), np.full(7, 31, np.int32))]
