@@ -69,7 +69,8 @@ __device__ __forceinline__ void entry(const float4* tab, int len, const Coef& k,
 /* Population update, ProcUpdMulti/Pop.cpp:222-311 and fill_spike 403-421.
    dynamic shared memory: 2*M floats. */
 __device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it, int P,
-                                        int h, float* sm, float* s_vsum_p, long long* probe_t) {
+                                        int h, float* sm, float* s_vsum_p, long long* probe_t,
+                                        uint32_t* s_hist = nullptr) {
   (void)probe_t;
   float& s_vsum = *s_vsum_p;
   __shared__ float s_red[32];
@@ -174,6 +175,7 @@ __device__ __forceinline__ void pop_hcu(const NetDev* __restrict__ net, const Ru
     const int idx = h * M + j;
     const int8_t sv = s_spk[j];
     ring[idx] = sv;
+    if (s_hist) s_hist[j] = (s_hist[j] << 1) | (sv > 0 ? 1u : 0u);
     pop.spike[idx] = sv;
     if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
     for (int q = 0; q < pop.n_out; ++q) net->projs[pop.out_proj[q]].si[cur][idx] = sv;
@@ -249,6 +251,32 @@ __device__ __forceinline__ void replay_cell(float4& c4, int tij, float zi2, int 
   c4 = make_float4(pij, eij, zi2, zj2);
 }
 
+/* replay_cell of the tick path (last tick exclusive, final decay always)
+   with the postsynaptic spikes of the last 32 ticks as a mask: bit b of
+   `hist` is the spike of this cell's MCU at tick simstep - b, as the ring
+   holds it (ring length B <= 32).  The ticks visited and the decays done are
+   those of replay_cell's loop over the ring: the ticks after
+   max(tij, simstep - B + 1) and before simstep, ascending. */
+__device__ __forceinline__ void replay_cell_hist(float4& c4, int tij, float zi2, int simstep, uint32_t hist, int B,
+                                                 const Coef& k, const float4* tab, int tlen, const TabRef* T,
+                                                 float kftj) {
+  float pij = c4.x, eij = c4.y, zj2 = c4.w;
+  const int lo = (simstep - tij >= B) ? simstep - B + 1 : tij;
+  const int span = simstep - lo; /* ticks lo+1 .. simstep are bits span-1 .. 0 */
+  uint32_t m = span > 1 ? (hist & (0xffffffffu >> (32 - span))) & ~1u : 0u;
+  while (m) {
+    const int b = 31 - __clz(m);
+    m &= ~(1u << b);
+    const int now = simstep - b;
+    decay_cell(pij, eij, zi2, zj2, k, tab, tlen, T, now - tij);
+    zj2 = zj2 + kftj;
+    tij = now;
+  }
+  float zi2_unused = zi2;
+  decay_cell(pij, eij, zi2_unused, zj2, k, tab, tlen, T, simstep - tij);
+  c4 = make_float4(pij, eij, zi2, zj2);
+}
+
 /* One tick of projection p for one destination HCU: update_jxx_cpu,
    update_ssi_cpu, update_row_cpu and update_que_cpu (Proj.cpp:557-706). */
 struct ProjShared {
@@ -256,7 +284,8 @@ struct ProjShared {
 };
 
 __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const RunParams* __restrict__ rp, int it,
-                                         int p, int h, float* sm, ProjShared* ps, long long* probe_t) {
+                                         int p, int h, float* sm, ProjShared* ps, long long* probe_t,
+                                         const uint32_t* s_hist = nullptr) {
   (void)probe_t;
   int* s_warp = ps->warp;
   int& s_total = ps->total;
@@ -349,8 +378,14 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
       const int rr = c / M, j = c - rr * M;
       const size_t index = (size_t)s_list[base + rr] * M + j;
       float4 c4 = J.cell[index];
-      replay_cell(c4, s_ti[rr], s_zi[rr], simstep, 1, pop.ring, B, n, h * M + j, k, tab, tlen, T, J.kftj, true);
-      if (sj[h * M + j] > 0) c4.w += J.kftj;
+      if (s_hist) {
+        const uint32_t hist = s_hist[j];
+        replay_cell_hist(c4, s_ti[rr], s_zi[rr], simstep, hist, B, k, tab, tlen, T, J.kftj);
+        if (hist & 1u) c4.w += J.kftj;
+      } else {
+        replay_cell(c4, s_ti[rr], s_zi[rr], simstep, 1, pop.ring, B, n, h * M + j, k, tab, tlen, T, J.kftj, true);
+        if (sj[h * M + j] > 0) c4.w += J.kftj;
+      }
       J.cell[index] = c4;
       s_w[c] = c4.x;
     }
@@ -384,28 +419,51 @@ __device__ __forceinline__ void proj_hcu(const NetDev* __restrict__ net, const R
      (update_ssi_cpu, :580-588), ascending */
   const int8_t* si = J.si[prev];
   int cnt = 0;
-  for (int s0 = 0; s0 < C; s0 += blockDim.x) {
-    const int s = s0 + tid;
-    bool act = false;
-    if (s < C) {
-      const int r = h * C + s;
-      const int src = J.ii[r];
-      if (src >= 0) {
-        if (src >= J.Ns) {
-          atomicOr(net->err, kErrIndex);
-        } else {
-          int qv = J.qi[r];
-          act = (qv & 0x01) != 0;
-          qv >>= 1;
-          if (si[src] > 0) qv |= (0x01 << (J.di[r] - 1));
-          J.qi[r] = qv;
+  /* kQB chunks of blockDim slots at a time: their table loads, then their
+     source-spike loads, are issued together, and the chunks' compactions
+     follow in slot order */
+  constexpr int kQB = 4;
+  for (int s0 = 0; s0 < C; s0 += kQB * (int)blockDim.x) {
+    int src[kQB], qv[kQB], dv[kQB];
+    bool act[kQB];
+#pragma unroll
+    for (int u = 0; u < kQB; ++u) {
+      const int s = s0 + u * (int)blockDim.x + tid;
+      src[u] = -1;
+      qv[u] = 0;
+      dv[u] = 1;
+      if (s < C) {
+        src[u] = J.ii[h * C + s];
+        if (src[u] >= 0) {
+          qv[u] = J.qi[h * C + s];
+          dv[u] = J.di[h * C + s];
         }
       }
     }
-    int tot;
-    const int pos = block_prefix(act, s_warp, &s_total, &tot);
-    if (act) J.list[h * C + cnt + pos] = h * C + s;
-    cnt += tot;
+#pragma unroll
+    for (int u = 0; u < kQB; ++u) {
+      const int s = s0 + u * (int)blockDim.x + tid;
+      act[u] = false;
+      if (src[u] >= 0) {
+        if (src[u] >= J.Ns) {
+          atomicOr(net->err, kErrIndex);
+        } else {
+          int q = qv[u];
+          act[u] = (q & 0x01) != 0;
+          q >>= 1;
+          if (si[src[u]] > 0) q |= (0x01 << (dv[u] - 1));
+          J.qi[h * C + s] = q;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kQB; ++u) {
+      if (s0 + u * (int)blockDim.x >= C) break;
+      int tot;
+      const int pos = block_prefix(act[u], s_warp, &s_total, &tot);
+      if (act[u]) J.list[h * C + cnt + pos] = h * C + s0 + u * (int)blockDim.x + tid;
+      cnt += tot;
+    }
   }
   if (tid == 0) {
     J.list_cnt[h] = cnt;
@@ -451,16 +509,35 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
   long long probe_clock = 0;
 #endif
   long long* probe_t = &probe_clock;
+  /* the HCU's spikes of the last 32 ticks, one mask per MCU (ring length
+     <= 32): bit b of s_hist[j] is the ring's entry for tick s - 1 - b before
+     the first tick s of this launch, and the entry for tick s - b once tick
+     s has sampled its spikes */
+  __shared__ uint32_t s_hist_buf[kProjThreads];
+  uint32_t* s_hist = nullptr;
+  if (pop.ring_len <= 32 && pop.M <= kProjThreads) {
+    s_hist = s_hist_buf;
+    const int B = pop.ring_len, M = pop.M, s0 = rp->simstep0 + it0;
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+      uint32_t m = 0;
+      for (int b = 0; b < B - 1; ++b) {
+        const int t = s0 - 1 - b;
+        if (t >= 0 && pop.ring[(size_t)(t % B) * pop.n + h * M + j] > 0) m |= 1u << b;
+      }
+      s_hist[j] = m;
+    }
+    __syncthreads();
+  }
   for (int it = it0; it < it0 + n_ticks; ++it) {
     if (it > it0 && !sync(it - it0)) break;
     MPROBE(0);
 #ifdef BCPNN_PHASE_PROBE
     if (threadIdx.x == 0) g_probe_smem[kProbeTicks] += 1;
 #endif
-    pop_hcu(net, rp, it, P, h, sm, &s_vsum, probe_t);
+    pop_hcu(net, rp, it, P, h, sm, &s_vsum, probe_t, s_hist);
     __syncthreads();
     for (int q = 0; q < pop.n_in; ++q) {
-      proj_hcu(net, rp, it, pop.in_proj[q], h, sm, &ps, probe_t);
+      proj_hcu(net, rp, it, pop.in_proj[q], h, sm, &ps, probe_t, s_hist);
       __syncthreads();
     }
   }
