@@ -45,6 +45,14 @@ __global__ void __launch_bounds__(kProjThreads, 1) tick_kernel(const NetDev* __r
   tick_loop(net, rp, it0, n_ticks,
             [&](int k) { return t512::grid_sync(bar, (unsigned int)k * gridDim.x, net->err, &s_ok); });
 }
+/* the same with each HCU's state resident in shared memory (res_tick_loop) */
+__global__ void __launch_bounds__(kProjThreads, 1) res_tick_kernel(const NetDev* __restrict__ net,
+                                                                  const RunParams* __restrict__ rp, int it0,
+                                                                  int n_ticks, unsigned int* bar) {
+  __shared__ int s_ok;
+  res_tick_loop(net, rp, it0, n_ticks,
+                [&](int k) { return t512::grid_sync(bar, (unsigned int)k * gridDim.x, net->err, &s_ok); });
+}
 }  // namespace multi
 }  // namespace bcpnn
 
@@ -110,6 +118,7 @@ struct bcpnn_net {
   bool fp64 = false;        /* FP64-built decay tables */
   bool multi = false;       /* ProcUpdMulti variant (bcpnn_multi.cuh) */
   bool multi_persistent = false; /* its one-launch-per-run form */
+  bool multi_resident = false;   /* ... with each HCU's state in shared memory */
   size_t multi_smem = 0;
   int ring_len = 1;         /* its spike buffer size */
   const void* tick_fn = nullptr;  /* the tick kernel variant of the persistent launch */
@@ -342,8 +351,9 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
       cudaMemsetAsync(net->bar, 0, sizeof(unsigned int), net->stream);
       int it0 = 0, n = n_ticks;
       void* args[] = {(void*)&net->d_net, (void*)&net->d_rp, (void*)&it0, (void*)&n, (void*)&net->bar};
-      cudaLaunchCooperativeKernel((const void*)multi::tick_kernel, dim3(net->total_hcu), dim3(multi::kProjThreads), args,
-                                  net->multi_smem, net->stream);
+      cudaLaunchCooperativeKernel(net->multi_resident ? (const void*)multi::res_tick_kernel
+                                                      : (const void*)multi::tick_kernel,
+                                  dim3(net->total_hcu), dim3(multi::kProjThreads), args, net->multi_smem, net->stream);
       return;
     }
     const size_t pop_smem = (size_t)(2 * net->max_m + net->max_m) * sizeof(float);
@@ -846,6 +856,17 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
       return bail(BCPNN_ERR_INVALID);
     }
     ms = std::max(ms, (size_t)(3 * net->max_m) * sizeof(float)); /* the population update's share */
+    /* the resident persistent form: every population's HCU state in shared
+       memory, spike ring of at most 32 ticks (its replay masks) */
+    size_t rs = 0;
+    for (const PopHost& P : net->pops) {
+      int C[kMaxIn] = {0};
+      for (size_t q = 0; q < P.in_proj.size(); ++q) C[q] = net->projs[P.in_proj[q]].C;
+      rs = std::max(rs, multi::res_smem_bytes(P.M, (int)P.in_proj.size(), C));
+    }
+    const char* er = std::getenv("GSBN_MULTI_RESIDENT");
+    net->multi_resident = !(er && er[0] == '0') && net->ring_len <= 32 && rs + 8192 <= (size_t)smem_max;
+    if (net->multi_resident) ms = std::max(ms, rs);
     net->multi_smem = ms;
     static std::mutex mu;
     static size_t raised[kMaxDevices] = {0};
@@ -854,6 +875,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
       if (cudaFuncSetAttribute(multi::proj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms) !=
               cudaSuccess ||
           cudaFuncSetAttribute(multi::tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms) !=
+              cudaSuccess ||
+          cudaFuncSetAttribute(multi::res_tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms) !=
               cudaSuccess) {
         net->err = "cannot raise the shared memory limit of the ProcUpdMulti kernels";
         return bail(BCPNN_ERR_CUDA);
@@ -863,7 +886,9 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     int coop = 0, sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, net->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi::tick_kernel, multi::kProjThreads, ms);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, net->multi_resident ? (const void*)multi::res_tick_kernel : (const void*)multi::tick_kernel,
+        multi::kProjThreads, ms);
     const char* e = std::getenv("GSBN_PER_TICK");
     const bool forced = e && e[0] == '1';
     net->multi_persistent = !forced && coop && (long long)per_sm * sms >= net->total_hcu;

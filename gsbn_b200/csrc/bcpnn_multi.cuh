@@ -18,7 +18,9 @@
  *
  * One launch of pop_kernel per tick over every (population, HCU), then one
  * launch of proj_kernel per projection over its destination HCUs (512
- * threads); all_kernel does the catch-up at a change of prn.  Per-tick
+ * threads), or one persistent launch per run (tick_loop, or res_tick_loop
+ * with each HCU's state resident in shared memory); all_kernel does the
+ * catch-up at a change of prn.  Per-tick
  * buffers follow the ProcUpdLazy path's tick parity (dsup, epsc, bj, si), so
  * state reads and the spike log work unchanged.
  */
@@ -40,7 +42,8 @@ __host__ __device__ inline int row_chunk(int M) { return M >= kRowCells ? 1 : kR
    the cycles since its previous mark to slot `slot` of its CTA's counters:
    0 barrier wait, 1 support, 2 softmax maximum and exponentials, 3 softmax
    sum, 4 spikes, 5 j-traces and row list, 6 row traces and cell replays,
-   7 weights, 8 epsc sums, 9 delay queue; kProbeTicks counts the ticks */
+   7 weights, 8 epsc sums, 9 delay queue, 10 (resident launch) wait for the
+   delay-queue warps; kProbeTicks counts the ticks */
 #ifdef BCPNN_PHASE_PROBE
 #define MPROBE(slot)                                                   \
   do {                                                                 \
@@ -545,6 +548,550 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
   __syncthreads();
   if (threadIdx.x < kProbeSlots && blockIdx.x < kProbeCtas)
     atomicAdd(&g_phase_probe[blockIdx.x * kProbeSlots + threadIdx.x], g_probe_smem[threadIdx.x]);
+#endif
+}
+
+/* ---- resident persistent launch ----------------------------------------
+
+   The same tick as tick_loop, with the HCU's state kept in shared memory for
+   the whole launch: the population's dsup, ada, act, counter and stimulus
+   row; per incoming projection pj, ej, zj, epsc, bj, the slot tables ii, di,
+   qi, the row traces pi, ei, zi, ti and the active-row list (by tick
+   parity).  They are loaded at launch and written back after the last tick,
+   epsc/bj/dsup into the buffer of the last tick's parity, which is where the
+   next run and the state reads look.  What other CTAs read stays in global
+   memory every tick: the source spikes si of the exchange, the ring, the
+   spike vector and the spike log; the cells (pij, eij, zi2, zj2) and wij
+   stay in global memory.
+
+   The delay queue of a tick reads only the previous tick's source spikes and
+   qi, so its 4 warps (threads 384-511) compute the next tick's active rows
+   while the other 12 warps do the population update; every thread then
+   takes part in the projections. */
+constexpr int kResQueueWarps = 4;
+constexpr int kResPopThreads = kProjThreads - 32 * kResQueueWarps; /* 384 */
+constexpr int kBarPop = 1, kBarQueue = 2;
+
+__device__ __forceinline__ void named_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+/* word offsets of the resident layout in dynamic shared memory */
+struct ResLayout {
+  int dsup, ada, act, cnt, lg, hist, spk; /* population, [M] (spk: bytes) */
+  int w, rpi, rti, rzi;                   /* row-chunk scratch            */
+  int qmask;                              /* delay-queue ballots          */
+  int q[kMaxIn];                          /* incoming projection blocks   */
+  int total;
+};
+
+/* one projection block: pj ej zj epsc bj [M]; ii di qi pi ei zi ti [C];
+   list [2][C] */
+__host__ __device__ inline int res_qwords(int M, int C) { return 5 * M + 9 * C; }
+
+__host__ __device__ inline void res_layout(int M, int n_in, const int* C, ResLayout& L) {
+  int o = 0;
+  L.dsup = o; o += M;
+  L.ada = o; o += M;
+  L.act = o; o += M;
+  L.cnt = o; o += M;
+  L.lg = o; o += M;
+  L.hist = o; o += M;
+  L.spk = o; o += (M + 3) / 4;
+  const int rch = row_chunk(M);
+  L.w = o; o += kRowCells;
+  L.rpi = o; o += rch;
+  L.rti = o; o += rch;
+  L.rzi = o; o += rch;
+  int cmax = 0;
+  for (int q = 0; q < n_in; ++q) cmax = C[q] > cmax ? C[q] : cmax;
+  L.qmask = o; o += (cmax + 31) / 32;
+  for (int q = 0; q < kMaxIn; ++q) {
+    L.q[q] = o;
+    if (q < n_in) o += res_qwords(M, C[q]);
+  }
+  L.total = o;
+}
+
+/* dynamic shared memory of the resident launch for one population, bytes */
+__host__ __device__ inline size_t res_smem_bytes(int M, int n_in, const int* C) {
+  ResLayout L;
+  res_layout(M, n_in, C, L);
+  return (size_t)L.total * 4;
+}
+
+struct ResQ {
+  float *pj, *ej, *zj, *epsc, *bj;
+  int *ii, *di, *qi;
+  float *pi, *ei, *zi;
+  int *ti, *list;
+};
+
+__device__ __forceinline__ ResQ res_q(float* sm, const ResLayout& L, int q, int M, int C) {
+  ResQ v;
+  float* b = sm + L.q[q];
+  v.pj = b;
+  v.ej = b + M;
+  v.zj = b + 2 * M;
+  v.epsc = b + 3 * M;
+  v.bj = b + 4 * M;
+  int* ib = (int*)(b + 5 * M);
+  v.ii = ib;
+  v.di = ib + C;
+  v.qi = ib + 2 * C;
+  v.pi = (float*)(ib + 3 * C);
+  v.ei = (float*)(ib + 4 * C);
+  v.zi = (float*)(ib + 5 * C);
+  v.ti = ib + 6 * C;
+  v.list = ib + 7 * C;
+  return v;
+}
+
+template <typename GridSync>
+__device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, const RunParams* __restrict__ rp,
+                                              int it0, int n_ticks, GridSync sync) {
+  extern __shared__ __align__(16) float sm[];
+  /* descriptors, copied once per launch: every tick reads them in chains */
+  __shared__ PopDev s_pop;
+  __shared__ ProjDev s_proj[kMaxIn];
+  __shared__ TabRef s_tab[kMaxIn];
+  __shared__ int s_inp[kMaxIn];
+  __shared__ int8_t* s_siout[kMaxIn][2];
+  __shared__ ResLayout s_L;
+  __shared__ int s_nlist[kMaxIn][2];
+  __shared__ int s_qcnt[kResQueueWarps];
+  __shared__ float s_red[32];
+  __shared__ float s_vsum, s_wm;
+  __shared__ int s_flag9;
+
+  const int tid = threadIdx.x;
+  const int P = net->cta_pop[blockIdx.x];
+  const int h = net->cta_hcu[blockIdx.x];
+  if (tid == 0) s_pop = net->pops[P];
+  __syncthreads();
+  if (tid < kMaxIn && tid < s_pop.n_in) {
+    const int p = s_pop.in_proj[tid];
+    s_inp[tid] = p;
+    s_proj[tid] = net->projs[p];
+    s_tab[tid] = rp->tabs[p];
+  }
+  if (tid < kMaxIn && tid < s_pop.n_out) {
+    const ProjDev& O = net->projs[s_pop.out_proj[tid]];
+    s_siout[tid][0] = O.si[0];
+    s_siout[tid][1] = O.si[1];
+  }
+  __syncthreads();
+  const PopDev& pop = s_pop;
+  const int M = pop.M, n = pop.n, n_in = pop.n_in, B = pop.ring_len;
+  if (tid == 0) {
+    int c[kMaxIn];
+#pragma unroll
+    for (int q = 0; q < kMaxIn; ++q) c[q] = q < n_in ? s_proj[q].C : 0;
+    res_layout(M, n_in, c, s_L);
+    s_wm = rp->wmask[pop.hcu_start + h];
+  }
+  __syncthreads();
+  const ResLayout& L = s_L;
+  float* r_dsup = sm + L.dsup;
+  float* r_ada = sm + L.ada;
+  float* r_act = sm + L.act;
+  int* r_cnt = (int*)(sm + L.cnt);
+  float* r_lg = sm + L.lg;
+  uint32_t* r_hist = (uint32_t*)(sm + L.hist);
+  int8_t* r_spk = (int8_t*)(sm + L.spk);
+  float* s_w = sm + L.w;
+  float* s_pi = sm + L.rpi;
+  int* s_ti = (int*)(sm + L.rti);
+  float* s_zi = sm + L.rzi;
+  uint32_t* s_qmask = (uint32_t*)(sm + L.qmask);
+  const int rch = row_chunk(M);
+
+  /* ---- load the resident state: buffers of the tick before the launch ---- */
+  {
+    const int prev0 = ((rp->k0 + it0) & 1) ^ 1;
+    const int s0 = rp->simstep0 + it0;
+    for (int j = tid; j < M; j += blockDim.x) {
+      const int idx = h * M + j;
+      r_dsup[j] = pop.dsup[prev0][idx];
+      r_ada[j] = pop.ada[idx];
+      r_act[j] = pop.act[idx];
+      r_cnt[j] = pop.counter[idx];
+      r_lg[j] = rp->lginp[pop.mcu_start + idx];
+      /* bit b: the ring's entry for tick s0 - 1 - b (ring length <= 32) */
+      uint32_t m = 0;
+      for (int b = 0; b < B - 1; ++b) {
+        const int t = s0 - 1 - b;
+        if (t >= 0 && pop.ring[(size_t)(t % B) * n + idx] > 0) m |= 1u << b;
+      }
+      r_hist[j] = m;
+    }
+    for (int q = 0; q < n_in; ++q) {
+      const ProjDev& J = s_proj[q];
+      const int C = J.C;
+      const ResQ V = res_q(sm, L, q, M, C);
+      const size_t eoff = (size_t)J.proj_in_pop * n;
+      for (int j = tid; j < M; j += blockDim.x) {
+        const int idx = h * M + j;
+        V.pj[j] = J.pj[idx];
+        V.ej[j] = J.ej[idx];
+        V.zj[j] = J.zj[idx];
+        V.epsc[j] = pop.epsc[prev0][eoff + idx];
+        V.bj[j] = pop.bj[prev0][eoff + idx];
+      }
+      for (int s = tid; s < C; s += blockDim.x) {
+        const int r = h * C + s;
+        V.ii[s] = J.ii[r];
+        V.di[s] = J.di[r];
+        V.qi[s] = J.qi[r];
+        V.pi[s] = J.pi[r];
+        V.ei[s] = J.ei[r];
+        V.zi[s] = J.zi[r];
+        V.ti[s] = J.ti[r];
+      }
+      const int cnt = J.list_cnt[h];
+      for (int e = tid; e < cnt; e += blockDim.x) V.list[e] = J.list[h * C + e] - h * C;
+      if (tid == 0) s_nlist[q][0] = cnt;
+    }
+  }
+  __syncthreads();
+#ifdef BCPNN_PHASE_PROBE
+  if (tid < kProbeSlots) g_probe_smem[tid] = 0;
+  __syncthreads();
+  long long probe_clock = clock64();
+#else
+  long long probe_clock = 0;
+#endif
+  long long* probe_t = &probe_clock;
+  (void)probe_t;
+
+  int it = it0;
+  for (; it < it0 + n_ticks; ++it) {
+    if (it > it0 && !sync(it - it0)) break;
+    MPROBE(0);
+#ifdef BCPNN_PHASE_PROBE
+    if (tid == 0) g_probe_smem[kProbeTicks] += 1;
+#endif
+    const int simstep = rp->simstep0 + it, kk = rp->k0 + it;
+    const int cur = kk & 1, prev = cur ^ 1;
+    const int lp = (it - it0) & 1; /* list parity: this tick's rows */
+
+    if (tid < kResPopThreads) {
+      /* ---- population update (ProcUpdMulti/Pop.cpp:222-311, 403-421) ---- */
+      constexpr int G = kResPopThreads;
+      const float wm = s_wm;
+      for (int j = tid; j < M; j += G) {
+        float wsup = 0.0f;
+        for (int m = 0; m < n_in; ++m) {
+          const float* b = sm + L.q[m];
+          wsup += b[4 * M + j] + b[3 * M + j]; /* bj + epsc of the previous tick */
+        }
+        float noise = 0.0f;
+        if (pop.snoise != 0.0f)
+          noise = pop.snoise * dev_normal01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)(h * M + j));
+        float sup = pop.lgbias + pop.igain * r_lg[j] + noise;
+        sup += (pop.wgain * wm) * wsup;
+        sup -= wm * r_ada[j];
+        sup = (float)((double)sup + 6.9 * (double)wm); /* a double constant in gsbn */
+        const float d = r_dsup[j];
+        r_dsup[j] = d + (sup - d) * pop.taumdt;
+      }
+      named_sync(kBarPop, G);
+      MPROBE(1);
+      /* the maximum (order does not matter) and the exponentials in
+         parallel, the sum serial in MCU order */
+      float mx = r_dsup[0];
+      for (int m = tid; m < M; m += G) mx = r_dsup[m] > mx ? r_dsup[m] : mx;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float w = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = w > mx ? w : mx;
+      }
+      if ((tid & 31) == 0) s_red[tid >> 5] = mx;
+      named_sync(kBarPop, G);
+      mx = s_red[0];
+      for (int w = 1; w < G / 32; ++w) mx = s_red[w] > mx ? s_red[w] : mx;
+      const float maxact = bx_expf(pop.wtagain * mx);
+      for (int m = tid; m < M; m += G) {
+        float a = bx_expf(pop.wtagain * (r_dsup[m] - mx));
+        if (maxact < 1.0f) a *= maxact;
+        r_act[m] = a;
+      }
+      named_sync(kBarPop, G);
+      MPROBE(2);
+      if (tid == 0) {
+        float vsum = 0.0f;
+#pragma unroll 4
+        for (int m = 0; m < M; ++m) vsum += r_act[m];
+        s_vsum = vsum;
+      }
+      named_sync(kBarPop, G);
+      MPROBE(3);
+      const float vsum = s_vsum;
+      const float pr = net->poisson_hz * net->dt;
+      for (int j = tid; j < M; j += G) {
+        const int idx = h * M + j;
+        float a = r_act[j];
+        if (vsum > 1.0f) a /= vsum;
+        r_act[j] = a;
+        const float u = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+        int8_t spk = (int8_t)(u < a * pop.maxfqdt);
+        if (net->poisson_hz > 0.0f) {
+          const float up = bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+          if (up < pr) spk = 1;
+        }
+        r_cnt[j] += spk;
+        r_ada[j] += (pop.adgain * a - r_ada[j]) * pop.tauadt;
+        r_spk[j] = spk;
+      }
+      if (pop.ext) { /* fill_spike: replayed spikes replace the sampled ones */
+        named_sync(kBarPop, G);
+        for (int j = tid; j < M; j += G) r_spk[j] = 0;
+        named_sync(kBarPop, G);
+        if (simstep >= pop.ext_t0 && simstep < pop.ext_t1) {
+          const int b0 = pop.ext_off[simstep - pop.ext_t0], b1 = pop.ext_off[simstep - pop.ext_t0 + 1];
+          for (int e = b0 + tid; e < b1; e += G) {
+            const int v = pop.ext_idx[e];
+            if (v >= h * M && v < h * M + M) r_spk[v - h * M] = 1;
+          }
+        }
+      }
+      named_sync(kBarPop, G);
+      int8_t* ring = pop.ring + (size_t)(simstep % B) * n;
+      uint32_t* log = pop.spk_log + (size_t)it * pop.log_words;
+      for (int j = tid; j < M; j += G) {
+        const int idx = h * M + j;
+        const int8_t sv = r_spk[j];
+        ring[idx] = sv;
+        r_hist[j] = (r_hist[j] << 1) | (sv > 0 ? 1u : 0u);
+        pop.spike[idx] = sv;
+        if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
+        for (int q = 0; q < pop.n_out; ++q) {
+          int8_t* si = q < kMaxIn ? s_siout[q][cur] : net->projs[pop.out_proj[q]].si[cur];
+          si[idx] = sv;
+        }
+      }
+      MPROBE(4);
+    } else {
+      /* ---- delay queue (update_que_cpu, Proj.cpp:620-636) and the next
+         tick's active rows (update_ssi_cpu, :580-588), ascending ---- */
+      const int qt = tid - kResPopThreads, qw = qt >> 5, lane = tid & 31;
+      const int nq = lp ^ 1;
+      for (int q = 0; q < n_in; ++q) {
+        const ProjDev& J = s_proj[q];
+        const int C = J.C, Ns = J.Ns;
+        const ResQ V = res_q(sm, L, q, M, C);
+        const int8_t* si = J.si[prev];
+        const int ng = (C + 31) >> 5; /* groups of 32 slots; warp qw takes a contiguous range */
+        const int per = (ng + kResQueueWarps - 1) / kResQueueWarps;
+        const int g0 = qw * per, g1 = min(ng, g0 + per);
+        int cnt = 0;
+        for (int gb = g0; gb < g1; gb += 8) {
+          int src[8], qv[8], dv[8];
+          int8_t sv[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int s = (gb + u) * 32 + lane;
+            src[u] = -1;
+            qv[u] = 0;
+            dv[u] = 1;
+            if (gb + u < g1 && s < C) {
+              src[u] = V.ii[s];
+              qv[u] = V.qi[s];
+              dv[u] = V.di[s];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) sv[u] = (src[u] >= 0 && src[u] < Ns) ? si[src[u]] : (int8_t)0;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (gb + u >= g1) break; /* warp-uniform */
+            bool act = false;
+            if (src[u] >= 0) {
+              if (src[u] >= Ns) {
+                atomicOr(net->err, kErrIndex);
+              } else {
+                int v = qv[u];
+                act = (v & 0x01) != 0;
+                v >>= 1;
+                if (sv[u] > 0) v |= (0x01 << (dv[u] - 1));
+                V.qi[(gb + u) * 32 + lane] = v;
+              }
+            }
+            const unsigned mb = __ballot_sync(0xffffffffu, act);
+            if (lane == 0) s_qmask[gb + u] = mb;
+            cnt += __popc(mb);
+          }
+        }
+        if (lane == 0) s_qcnt[qw] = cnt;
+        named_sync(kBarQueue, 32 * kResQueueWarps);
+        int base = 0;
+        for (int w = 0; w < qw; ++w) base += s_qcnt[w];
+        int* out = V.list + nq * C;
+        for (int g = g0; g < g1; ++g) {
+          const uint32_t mb = s_qmask[g];
+          if ((mb >> lane) & 1u) out[base + __popc(mb & ((1u << lane) - 1u))] = g * 32 + lane;
+          base += __popc(mb);
+        }
+        if (qw == kResQueueWarps - 1 && lane == 0) s_nlist[q][nq] = base;
+        named_sync(kBarQueue, 32 * kResQueueWarps); /* s_qmask and s_qcnt are reused */
+      }
+    }
+    __syncthreads();
+    MPROBE(10);
+
+    /* ---- projections: update_jxx_cpu, update_row_cpu (Proj.cpp:557-706) ---- */
+    for (int q = 0; q < n_in; ++q) {
+      const ProjDev& J = s_proj[q];
+      const TabRef* T = &s_tab[q]; /* coefficients and reciprocals of this kp */
+      const int C = J.C;
+      const ResQ V = res_q(sm, L, q, M, C);
+      const float kp = J.taupdt * rp->prn;
+      const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+      const float4* tab = T->tab;
+      const int tlen = T->len;
+      for (int j = tid; j < M; j += blockDim.x) {
+        float pj = V.pj[j], ej = V.ej[j], zj = V.zj[j];
+        float e = V.epsc[j];
+        e *= (1 - J.kepsc);
+        pj += (ej - pj) * kp;
+        ej += (zj - ej) * k.ke;
+        zj *= (1 - J.kzj);
+        if (r_hist[j] & 1u) zj += J.kftj;
+        if (kp != 0.0f) V.bj[j] = J.bgain * bx_logf(pj + J.eps);
+        V.pj[j] = pj;
+        V.ej[j] = ej;
+        V.zj[j] = zj;
+        V.epsc[j] = e;
+      }
+      const int nrow = s_nlist[q][lp];
+      const int* list = V.list + lp * C;
+      if (tid == 0) s_flag9 = 0;
+      __syncthreads();
+      MPROBE(5);
+      for (int base = 0; base < nrow; base += rch) {
+        const int nr = (nrow - base) < rch ? (nrow - base) : rch;
+        for (int t = tid; t < nr; t += blockDim.x) {
+          const int sl = list[base + t];
+          s_ti[t] = V.ti[sl];
+          s_zi[t] = V.zi[sl];
+          if (h * C + sl == 9) s_flag9 = 1;
+        }
+        __syncthreads();
+        /* row traces (from the top thread down) beside the cells (from
+           thread 0 up) */
+        for (int t = blockDim.x - 1 - tid; t < nr; t += blockDim.x) {
+          const int sl = list[base + t];
+          const int pdt = simstep - s_ti[t];
+          float pi = V.pi[sl];
+          if (pdt > 0) {
+            float4 A, Bv;
+            double2 R0, R1;
+            if (pdt < tlen) {
+              A = tab[(size_t)pdt * 4 + 2];
+              Bv = tab[(size_t)pdt * 4 + 3];
+              R0 = T->rtab[(size_t)pdt * 4 + 2];
+              R1 = T->rtab[(size_t)pdt * 4 + 3];
+            } else {
+              table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
+              recip_part(A, Bv, 2, R0, R1);
+            }
+            /* zi becomes zi*exp(-kzi*pdt) */
+            const float4 rv = row_step_nl(make_float4(pi, V.ei[sl], s_zi[t], 0.0f), T, A, Bv, R0, R1);
+            pi = rv.x;
+            V.pi[sl] = rv.x;
+            V.ei[sl] = rv.y;
+            V.zi[sl] = rv.z + J.kfti;
+          }
+          V.ti[sl] = simstep;
+          s_pi[t] = pi;
+        }
+        for (int c = tid; c < nr * M; c += blockDim.x) {
+          const int rr = c / M, j = c - rr * M;
+          const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
+          float4 c4 = J.cell[index];
+          const uint32_t hist = r_hist[j];
+          replay_cell_hist(c4, s_ti[rr], s_zi[rr], simstep, hist, B, k, tab, tlen, T, J.kftj);
+          if (hist & 1u) c4.w += J.kftj;
+          J.cell[index] = c4;
+          s_w[c] = c4.x;
+        }
+        __syncthreads();
+        MPROBE(6);
+        for (int c = tid; c < nr * M; c += blockDim.x) {
+          const int rr = c / M, j = c - rr * M;
+          const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
+          float w;
+          if (kp != 0.0f) {
+            w = J.wgain * bx_logf((s_w[c] + J.eps2) / ((s_pi[rr] + J.eps) * (V.pj[j] + J.eps)));
+            J.wij[index] = w;
+          } else {
+            w = J.wij[index];
+          }
+          s_w[c] = w;
+        }
+        __syncthreads();
+        MPROBE(7);
+        for (int j = tid; j < M; j += blockDim.x) {
+          float e = V.epsc[j];
+          for (int rr = 0; rr < nr; ++rr) e += s_w[rr * M + j];
+          V.epsc[j] = e;
+        }
+        __syncthreads();
+        MPROBE(8);
+      }
+      if (tid == 0) {
+        uint32_t f = 0;
+        if (s_flag9) f |= 1;
+        if (h == 9 / M && 9 < n && (r_hist[9 - h * M] & 1u)) f |= 2;
+        if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + s_inp[q]], f);
+        atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
+      }
+    }
+  }
+
+  /* ---- write the resident state back: the last tick's buffers ---- */
+  __syncthreads();
+  if (it > it0) {
+    const int last = it - 1;
+    const int curL = (rp->k0 + last) & 1;
+    const int lpn = ((last - it0) & 1) ^ 1; /* the list the next tick reads */
+    for (int j = tid; j < M; j += blockDim.x) {
+      const int idx = h * M + j;
+      pop.dsup[curL][idx] = r_dsup[j];
+      pop.ada[idx] = r_ada[j];
+      pop.act[idx] = r_act[j];
+      pop.counter[idx] = r_cnt[j];
+    }
+    for (int q = 0; q < n_in; ++q) {
+      const ProjDev& J = s_proj[q];
+      const int C = J.C;
+      const ResQ V = res_q(sm, L, q, M, C);
+      const size_t eoff = (size_t)J.proj_in_pop * n;
+      for (int j = tid; j < M; j += blockDim.x) {
+        const int idx = h * M + j;
+        J.pj[idx] = V.pj[j];
+        J.ej[idx] = V.ej[j];
+        J.zj[idx] = V.zj[j];
+        pop.epsc[curL][eoff + idx] = V.epsc[j];
+        pop.bj[curL][eoff + idx] = V.bj[j];
+      }
+      for (int s = tid; s < C; s += blockDim.x) {
+        const int r = h * C + s;
+        J.qi[r] = V.qi[s];
+        J.pi[r] = V.pi[s];
+        J.ei[r] = V.ei[s];
+        J.zi[r] = V.zi[s];
+        J.ti[r] = V.ti[s];
+      }
+      const int cnt = s_nlist[q][lpn];
+      for (int e = tid; e < cnt; e += blockDim.x) J.list[h * C + e] = h * C + V.list[lpn * C + e];
+      if (tid == 0) J.list_cnt[h] = cnt;
+    }
+  }
+#ifdef BCPNN_PHASE_PROBE
+  __syncthreads();
+  if (tid < kProbeSlots && blockIdx.x < kProbeCtas)
+    atomicAdd(&g_phase_probe[blockIdx.x * kProbeSlots + tid], g_probe_smem[tid]);
 #endif
 }
 

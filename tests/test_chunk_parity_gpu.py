@@ -101,7 +101,7 @@ def test_row_chunks_overflow_procupdlazy(mode):
         gpu.close()
 
 
-@pytest.mark.parametrize("per_tick", [False, True])
+@pytest.mark.parametrize("per_tick", [False, True, "global"])
 def test_row_chunks_overflow_procupdmulti(per_tick):
     H, S = 64, 60
     pops, projs, ii, di, rng = network(H, S, seed=4)

@@ -150,7 +150,7 @@ def test_edge_parity_procupdlazy(case, mode):
         gpu.close()
 
 
-@pytest.mark.parametrize("per_tick", [False, True])
+@pytest.mark.parametrize("per_tick", [False, True, "global"])
 def test_sparse_slots_procupdmulti(per_tick):
     rng = np.random.default_rng(7)
     pops, projs, conn, _ = sparse_case(rng)

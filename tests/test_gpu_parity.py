@@ -21,19 +21,24 @@ pytestmark = pytest.mark.gpu
 def gpu_net(*args, per_tick=False, **kw):
     """a capi.Net on the persistent cooperative path (default) or on the
     one-launch-per-tick path; per_tick="t256" is the persistent path with
-    256-thread CTAs"""
-    old = os.environ.get("GSBN_PER_TICK")
+    256-thread CTAs, per_tick="global" (ProcUpdMulti) the persistent launch
+    that keeps the HCU state in global memory instead of shared memory"""
+    saved = {k: os.environ.get(k) for k in ("GSBN_PER_TICK", "GSBN_MULTI_RESIDENT")}
     if per_tick == "t256":
         kw["tick_threads"] = 256
+        per_tick = False
+    os.environ["GSBN_MULTI_RESIDENT"] = "0" if per_tick == "global" else "1"
+    if per_tick == "global":
         per_tick = False
     os.environ["GSBN_PER_TICK"] = "1" if per_tick else "0"
     try:
         return capi.Net(*args, **kw)
     finally:
-        if old is None:
-            del os.environ["GSBN_PER_TICK"]
-        else:
-            os.environ["GSBN_PER_TICK"] = old
+        for k, v in saved.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 @pytest.fixture(params=["persistent", "per_tick", "t256"])

@@ -23,9 +23,11 @@ def lginp_row(row, pops, eps):
     return np.array([hit if row[h] == m else miss for h in range(H) for m in range(M)], np.float32)
 
 
-@pytest.mark.parametrize("ring,per_tick", [(25, False), (25, True), (1, False)])
+@pytest.mark.parametrize("ring,per_tick", [(25, False), (25, True), (25, "global"), (1, False), (40, False)])
 def test_multi_matches_oracle(tmp_path, ring, per_tick):
-    """persistent launch (one per run) and one launch per tick"""
+    """persistent launch (one per run; with the HCU state in shared memory,
+    or in global memory with "global" and for rings longer than 32 ticks)
+    and one launch per tick"""
     w = workloads.config0()
     sp, _ = w.solver_param(str(tmp_path))
     pops, projs = workloads.net_from_solver_param(sp)
