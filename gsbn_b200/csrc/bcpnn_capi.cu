@@ -50,8 +50,12 @@ __global__ void __launch_bounds__(kProjThreads, 1) res_tick_kernel(const NetDev*
                                                                   const RunParams* __restrict__ rp, int it0,
                                                                   int n_ticks, unsigned int* bar) {
   __shared__ int s_ok;
-  res_tick_loop(net, rp, it0, n_ticks,
-                [&](int k) { return t512::grid_sync(bar, (unsigned int)k * gridDim.x, net->err, &s_ok); });
+  __shared__ float s_unused;
+  res_tick_loop(
+      net, rp, it0, n_ticks, [&]() { t512::grid_arrive(bar); },
+      [&](int k) {
+        return t512::grid_wait(bar, (unsigned int)k * gridDim.x, net->err, &s_ok, nullptr, 0u, &s_unused);
+      });
 }
 }  // namespace multi
 }  // namespace bcpnn

@@ -578,7 +578,7 @@ __device__ __forceinline__ void named_sync(int id, int n) {
 
 /* word offsets of the resident layout in dynamic shared memory */
 struct ResLayout {
-  int dsup, ada, act, cnt, lg, hist, spk; /* population, [M] (spk: bytes) */
+  int dsup, ada, act, cnt, lg, hist, u, up, spk; /* population, [M] (spk: bytes) */
   int w, rpi, rti, rzi;                   /* row-chunk scratch            */
   int qmask;                              /* delay-queue ballots          */
   int q[kMaxIn];                          /* incoming projection blocks   */
@@ -591,12 +591,15 @@ __host__ __device__ inline int res_qwords(int M, int C) { return 5 * M + 9 * C; 
 
 __host__ __device__ inline void res_layout(int M, int n_in, const int* C, ResLayout& L) {
   int o = 0;
-  L.dsup = o; o += M;
-  L.ada = o; o += M;
-  L.act = o; o += M;
-  L.cnt = o; o += M;
-  L.lg = o; o += M;
-  L.hist = o; o += M;
+  const int M4 = (M + 3) & ~3; /* population arrays start on 16-byte boundaries */
+  L.dsup = o; o += M4;
+  L.ada = o; o += M4;
+  L.act = o; o += M4;
+  L.cnt = o; o += M4;
+  L.lg = o; o += M4;
+  L.hist = o; o += M4;
+  L.u = o; o += M4;
+  L.up = o; o += M4;
   L.spk = o; o += (M + 3) / 4;
   const int rch = row_chunk(M);
   L.w = o; o += kRowCells;
@@ -647,9 +650,23 @@ __device__ __forceinline__ ResQ res_q(float* sm, const ResLayout& L, int q, int 
   return v;
 }
 
-template <typename GridSync>
+/* uniforms of one tick's spike sampling for the HCU's MCUs (they depend on
+   the tick and the MCU only), drawn ahead by threads tid, tid + nth, ... */
+__device__ __forceinline__ void res_draw(const PopDev& pop, bool poisson, int simstep, int h, float* r_u, float* r_up,
+                                         int tid, int nth) {
+  for (int j = tid; j < pop.M; j += nth) {
+    const uint32_t idx = (uint32_t)(h * pop.M + j);
+    r_u[j] = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, idx);
+    r_up[j] = poisson ? bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, idx) : 1.0f;
+  }
+}
+
+/* arrive(): this CTA's arrival at the grid barrier after a tick (all its
+   writes of the tick made); wait(k): the wait for every CTA's k-th arrival,
+   false when it gave up */
+template <typename Arrive, typename Wait>
 __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, const RunParams* __restrict__ rp,
-                                              int it0, int n_ticks, GridSync sync) {
+                                              int it0, int n_ticks, Arrive arrive, Wait wait) {
   extern __shared__ __align__(16) float sm[];
   /* descriptors, copied once per launch: every tick reads them in chains */
   __shared__ PopDev s_pop;
@@ -698,7 +715,10 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
   int* r_cnt = (int*)(sm + L.cnt);
   float* r_lg = sm + L.lg;
   uint32_t* r_hist = (uint32_t*)(sm + L.hist);
+  float* r_u = sm + L.u;
+  float* r_up = sm + L.up;
   int8_t* r_spk = (int8_t*)(sm + L.spk);
+  const bool poisson = net->poisson_hz > 0.0f;
   float* s_w = sm + L.w;
   float* s_pi = sm + L.rpi;
   int* s_ti = (int*)(sm + L.rti);
@@ -752,6 +772,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       for (int e = tid; e < cnt; e += blockDim.x) V.list[e] = J.list[h * C + e] - h * C;
       if (tid == 0) s_nlist[q][0] = cnt;
     }
+    res_draw(pop, poisson, s0, h, r_u, r_up, tid, blockDim.x);
   }
   __syncthreads();
 #ifdef BCPNN_PHASE_PROBE
@@ -766,7 +787,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
 
   int it = it0;
   for (; it < it0 + n_ticks; ++it) {
-    if (it > it0 && !sync(it - it0)) break;
+    if (it > it0 && !wait(it - it0)) break;
     MPROBE(0);
 #ifdef BCPNN_PHASE_PROBE
     if (tid == 0) g_probe_smem[kProbeTicks] += 1;
@@ -820,8 +841,17 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       MPROBE(2);
       if (tid == 0) {
         float vsum = 0.0f;
+        const float4* a4 = (const float4*)r_act;
+        int m = 0;
 #pragma unroll 4
-        for (int m = 0; m < M; ++m) vsum += r_act[m];
+        for (; m + 4 <= M; m += 4) {
+          const float4 v = a4[m >> 2];
+          vsum += v.x;
+          vsum += v.y;
+          vsum += v.z;
+          vsum += v.w;
+        }
+        for (; m < M; ++m) vsum += r_act[m];
         s_vsum = vsum;
       }
       named_sync(kBarPop, G);
@@ -829,16 +859,11 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       const float vsum = s_vsum;
       const float pr = net->poisson_hz * net->dt;
       for (int j = tid; j < M; j += G) {
-        const int idx = h * M + j;
         float a = r_act[j];
         if (vsum > 1.0f) a /= vsum;
         r_act[j] = a;
-        const float u = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
-        int8_t spk = (int8_t)(u < a * pop.maxfqdt);
-        if (net->poisson_hz > 0.0f) {
-          const float up = bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
-          if (up < pr) spk = 1;
-        }
+        int8_t spk = (int8_t)(r_u[j] < a * pop.maxfqdt); /* uniforms drawn before the tick */
+        if (poisson && r_up[j] < pr) spk = 1;
         r_cnt[j] += spk;
         r_ada[j] += (pop.adgain * a - r_ada[j]) * pop.tauadt;
         r_spk[j] = spk;
@@ -933,7 +958,17 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
           base += __popc(mb);
         }
         if (qw == kResQueueWarps - 1 && lane == 0) s_nlist[q][nq] = base;
-        named_sync(kBarQueue, 32 * kResQueueWarps); /* s_qmask and s_qcnt are reused */
+        named_sync(kBarQueue, 32 * kResQueueWarps); /* s_qmask and s_qcnt are reused; the list is complete */
+        /* the cells of the next tick's rows, into L2 ahead of their loads */
+        const int nnext = s_nlist[q][nq];
+        const int lines = (M * 16 + 127) / 128 + 1; /* a row's cells, not 128-byte aligned */
+        for (int e = qt; e < nnext * lines; e += 32 * kResQueueWarps) {
+          const int rr = e / lines, ln = e - rr * lines;
+          const char* row = (const char*)(J.cell + (size_t)(h * C + out[rr]) * M);
+          const char* end = row + (size_t)M * 16;
+          const char* a = (const char*)((uintptr_t)row & ~(uintptr_t)127) + (size_t)ln * 128;
+          if (a < end) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+        }
       }
     }
     __syncthreads();
@@ -1046,6 +1081,13 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + s_inp[q]], f);
         atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
       }
+    }
+    /* every write of this tick is made: arrive, and draw the next tick's
+       uniforms while the other CTAs arrive */
+    if (it + 1 < it0 + n_ticks) {
+      __syncthreads();
+      arrive();
+      res_draw(pop, poisson, simstep + 1, h, r_u, r_up, tid, blockDim.x);
     }
   }
 
