@@ -150,7 +150,6 @@ struct TickLayout {
   int stg_row, stg_ti;           /* [rows] int                                             */
   int stg_tv, stg_wv;            /* [kRowChunkCells] int / float                           */
   int w_dsup, w_act, w_spkl, w_pi, w_w, w_lg;
-  int w_u, w_up;                 /* [M] the tick's sampling uniforms, drawn ahead */
   int w_spkp;                    /* [2][M] int: spike lists by tick parity (deferred columns) */
   int w_spk, w_skip;             /* bytes                                                  */
   int st_dsup, st_act, st_cnt;
@@ -185,8 +184,6 @@ __host__ __device__ inline void tick_layout(int M, int n_in, const int* C, TickL
   L.stg_wv = o; o += kRowChunkCells;
   L.w_dsup = o; o += M;
   L.w_lg = o; o += M;
-  L.w_u = o; o += M;
-  L.w_up = o; o += M;
   L.w_act = o; o += M;
   L.w_spkl = o; o += M;
   L.w_pi = o; o += rows;
@@ -649,19 +646,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
   int* w_spkp = (int*)(sm + L.w_spkp);
   int8_t* w_skip = (int8_t*)(sm + L.w_skip);
   float* w_lgc = sm + L.w_lg;
-  float* w_u = sm + L.w_u;
-  float* w_up = sm + L.w_up;
-  const bool poisson = net->poisson_hz > 0.0f;
-  /* the uniforms of a tick's spike sampling depend on the tick and the MCU
-     only: drawn ahead, for the launch's first tick here and for each next
-     tick by group B before the groups join */
-  auto draw = [&](int simstep_of, int t, int nth) {
-    for (int j = t; j < M; j += nth) {
-      const uint32_t idx = (uint32_t)(h * M + j);
-      w_u[j] = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep_of, idx);
-      w_up[j] = poisson ? bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep_of, idx) : 1.0f;
-    }
-  };
   float* st_dsup = sm + L.st_dsup;
   float* st_act = sm + L.st_act;
   int* st_cnt = (int*)(sm + L.st_cnt);
@@ -701,7 +685,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
     }
     /* the run's stimulus of this HCU (constant within the launch) */
     for (int j = tid; j < M; j += kBlock) w_lgc[j] = rp->lginp[pop.mcu_start + h * M + j];
-    draw(rp->simstep0 + it0, tid, kBlock);
     if (tid == 0) {
       s_rows_acc = 0;
       s_cols_acc = 0;
@@ -832,12 +815,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
       const float vsum = s_vsum;
       const float pr = net->poisson_hz * net->dt;
       for (int j = gtid; j < M; j += kGroup) {
+        int idx = h * M + j;
         float a = w_act[j];
         if (vsum > 1.0f) a /= vsum;
         st_act[j] = a;
         st_dsup[j] = w_dsup[j];
-        int8_t spk = (int8_t)(w_u[j] < a * pop.maxfqdt);
-        if (poisson && w_up[j] < pr) spk = 1;
+        float u = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+        int8_t spk = (int8_t)(u < a * pop.maxfqdt);
+        if (net->poisson_hz > 0.0f) {
+          float up = bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)simstep, (uint32_t)idx);
+          if (up < pr) spk = 1;
+        }
         st_cnt[j] += spk;
         w_spk[j] = spk;
       }
@@ -1332,9 +1320,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tick_kernel(const NetDev* 
         }
       }
     }
-    /* group B: the next tick's uniforms (group A read this tick's before the
-       spike hand-over) */
-    if (!groupA && it + 1 < it0 + n_ticks) draw(simstep + 1, gtid, kGroup);
     PROBE(13);
     __syncthreads();
     PROBE(8);
