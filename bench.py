@@ -593,8 +593,8 @@ def run_recall_extension(dev, steps, warmup, replicates=4096, ticks=200, plain_s
 def run_multi_extension(dev, steps, warmup, ring=25, cpu=True):
     """ProcUpdMulti (row-only updates replaying a ring of postsynaptic spikes,
     adaptation) on the 100x100 density-0.1 workload with gsbn's spike buffer
-    size 25: the same 200-segment step as the headline, one population launch
-    and one projection launch per tick (CUDA graph per run)."""
+    size 25: the same 200-segment step as the headline, one persistent launch
+    per run (the resident form: each HCU's state in shared memory)."""
     import torch
     from gsbn_b200 import capi, extgen
     work = tempfile.mkdtemp(prefix="gsbn_multi_")
