@@ -43,7 +43,8 @@ __host__ __device__ inline int row_chunk(int M) { return M >= kRowCells ? 1 : kR
    0 barrier wait, 1 support, 2 softmax maximum and exponentials, 3 softmax
    sum, 4 spikes, 5 j-traces and row list, 6 row traces and cell replays,
    7 weights, 8 epsc sums, 9 delay queue, 10 (resident launch) wait for the
-   delay-queue warps; kProbeTicks counts the ticks */
+   delay-queue warps, 11 (resident launch) staging of the next tick's first
+   row chunk after the barrier arrival; kProbeTicks counts the ticks */
 #ifdef BCPNN_PHASE_PROBE
 #define MPROBE(slot)                                                   \
   do {                                                                 \
@@ -578,6 +579,7 @@ __device__ __forceinline__ void named_sync(int id, int n) {
 
 /* word offsets of the resident layout in dynamic shared memory */
 struct ResLayout {
+  int stc;                                 /* [kRowCells] float4: staged cells */
   int dsup, ada, act, cnt, lg, hist, u, up, spk; /* population, [M] (spk: bytes) */
   int w, rpi, rti, rzi;                   /* row-chunk scratch            */
   int qmask;                              /* delay-queue ballots          */
@@ -591,6 +593,7 @@ __host__ __device__ inline int res_qwords(int M, int C) { return 5 * M + 9 * C; 
 
 __host__ __device__ inline void res_layout(int M, int n_in, const int* C, ResLayout& L) {
   int o = 0;
+  L.stc = o; o += 4 * kRowCells;
   const int M4 = (M + 3) & ~3; /* population arrays start on 16-byte boundaries */
   L.dsup = o; o += M4;
   L.ada = o; o += M4;
@@ -680,6 +683,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
   __shared__ float s_red[32];
   __shared__ float s_vsum, s_wm;
   __shared__ int s_flag9;
+  __shared__ int s_staged; /* rows of projection 0's first chunk staged for this tick, or -1 */
 
   const int tid = threadIdx.x;
   const int P = net->cta_pop[blockIdx.x];
@@ -719,6 +723,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
   float* r_up = sm + L.up;
   int8_t* r_spk = (int8_t*)(sm + L.spk);
   const bool poisson = net->poisson_hz > 0.0f;
+  float4* st_c4 = (float4*)(sm + L.stc);
   float* s_w = sm + L.w;
   float* s_pi = sm + L.rpi;
   int* s_ti = (int*)(sm + L.rti);
@@ -773,6 +778,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       if (tid == 0) s_nlist[q][0] = cnt;
     }
     res_draw(pop, poisson, s0, h, r_u, r_up, tid, blockDim.x);
+    if (tid == 0) s_staged = -1;
   }
   __syncthreads();
 #ifdef BCPNN_PHASE_PROBE
@@ -1005,6 +1011,23 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       MPROBE(5);
       for (int base = 0; base < nrow; base += rch) {
         const int nr = (nrow - base) < rch ? (nrow - base) : rch;
+        if (q == 0 && base == 0 && s_staged == nr) {
+          /* staged after the previous tick's barrier arrival: the row
+             traces are up to date, the cells replayed and decayed to this
+             tick; what is left is a spike now */
+          for (int t = tid; t < nr; t += blockDim.x)
+            if (h * C + list[t] == 9) s_flag9 = 1;
+          for (int c = tid; c < nr * M; c += blockDim.x) {
+            const int rr = c / M, j = c - rr * M;
+            const size_t index = (size_t)(h * C + list[rr]) * M + j;
+            float4 c4 = st_c4[c];
+            if (r_hist[j] & 1u) c4.w += J.kftj;
+            J.cell[index] = c4;
+            s_w[c] = c4.x;
+          }
+          __syncthreads();
+          MPROBE(6);
+        } else {
         for (int t = tid; t < nr; t += blockDim.x) {
           const int sl = list[base + t];
           s_ti[t] = V.ti[sl];
@@ -1052,6 +1075,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         }
         __syncthreads();
         MPROBE(6);
+        }
         for (int c = tid; c < nr * M; c += blockDim.x) {
           const int rr = c / M, j = c - rr * M;
           const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
@@ -1088,6 +1112,67 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       __syncthreads();
       arrive();
       res_draw(pop, poisson, simstep + 1, h, r_u, r_up, tid, blockDim.x);
+      /* stage the next tick's first row chunk of projection 0: its rows
+         (listed by this tick's delay queue) and their cells change only in
+         their own row update, so their row traces and their cells' replays
+         and decays to the next tick can run now, while the other CTAs
+         arrive; the next tick adds a spike now and writes the cells */
+      if (n_in > 0) {
+        const ProjDev& J = s_proj[0];
+        const TabRef* T = &s_tab[0];
+        const int C = J.C;
+        const ResQ V = res_q(sm, L, 0, M, C);
+        const float kp = J.taupdt * rp->prn;
+        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+        const float4* tab = T->tab;
+        const int tlen = T->len;
+        const int ts = simstep + 1;
+        const int* nl = V.list + (lp ^ 1) * C;
+        const int nrow1 = s_nlist[0][lp ^ 1];
+        const int nr = nrow1 < rch ? nrow1 : rch;
+        for (int t = tid; t < nr; t += blockDim.x) {
+          const int sl = nl[t];
+          s_ti[t] = V.ti[sl];
+          s_zi[t] = V.zi[sl];
+        }
+        __syncthreads();
+        for (int t = blockDim.x - 1 - tid; t < nr; t += blockDim.x) {
+          const int sl = nl[t];
+          const int pdt = ts - s_ti[t];
+          float pi = V.pi[sl];
+          if (pdt > 0) {
+            float4 A, Bv;
+            double2 R0, R1;
+            if (pdt < tlen) {
+              A = tab[(size_t)pdt * 4 + 2];
+              Bv = tab[(size_t)pdt * 4 + 3];
+              R0 = T->rtab[(size_t)pdt * 4 + 2];
+              R1 = T->rtab[(size_t)pdt * 4 + 3];
+            } else {
+              table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
+              recip_part(A, Bv, 2, R0, R1);
+            }
+            /* zi becomes zi*exp(-kzi*pdt) */
+            const float4 rv = row_step_nl(make_float4(pi, V.ei[sl], s_zi[t], 0.0f), T, A, Bv, R0, R1);
+            pi = rv.x;
+            V.pi[sl] = rv.x;
+            V.ei[sl] = rv.y;
+            V.zi[sl] = rv.z + J.kfti;
+          }
+          V.ti[sl] = ts;
+          s_pi[t] = pi;
+        }
+        for (int c = tid; c < nr * M; c += blockDim.x) {
+          const int rr = c / M, j = c - rr * M;
+          float4 c4 = J.cell[(size_t)(h * C + nl[rr]) * M + j];
+          /* bit b + 1 of the shifted history is tick ts - 1 - b; bit 0 (the
+             next tick's own spike) is not replayed */
+          replay_cell_hist(c4, s_ti[rr], s_zi[rr], ts, r_hist[j] << 1, B, k, tab, tlen, T, J.kftj);
+          st_c4[c] = c4;
+        }
+        if (tid == 0) s_staged = nr;
+      }
+      MPROBE(11);
     }
   }
 

@@ -36,7 +36,8 @@ PHASES_B = {16: "barrier wait", 26: "column units of the grid", 19: "  units: ri
             24: "join wait", 25: "staging next chunk"}
 PHASES_MULTI = {0: "barrier wait", 1: "support", 2: "softmax: max, exp", 3: "softmax: sum", 4: "spikes",
                 5: "j-traces, row list", 6: "row traces, cell replays", 7: "weights", 8: "epsc sums",
-                9: "delay queue", 10: "wait for the delay-queue warps"}
+                9: "delay queue", 10: "wait for the delay-queue warps",
+                11: "staging next rows (after arrival)"}
 
 
 def main():
