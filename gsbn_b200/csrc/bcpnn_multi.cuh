@@ -1111,7 +1111,16 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
     if (it + 1 < it0 + n_ticks) {
       __syncthreads();
       arrive();
-      res_draw(pop, poisson, simstep + 1, h, r_u, r_up, tid, blockDim.x);
+      /* the uniforms by threads 256 up (MCU (tid + 256) mod 512): the staging
+         below takes its cells from thread 0 up and its rows from the top */
+      {
+        const int j = (tid + kProjThreads / 2) & (kProjThreads - 1);
+        if (j < M) {
+          const uint32_t idx = (uint32_t)(h * M + j);
+          r_u[j] = bx_uniform01(pop.rng_seed, pop.rng_pop, (uint32_t)(simstep + 1), idx);
+          r_up[j] = poisson ? bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)(simstep + 1), idx) : 1.0f;
+        }
+      }
       /* stage the next tick's first row chunk of projection 0: its rows
          (listed by this tick's delay queue) and their cells change only in
          their own row update, so their row traces and their cells' replays
