@@ -23,7 +23,7 @@ gsbn's closed-form decays divide by their differences.
 Each case runs training segments and then recall segments (prn changes, so
 the all-cells catch-up runs), compares the spikes of every tick and, at the
 end, every state vector by bit pattern and the cell-update counters with the
-oracle using the shared exp/log; the sparse case also runs through the
+oracle using the shared exp/log; every case also runs through the
 ProcUpdMulti variant against its compiled restatement.
 """
 import numpy as np
@@ -151,27 +151,37 @@ def test_edge_parity_procupdlazy(case, mode):
 
 
 @pytest.mark.parametrize("per_tick", [False, True, "global"])
-def test_sparse_slots_procupdmulti(per_tick):
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_edge_parity_procupdmulti(case, per_tick):
+    """the same cases through the ProcUpdMulti variant (spike ring of 32
+    ticks, adaptation on; without Poisson input noise, which the variant's
+    restatement does not draw): the resident persistent launch (False), the
+    persistent launch with the state in global memory, one launch per tick"""
     rng = np.random.default_rng(7)
-    pops, projs, conn, _ = sparse_case(rng)
+    pops, projs, conn, _ = CASES[case](rng)
     for p in pops:
         p.update(taua=0.05, adgain=1.0)
     orc = multi.MultiNetC(pops, projs, DT, seed=9, spike_buffer=32)
     gpu = gpu_net(pops, projs, DT, seed=9, max_ticks=64, variant=1, spike_buffer=32, per_tick=per_tick)
     try:
-        orc.set_conn(0, *conn[0])
-        gpu.set_conn(0, *conn[0])
+        for q, (ii, di) in enumerate(conn):
+            orc.set_conn(q, ii, di)
+            gpu.set_conn(q, ii, di)
         spikes = 0
         for first, n, prn, old_prn, lg, wm in runs_of(pops, rng):
             orc.set_stimulus(lg, wm)
             gpu.set_stimulus(lg, wm)
             want = orc.run(first, n, prn, old_prn)
             gpu.run(first, n, prn, old_prn)
-            got = gpu.spike_log(0)
-            assert np.array_equal(got, want[0]), f"spikes differ in the run at {first}"
-            spikes += int(np.unpackbits(got.view(np.uint8)).sum())
+            for p in range(len(pops)):
+                got = gpu.spike_log(p)
+                assert np.array_equal(got, want[p]), f"pop {p}: spikes differ in the run at {first}"
+                spikes += int(np.unpackbits(got.view(np.uint8)).sum())
         assert spikes > 100, spikes
-        for name in ARRAYS:
+        names = [f"{k}_{p}" for p in range(len(pops)) for k in ("dsup", "act", "ada", ".counter", "epsc", "bj")]
+        names += [f"{k}_{q}" for q in range(len(projs))
+                  for k in ("pi", "ei", "zi", "ti", "pj", "ej", "zj", "pij", "eij", "zj2", "wij", "qi")]
+        for name in names:
             a, b = gpu.read(name), orc.read(name)
             b = np.asarray(b).astype(a.dtype)
             assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), name
