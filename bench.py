@@ -234,17 +234,17 @@ def run_ours(args, rank, world, local_rank, cpu=False):
     ms, cells = combine_over_ranks(ms, cells, f"cuda:{dev}")
 
     # e2e: host buffers through the C ABI, every segment's spike log read back
-    # (ProcSpkRec's input) and ProcCheck's recall counted on the device.  Each
-    # segment's stimulus row, spike-log copy and recall result are queued on
-    # the library stream behind its run; one sync per step.
-    pin_lg = [torch.empty(lgidx.shape[1], dtype=torch.int32, pin_memory=True).numpy() for r in runs]
-    pin_wm = [torch.empty(wmask.shape[1], dtype=torch.float32, pin_memory=True).numpy() for r in runs]
-    for i, r in enumerate(runs):
-        pin_lg[i][:] = lgidx[r.lgidx]
-        pin_wm[i][:] = wmask[r.wmask]
+    # (ProcSpkRec's input) and ProcCheck's recall counted on the device.  The
+    # step's stimulus tables (ProcExtGen's pattern-index and mask rows) are
+    # copied from page-locked memory at the start of every step; each
+    # segment's row selection, run, spike-log copy and recall result are
+    # queued on the library stream; one sync per step.
+    pin_lg = torch.empty(lgidx.shape, dtype=torch.int32, pin_memory=True).numpy()
+    pin_wm = torch.empty(wmask.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pin_lg[:], pin_wm[:] = lgidx, wmask
     words = (pops[0]["hcu_num"] * pops[0]["mcu_num"] + 31) // 32
     pin_log = [torch.empty((r.n, words), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32) for r in runs]
-    h2d = sum(a.nbytes + b.nbytes for a, b in zip(pin_lg, pin_wm))
+    h2d = pin_lg.nbytes + pin_wm.nbytes
     d2h = sum(a.nbytes for a in pin_log)
     lib = capi.load()
 
@@ -255,9 +255,10 @@ def run_ours(args, rank, world, local_rank, cpu=False):
     def e2e_step():
         net.reset()
         check.reset()
+        net._check(lib.bcpnn_upload_stimuli_idx_async(net._h, pin_lg.shape[0], capi._ptr(pin_lg), eps,
+                                                      pin_wm.shape[0], capi._ptr(pin_wm)))
         for i, r in enumerate(runs):
-            net._check(lib.bcpnn_set_stimulus_idx(net._h, capi._ptr(pin_lg[i]), pin_lg[i].size, eps,
-                                                  capi._ptr(pin_wm[i]), pin_wm[i].size))
+            net._check(lib.bcpnn_use_stimulus(net._h, r.lgidx, r.wmask))
             net.run(r.first, r.n, r.prn, r.old_prn)
             net._check(lib.bcpnn_get_spike_log_async(net._h, 0, capi._ptr(pin_log[i]), pin_log[i].size))
             check.after_run(r)

@@ -20,7 +20,7 @@ _NP = {F32: np.float32, I32: np.int32, I8: np.int8}
 # every entry point declared in include/bcpnn.h
 EXPORTS = (
     "bcpnn_net_create", "bcpnn_net_destroy", "bcpnn_set_conn", "bcpnn_set_stimulus", "bcpnn_upload_stimuli",
-    "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
+    "bcpnn_use_stimulus", "bcpnn_set_stimulus_idx", "bcpnn_upload_stimuli_idx", "bcpnn_upload_stimuli_idx_async", "bcpnn_set_ext_spikes", "bcpnn_reset", "bcpnn_get_stream",
     "bcpnn_run", "bcpnn_sync", "bcpnn_spike_log_words", "bcpnn_get_spike_log", "bcpnn_get_spike_log_async", "bcpnn_check_count",
     "bcpnn_check_result_async", "bcpnn_get_ss_flags",
     "bcpnn_state_info", "bcpnn_read_state", "bcpnn_write_state", "bcpnn_read_state_noalloc", "bcpnn_counters", "bcpnn_kernel_launches",
@@ -81,6 +81,7 @@ def load():
         "bcpnn_use_stimulus": (ctypes.c_int, [vp, i32, i32]),
         "bcpnn_set_stimulus_idx": (ctypes.c_int, [vp, vp, sz, ctypes.c_float, vp, sz]),
         "bcpnn_upload_stimuli_idx": (ctypes.c_int, [vp, i32, vp, ctypes.c_float, i32, vp]),
+        "bcpnn_upload_stimuli_idx_async": (ctypes.c_int, [vp, i32, vp, ctypes.c_float, i32, vp]),
         "bcpnn_set_ext_spikes": (ctypes.c_int, [vp, i32, i32, vp, vp, vp]),
         "bcpnn_reset": (ctypes.c_int, [vp]),
         "bcpnn_get_stream": (ctypes.c_int, [vp, P(vp)]),
@@ -189,6 +190,17 @@ class Net:
         lg = np.ascontiguousarray(lgidx_rows, dtype=np.int32)
         wm = np.ascontiguousarray(wmask_rows, dtype=np.float32)
         self._check(self._lib.bcpnn_upload_stimuli_idx(self._h, lg.shape[0], _ptr(lg), eps, wm.shape[0], _ptr(wm)))
+
+    def upload_stimuli_idx_async(self, lgidx_rows, eps, wmask_rows):
+        """the tables of upload_stimuli_idx, queued on the network's stream;
+        page-locked arrays are read when the stream reaches the copies, so
+        the caller keeps them unchanged until sync()"""
+        lg = np.ascontiguousarray(lgidx_rows, dtype=np.int32)
+        wm = np.ascontiguousarray(wmask_rows, dtype=np.float32)
+        if lg.ndim != 2 or wm.ndim != 2:
+            raise ValueError("tables of rows expected")
+        self._check(self._lib.bcpnn_upload_stimuli_idx_async(self._h, lg.shape[0], _ptr(lg), eps, wm.shape[0],
+                                                             _ptr(wm)))
 
     def use_stimulus(self, lginp_row, wmask_row):
         self._check(self._lib.bcpnn_use_stimulus(self._h, lginp_row, wmask_row))

@@ -140,6 +140,9 @@ struct bcpnn_net {
   std::vector<int32_t*> check_out; /* per population: [2][H] idx, count of the last check */
   float* stim_wm = nullptr;
   int stim_lg_rows = 0, stim_wm_rows = 0;
+  int stim_lg_cap = 0, stim_wm_cap = 0; /* rows the stimulus tables have room for */
+  int32_t* d_lgidx_tab = nullptr;       /* pattern-index rows (bcpnn_upload_stimuli_idx_async) */
+  int lgidx_tab_cap = 0;
   const float* cur_lg = nullptr; /* stimulus of the next run */
   const float* cur_wm = nullptr;
   float* scratch = nullptr; /* staging for strided cell fields */
@@ -941,6 +944,7 @@ int bcpnn_net_destroy(bcpnn_net* net) {
   if (net->scratch) cudaFree(net->scratch);
   if (net->stim_lg) cudaFree(net->stim_lg);
   if (net->stim_wm) cudaFree(net->stim_wm);
+  if (net->d_lgidx_tab) cudaFree(net->d_lgidx_tab);
   if (net->stream) cudaStreamDestroy(net->stream);
   delete net;
   return BCPNN_OK;
@@ -992,8 +996,8 @@ int bcpnn_upload_stimuli(bcpnn_net* net, int32_t n_lginp_rows, const float* lgin
   CU(cudaMalloc((void**)&net->stim_wm, nw * sizeof(float)));
   CU(cudaMemcpy(net->stim_lg, lginp_rows, nl * sizeof(float), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(net->stim_wm, wmask_rows, nw * sizeof(float), cudaMemcpyHostToDevice));
-  net->stim_lg_rows = n_lginp_rows;
-  net->stim_wm_rows = n_wmask_rows;
+  net->stim_lg_rows = net->stim_lg_cap = n_lginp_rows;
+  net->stim_wm_rows = net->stim_wm_cap = n_wmask_rows;
   net->cur_lg = net->h.lginp;
   net->cur_wm = net->h.wmask;
   return BCPNN_OK;
@@ -1049,6 +1053,62 @@ int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hc
   CU(cudaGetLastError());
   net->launches += 1;
   CU(cudaMemcpyAsync(net->h.wmask, wmask_row, n_wmask * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+  net->cur_lg = net->h.lginp;
+  net->cur_wm = net->h.wmask;
+  return BCPNN_OK;
+}
+
+/* lginp of n pattern-index rows on the device: block (HCU, row), the values
+   of lginp_idx_kernel */
+__global__ void lginp_idx_rows_kernel(const NetDev* __restrict__ net, const int32_t* __restrict__ lgidx, int n_hcu,
+                                      int n_mcu, float hit, float miss, float* __restrict__ out) {
+  const PopDev& P = net->pops[net->cta_pop[blockIdx.x]];
+  const int h = net->cta_hcu[blockIdx.x];
+  const size_t r = blockIdx.y;
+  const int want = lgidx[r * n_hcu + P.hcu_start + h];
+  float* o = out + r * n_mcu + P.mcu_start + h * P.M;
+  for (int j = threadIdx.x; j < P.M; j += blockDim.x) o[j] = (want == j) ? hit : miss;
+}
+
+int bcpnn_upload_stimuli_idx_async(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
+                                   int32_t n_wmask_rows, const float* wmask_rows) {
+  if (!net) return BCPNN_ERR_INVALID;
+  if (n_lgidx_rows <= 0 || n_wmask_rows <= 0 || !lgidx_rows || !wmask_rows)
+    return fail(net, BCPNN_ERR_INVALID, "bcpnn_upload_stimuli_idx_async: empty tables");
+  if (n_lgidx_rows > 65535)
+    return fail(net, BCPNN_ERR_SIZE, "bcpnn_upload_stimuli_idx_async: at most 65535 pattern-index rows");
+  CU(cudaSetDevice(net->device));
+  const size_t H = (size_t)net->total_hcu, N = (size_t)net->total_mcu;
+  if (n_lgidx_rows > net->stim_lg_cap || n_wmask_rows > net->stim_wm_cap || n_lgidx_rows > net->lgidx_tab_cap) {
+    /* larger tables: runs queued earlier may still read the old ones */
+    CU(cudaStreamSynchronize(net->stream));
+    if (n_lgidx_rows > net->stim_lg_cap) {
+      if (net->stim_lg) { CU(cudaFree(net->stim_lg)); net->stim_lg = nullptr; net->stim_lg_cap = 0; }
+      CU(cudaMalloc((void**)&net->stim_lg, (size_t)n_lgidx_rows * N * sizeof(float)));
+      net->stim_lg_cap = n_lgidx_rows;
+    }
+    if (n_wmask_rows > net->stim_wm_cap) {
+      if (net->stim_wm) { CU(cudaFree(net->stim_wm)); net->stim_wm = nullptr; net->stim_wm_cap = 0; }
+      CU(cudaMalloc((void**)&net->stim_wm, (size_t)n_wmask_rows * H * sizeof(float)));
+      net->stim_wm_cap = n_wmask_rows;
+    }
+    if (n_lgidx_rows > net->lgidx_tab_cap) {
+      if (net->d_lgidx_tab) { CU(cudaFree(net->d_lgidx_tab)); net->d_lgidx_tab = nullptr; net->lgidx_tab_cap = 0; }
+      CU(cudaMalloc((void**)&net->d_lgidx_tab, (size_t)n_lgidx_rows * H * sizeof(int32_t)));
+      net->lgidx_tab_cap = n_lgidx_rows;
+    }
+  }
+  CU(cudaMemcpyAsync(net->d_lgidx_tab, lgidx_rows, (size_t)n_lgidx_rows * H * sizeof(int32_t),
+                     cudaMemcpyHostToDevice, net->stream));
+  lginp_idx_rows_kernel<<<dim3(net->total_hcu, n_lgidx_rows), 128, 0, net->stream>>>(
+      net->d_net, net->d_lgidx_tab, net->total_hcu, net->total_mcu, bx_extgen_logf(1 + eps), bx_extgen_logf(0 + eps),
+      net->stim_lg);
+  CU(cudaGetLastError());
+  net->launches += 1;
+  CU(cudaMemcpyAsync(net->stim_wm, wmask_rows, (size_t)n_wmask_rows * H * sizeof(float), cudaMemcpyHostToDevice,
+                     net->stream));
+  net->stim_lg_rows = n_lgidx_rows;
+  net->stim_wm_rows = n_wmask_rows;
   net->cur_lg = net->h.lginp;
   net->cur_wm = net->h.wmask;
   return BCPNN_OK;

@@ -146,6 +146,18 @@ int bcpnn_set_stimulus_idx(bcpnn_net* net, const int32_t* lgidx_row, size_t n_hc
 int bcpnn_upload_stimuli_idx(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
                              int32_t n_wmask_rows, const float* wmask_rows);
 
+/* bcpnn_upload_stimuli_idx queued on the network's stream without a wait,
+   for a caller that uploads a run schedule's tables once per pass (as
+   ProcExtGen reads its stimulus file once, ProcExtGen.cpp:57-103, and picks
+   rows per segment): the pattern-index and mask rows are copied from the
+   caller's buffers (page-locked: read when the stream reaches the copies, so
+   keep them unchanged until the next bcpnn_sync) and the lginp rows computed
+   on the device.  The device tables grow, with a wait and a device
+   allocation, only when a call has more rows than every earlier one; then
+   bcpnn_use_stimulus selects rows.  At most 65535 pattern-index rows. */
+int bcpnn_upload_stimuli_idx_async(bcpnn_net* net, int32_t n_lgidx_rows, const int32_t* lgidx_rows, float eps,
+                                   int32_t n_wmask_rows, const float* wmask_rows);
+
 /* External spike replay of one population (ProcUpdLazy args "external spike",
    ProcUpdLazy/Pop.cpp:67-110 and fill_spike :389-409): n entries, entry k
    overrides the spikes of tick ticks[k] with idx[offsets[k] .. offsets[k+1]);

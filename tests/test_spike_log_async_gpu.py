@@ -75,6 +75,58 @@ def test_stimulus_rows_from_indices_on_device(tmp_path):
 
 
 @pytest.mark.parametrize("make", ["config0", "config2"])
+def test_stimulus_tables_uploaded_async(tmp_path, make):
+    """bcpnn_upload_stimuli_idx_async, once per pass from page-locked tables,
+    then bcpnn_use_stimulus per segment, with no wait between: the same
+    spikes and end state as tables uploaded synchronously; a second pass
+    re-uploads into the tables (no growth), a third with an extra row grows
+    them."""
+    from gsbn_b200 import extgen
+    sp, pops, projs, stim, conn, seed, phz = load_workload(getattr(workloads, make)(), str(tmp_path))
+    lgidx, wmask = extgen.stim_tables(stim)
+    eps = float(np.float32(sp.gen_param.eps))
+    runs = extgen.segments(sp)[:30]
+    dt = float(np.float32(sp.gen_param.dt))
+    nets = [gpu_net(pops, projs, dt, seed=seed, poisson_hz=phz, max_ticks=256) for _ in range(2)]
+    words = (pops[0]["hcu_num"] * pops[0]["mcu_num"] + 31) // 32
+    try:
+        for net in nets:
+            for k, (ii, di) in enumerate(conn):
+                net.set_conn(k, ii, di)
+        nets[0].upload_stimuli_idx(lgidx, eps, wmask)
+        lg_pin = torch.zeros(lgidx.shape, dtype=torch.int32, pin_memory=True).numpy()
+        wm_pin = torch.zeros(wmask.shape, dtype=torch.float32, pin_memory=True).numpy()
+        lg_pin[:], wm_pin[:] = lgidx, wmask
+        logs = [torch.zeros((r.n, words), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32) for r in runs]
+        for extra in (0, 0, 1):
+            lg_t, wm_t = lg_pin, wm_pin
+            if extra:
+                lg_t = torch.zeros((lgidx.shape[0] + 1, lgidx.shape[1]), dtype=torch.int32, pin_memory=True).numpy()
+                wm_t = torch.zeros((wmask.shape[0] + 1, wmask.shape[1]), dtype=torch.float32, pin_memory=True).numpy()
+                lg_t[:-1], wm_t[:-1] = lgidx, wmask
+                lg_t[-1], wm_t[-1] = -1, 1.0
+            for net in nets:
+                net.reset()
+            nets[1].upload_stimuli_idx_async(lg_t, eps, wm_t)
+            want = []
+            for r, buf in zip(runs, logs):
+                for net in nets:
+                    net.use_stimulus(r.lgidx, r.wmask)
+                    net.run(r.first, r.n, r.prn, r.old_prn)
+                nets[1].spike_log_async(0, buf)
+                want.append(nets[0].spike_log(0))
+            nets[1].sync()
+            for k, (a, b) in enumerate(zip(logs, want)):
+                assert np.array_equal(a, b), (extra, k)
+            for name in ("dsup_0", "pij_0", "wij_0", "epsc_0"):
+                assert np.array_equal(nets[0].read(name).view(np.uint32), nets[1].read(name).view(np.uint32)), name
+        assert sum(int(np.unpackbits(a.view(np.uint8)).sum()) for a in logs) > 100
+    finally:
+        for net in nets:
+            net.close()
+
+
+@pytest.mark.parametrize("make", ["config0", "config2"])
 def test_recall_counters_on_device(tmp_path, make):
     """ProcCheck's counters on the device (extgen.DeviceCheck) must give the
     same (correct, evaluated) as the host evaluation of the spike logs, and
