@@ -110,6 +110,13 @@ struct bcpnn_net {
   int total_hcu = 0, total_mcu = 0, max_m = 1;
   int max_ticks = 0;
   uint32_t* log_buf = nullptr;
+  /* bcpnn_get_spike_log_async: the log is copied to one of two device
+     staging buffers on the network's stream, and from there to the host on
+     copy_stream, so the next run need not wait for the host copy */
+  cudaStream_t copy_stream = nullptr;
+  uint32_t* log_stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ready[2] = {nullptr, nullptr}, stage_free[2] = {nullptr, nullptr};
+  int stage_next = 0;
   size_t log_words_per_tick = 0;
   int64_t k_total = 0;      /* ticks executed since creation */
   uint32_t tick_serial = 1; /* tags of the softmax seeds (NetDev::seed64); never reset */
@@ -576,10 +583,17 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
   int rc = BCPNN_OK;
   auto bail = [&](int code) { *out = net; return code; };
   if (cudaSetDevice(net->device) != cudaSuccess) { net->err = "cudaSetDevice failed"; return bail(BCPNN_ERR_CUDA); }
-  if (cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&net->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
     net->err = "cudaStreamCreate failed";
     return bail(BCPNN_ERR_CUDA);
   }
+  for (int k = 0; k < 2; ++k)
+    if (cudaEventCreateWithFlags(&net->stage_ready[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&net->stage_free[k], cudaEventDisableTiming) != cudaSuccess) {
+      net->err = "cudaEventCreate failed";
+      return bail(BCPNN_ERR_CUDA);
+    }
 
   /* populations: running HCU/MCU offsets (ProcUpdLazy.cpp:19-29) */
   NetDev& H = net->h;
@@ -638,6 +652,8 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
 
   float dt = desc->dt;
   if ((rc = dalloc(net, &net->log_buf, (size_t)net->max_ticks * net->log_words_per_tick))) return bail(rc);
+  for (int k = 0; k < 2; ++k)
+    if ((rc = dalloc(net, &net->log_stage[k], (size_t)net->max_ticks * net->log_words_per_tick))) return bail(rc);
   uint32_t* ss = nullptr;
   if ((rc = dalloc(net, &ss, (size_t)net->max_ticks * std::max(1, desc->n_projs)))) return bail(rc);
   H.ss_log = ss;
@@ -936,6 +952,7 @@ int bcpnn_net_destroy(bcpnn_net* net) {
   if (!net) return BCPNN_ERR_INVALID;
   cudaSetDevice(net->device);
   if (net->stream) cudaStreamSynchronize(net->stream);
+  if (net->copy_stream) cudaStreamSynchronize(net->copy_stream);
   for (auto& kv : net->graphs) cudaGraphExecDestroy(kv.second);
   for (auto& J : net->projs)
     for (auto& s : J.slot)
@@ -946,6 +963,11 @@ int bcpnn_net_destroy(bcpnn_net* net) {
   if (net->stim_wm) cudaFree(net->stim_wm);
   if (net->d_lgidx_tab) cudaFree(net->d_lgidx_tab);
   if (net->stream) cudaStreamDestroy(net->stream);
+  if (net->copy_stream) cudaStreamDestroy(net->copy_stream);
+  for (int k = 0; k < 2; ++k) {
+    if (net->stage_ready[k]) cudaEventDestroy(net->stage_ready[k]);
+    if (net->stage_free[k]) cudaEventDestroy(net->stage_free[k]);
+  }
   delete net;
   return BCPNN_OK;
 }
@@ -1289,6 +1311,7 @@ int bcpnn_sync(bcpnn_net* net) {
   if (!net) return BCPNN_ERR_INVALID;
   CU(cudaSetDevice(net->device));
   CU(cudaStreamSynchronize(net->stream));
+  CU(cudaStreamSynchronize(net->copy_stream));
   return check_device_error(net);
 }
 
@@ -1318,7 +1341,20 @@ int bcpnn_get_spike_log_async(bcpnn_net* net, int32_t pop, uint32_t* out, size_t
   size_t need = (size_t)net->last_run_ticks * P.log_words;
   if (n_words != need) return fail(net, BCPNN_ERR_SIZE, "bcpnn_get_spike_log_async: n_words != last run ticks * words");
   CU(cudaSetDevice(net->device));
-  if (need) CU(cudaMemcpyAsync(out, net->log_buf + P.log_offset, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, net->stream));
+  if (need) {
+    /* device copy into a staging slot on the network's stream, once the host
+       copy that last read the slot is done; the host copy on copy_stream */
+    const int k = net->stage_next;
+    net->stage_next ^= 1;
+    uint32_t* st = net->log_stage[k] + P.log_offset;
+    const size_t bytes = need * sizeof(uint32_t);
+    CU(cudaStreamWaitEvent(net->stream, net->stage_free[k], 0));
+    CU(cudaMemcpyAsync(st, net->log_buf + P.log_offset, bytes, cudaMemcpyDeviceToDevice, net->stream));
+    CU(cudaEventRecord(net->stage_ready[k], net->stream));
+    CU(cudaStreamWaitEvent(net->copy_stream, net->stage_ready[k], 0));
+    CU(cudaMemcpyAsync(out, st, bytes, cudaMemcpyDeviceToHost, net->copy_stream));
+    CU(cudaEventRecord(net->stage_free[k], net->copy_stream));
+  }
   return BCPNN_OK;
 }
 

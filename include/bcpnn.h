@@ -217,13 +217,16 @@ int bcpnn_spike_log_words(const bcpnn_net* net, int32_t pop, int32_t* words);
    Synchronises the stream. */
 int bcpnn_get_spike_log(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words);
 
-/* The same copy queued on the network's stream without waiting for it: the
-   host can queue the next segment's stimulus and run behind it, and the
-   device runs the segments back to back.  `out` must stay valid, and is only
-   complete, after the next bcpnn_sync (which also reports a device error of
-   the runs); with page-locked `out` the copy is asynchronous, with pageable
-   memory the driver may complete it before returning.  A later bcpnn_run
-   does not disturb a queued copy (stream order). */
+/* The same copy queued without waiting for it: the host can queue the next
+   segment's stimulus and run behind it, and the device runs the segments
+   back to back.  The log is copied on the network's stream into one of two
+   device staging buffers and from there to `out` on a second stream of the
+   network, so the next run does not wait for the host copy.  `out` must stay
+   valid, and is only complete, after the next bcpnn_sync (which waits for
+   both streams and reports a device error of the runs); with page-locked
+   `out` the copy is asynchronous, with pageable memory the driver may
+   complete it before returning.  A later bcpnn_run does not disturb a queued
+   copy (stream order). */
 int bcpnn_get_spike_log_async(bcpnn_net* net, int32_t pop, uint32_t* out, size_t n_words);
 
 /* ProcCheck's recall counters on the device (ProcCheck/Pop.cpp:36-44
