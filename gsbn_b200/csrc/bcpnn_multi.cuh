@@ -268,6 +268,19 @@ __device__ __forceinline__ void replay_cell_hist(float4& c4, int tij, float zi2,
   const int lo = (simstep - tij >= B) ? simstep - B + 1 : tij;
   const int span = simstep - lo; /* ticks lo+1 .. simstep are bits span-1 .. 0 */
   uint32_t m = span > 1 ? (hist & (0xffffffffu >> (32 - span))) & ~1u : 0u;
+  /* the final decay runs from the last replayed tick (the lowest set bit b:
+     tick simstep - b) or from tij; its table entries are loaded before the
+     replays, beside the cell's own load */
+  const int pdt_f = m ? __ffs(m) - 1 : simstep - tij;
+  const bool tab_f = (unsigned)pdt_f < (unsigned)tlen;
+  float4 Af = make_float4(0, 0, 0, 0), Bf = Af;
+  double2 R0f = make_double2(0, 0), R1f = R0f;
+  if (tab_f) {
+    Af = tab[(size_t)pdt_f * 4];
+    Bf = tab[(size_t)pdt_f * 4 + 1];
+    R0f = T->rtab[(size_t)pdt_f * 4];
+    R1f = T->rtab[(size_t)pdt_f * 4 + 1];
+  }
   while (m) {
     const int b = 31 - __clz(m);
     m &= ~(1u << b);
@@ -276,9 +289,12 @@ __device__ __forceinline__ void replay_cell_hist(float4& c4, int tij, float zi2,
     zj2 = zj2 + kftj;
     tij = now;
   }
-  float zi2_unused = zi2;
-  decay_cell(pij, eij, zi2_unused, zj2, k, tab, tlen, T, simstep - tij);
-  c4 = make_float4(pij, eij, zi2, zj2);
+  if (!tab_f) {
+    table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt_f, 0, Af, Bf, k.fp64);
+    recip_part(Af, Bf, 0, R0f, R1f);
+  }
+  const float4 c = cell_step_nl(make_float4(pij, eij, zi2, zj2), T, Af, Bf, R0f, R1f);
+  c4 = make_float4(c.x, c.y, zi2, c.w); /* the cell keeps the zi2 of its last replay */
 }
 
 /* One tick of projection p for one destination HCU: update_jxx_cpu,
