@@ -16,13 +16,15 @@
  * The closed forms are gsbn's (same expressions as ProcUpdLazy), evaluated
  * with the shared decay tables and the exact division of bcpnn_device.cuh.
  *
- * One launch of pop_kernel per tick over every (population, HCU), then one
- * launch of proj_kernel per projection over its destination HCUs (512
- * threads), or one persistent launch per run (tick_loop, or res_tick_loop
- * with each HCU's state resident in shared memory); all_kernel does the
- * catch-up at a change of prn.  Per-tick
- * buffers follow the ProcUpdLazy path's tick parity (dsup, epsc, bj, si), so
- * state reads and the spike log work unchanged.
+ * Launch forms: one persistent cooperative launch per run, with each HCU's
+ * state resident in shared memory (res_tick_loop) or in global memory
+ * (tick_loop, for spike rings longer than 32 ticks or states too large for
+ * shared memory); or, when the grid cannot be co-resident, one launch of
+ * pop_kernel per tick over every (population, HCU) and one of proj_kernel
+ * per projection over its destination HCUs (512 threads).  all_kernel does
+ * the catch-up at a change of prn.  Per-tick buffers follow the ProcUpdLazy
+ * path's tick parity (dsup, epsc, bj, si), so state reads and the spike log
+ * work unchanged.
  */
 #ifndef BCPNN_MULTI_CUH
 #define BCPNN_MULTI_CUH
@@ -584,7 +586,10 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
    The delay queue of a tick reads only the previous tick's source spikes and
    qi, so its 4 warps (threads 384-511) compute the next tick's active rows
    while the other 12 warps do the population update; every thread then
-   takes part in the projections. */
+   takes part in the projections.  After its last write of a tick the CTA
+   arrives at the grid barrier and, before it waits, draws the next tick's
+   sampling uniforms and stages the next tick's first row chunk of
+   projection 0 (row traces, cell replays and decays to the next tick). */
 constexpr int kResQueueWarps = 4;
 constexpr int kResPopThreads = kProjThreads - 32 * kResQueueWarps; /* 384 */
 constexpr int kBarPop = 1, kBarQueue = 2;
