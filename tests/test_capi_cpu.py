@@ -5,6 +5,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 from gsbn_b200 import capi
@@ -104,6 +105,10 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.bcpnn_last_error(None) == b"null handle"
     out = ctypes.c_void_p()
     assert lib.bcpnn_net_create(None, ctypes.byref(out)) == -1
+    lg = np.zeros(4, np.int32)
+    wm = np.zeros(4, np.float32)
+    assert lib.bcpnn_upload_stimuli_idx_async(None, 1, lg.ctypes.data, 1e-4, 1, wm.ctypes.data) == -1
+    assert lib.bcpnn_get_spike_log_async(None, 0, lg.ctypes.data, 4) == -1
 
 
 def test_output_buffers_are_checked_before_the_library_writes():
