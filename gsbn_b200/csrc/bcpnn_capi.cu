@@ -145,6 +145,9 @@ struct bcpnn_net {
   int32_t* d_lgidx = nullptr; /* one pattern-index row (bcpnn_set_stimulus_idx) */
   std::vector<int32_t*> check_cnt; /* per population: ProcCheck counters [H*M] (bcpnn_check_count) */
   std::vector<int32_t*> check_out; /* per population: [2][H] idx, count of the last check */
+  /* per population: check_out written (network's stream) / read by the host
+     copies (copy_stream) */
+  std::vector<cudaEvent_t> check_ready, check_free;
   float* stim_wm = nullptr;
   int stim_lg_rows = 0, stim_wm_rows = 0;
   int stim_lg_cap = 0, stim_wm_cap = 0; /* rows the stimulus tables have room for */
@@ -968,6 +971,10 @@ int bcpnn_net_destroy(bcpnn_net* net) {
     if (net->stage_ready[k]) cudaEventDestroy(net->stage_ready[k]);
     if (net->stage_free[k]) cudaEventDestroy(net->stage_free[k]);
   }
+  for (cudaEvent_t e : net->check_ready)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : net->check_free)
+    if (e) cudaEventDestroy(e);
   delete net;
   return BCPNN_OK;
 }
@@ -1411,9 +1418,13 @@ static int check_buffers(bcpnn_net* net, int pop) {
   if (net->check_cnt.empty()) {
     net->check_cnt.assign(net->pops.size(), nullptr);
     net->check_out.assign(net->pops.size(), nullptr);
+    net->check_ready.assign(net->pops.size(), nullptr);
+    net->check_free.assign(net->pops.size(), nullptr);
   }
   if (!net->check_cnt[pop]) {
     const PopHost& P = net->pops[pop];
+    if (!net->check_ready[pop]) CU(cudaEventCreateWithFlags(&net->check_ready[pop], cudaEventDisableTiming));
+    if (!net->check_free[pop]) CU(cudaEventCreateWithFlags(&net->check_free[pop], cudaEventDisableTiming));
     int rc = dalloc(net, &net->check_cnt[pop], (size_t)P.H * P.M);
     if (rc) return rc;
     if ((rc = dalloc(net, &net->check_out[pop], 2 * (size_t)P.H))) return rc;
@@ -1450,11 +1461,19 @@ int bcpnn_check_result_async(bcpnn_net* net, int32_t pop, int32_t* idx, int32_t*
   CU(cudaSetDevice(net->device));
   int rc = check_buffers(net, pop);
   if (rc) return rc;
+  /* the result kernel on the network's stream, once the host copies of the
+     previous result are done; the host copies on copy_stream, so the next
+     run does not wait for them */
+  CU(cudaStreamWaitEvent(net->stream, net->check_free[pop], 0));
   check_result_kernel<<<(P.H + 7) / 8, 256, 0, net->stream>>>(net->check_cnt[pop], P.H, P.M, net->check_out[pop]);
   CU(cudaGetLastError());
   net->launches += 1;
-  CU(cudaMemcpyAsync(idx, net->check_out[pop], n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost, net->stream));
-  CU(cudaMemcpyAsync(cnt, net->check_out[pop] + P.H, n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaEventRecord(net->check_ready[pop], net->stream));
+  CU(cudaStreamWaitEvent(net->copy_stream, net->check_ready[pop], 0));
+  CU(cudaMemcpyAsync(idx, net->check_out[pop], n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost, net->copy_stream));
+  CU(cudaMemcpyAsync(cnt, net->check_out[pop] + P.H, n_hcu * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                     net->copy_stream));
+  CU(cudaEventRecord(net->check_free[pop], net->copy_stream));
   return BCPNN_OK;
 }
 

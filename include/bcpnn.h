@@ -237,7 +237,8 @@ int bcpnn_get_spike_log_async(bcpnn_net* net, int32_t pop, uint32_t* out, size_t
    bcpnn_check_result_async queues, per HCU, the MCU with the most counted
    spikes (the first on ties, -1 when none spiked) and that count into
    idx/cnt (n_hcu = the population's HCUs) and clears the counters; like the
-   asynchronous spike log, idx/cnt are complete after the next bcpnn_sync.
+   asynchronous spike log (and on the same second stream), idx/cnt are
+   complete after the next bcpnn_sync.
    The caller walks ProcCheck's tick cursor (which ticks count, when a
    segment is evaluated) and compares idx/cnt with the expected pattern. */
 int bcpnn_check_count(bcpnn_net* net, int32_t pop, int32_t k0, int32_t k1);
