@@ -49,13 +49,7 @@ __global__ void __launch_bounds__(kProjThreads, 1) tick_kernel(const NetDev* __r
 __global__ void __launch_bounds__(kProjThreads, 1) res_tick_kernel(const NetDev* __restrict__ net,
                                                                   const RunParams* __restrict__ rp, int it0,
                                                                   int n_ticks, unsigned int* bar) {
-  __shared__ int s_ok;
-  __shared__ float s_unused;
-  res_tick_loop(
-      net, rp, it0, n_ticks, [&]() { t512::grid_arrive(bar); },
-      [&](int k) {
-        return t512::grid_wait(bar, (unsigned int)k * gridDim.x, net->err, &s_ok, nullptr, 0u, &s_unused);
-      });
+  res_tick_loop(net, rp, it0, n_ticks, bar);
 }
 }  // namespace multi
 }  // namespace bcpnn
@@ -332,8 +326,7 @@ int reset_state(bcpnn_net* net) {
     if ((rc = dset(net, D.cell, cells, make_float4(pij0, 0.0f, 0.0f, 0.0f)))) return rc;
     if ((rc = dzero(net, D.tij, cells * sizeof(int)))) return rc;
     if ((rc = dzero(net, D.wij, cells * sizeof(float)))) return rc;
-    if ((rc = dzero(net, D.si[0], (size_t)J.Ns))) return rc;
-    if ((rc = dzero(net, D.si[1], (size_t)J.Ns))) return rc;
+    if ((rc = dzero(net, D.si[0], 3 * (size_t)J.Ns))) return rc;
     if ((rc = dzero(net, D.list_cnt, (size_t)J.H * sizeof(int)))) return rc;
   }
   for (size_t q = 0; q < net->check_cnt.size(); ++q)
@@ -432,6 +425,17 @@ struct Resolved {
   float4* cell;
   int proj;
 };
+
+/* the source-spike buffer of the last tick: by tick parity, or, for
+   ProcUpdMulti's resident launch, one of three by tick mod 3 (par[0] is the
+   block of three) */
+static void* si_last(const bcpnn_net* net, const Resolved& r) {
+  if (net->multi && net->multi_persistent && net->multi_resident) {
+    const long long k = ((net->k_total - 1) % 3 + 3) % 3;
+    return (int8_t*)r.par[0] + (size_t)k * r.count;
+  }
+  return r.par[(int)((net->k_total - 1) & 1)];
+}
 
 bool resolve(const bcpnn_net* net, const char* cname, Resolved* r) {
   if (!cname) return false;
@@ -777,8 +781,10 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     if ((rc = dalloc(net, &D.cell, cells))) return bail(rc);
     if ((rc = dalloc(net, &D.tij, cells))) return bail(rc);
     if ((rc = dalloc(net, &D.wij, cells))) return bail(rc);
-    if ((rc = dalloc(net, &D.si[0], J.Ns))) return bail(rc);
-    if ((rc = dalloc(net, &D.si[1], J.Ns))) return bail(rc);
+    /* source spikes: one block of three buffers of Ns; the tick parity
+       forms use the first two, ProcUpdMulti's resident launch all three */
+    if ((rc = dalloc(net, &D.si[0], 3 * (size_t)J.Ns))) return bail(rc);
+    D.si[1] = D.si[0] + J.Ns;
     if ((rc = dalloc(net, &D.list, R))) return bail(rc);
     if ((rc = dalloc(net, &D.list_cnt, J.H))) return bail(rc);
   }
@@ -1510,8 +1516,10 @@ int bcpnn_read_state(bcpnn_net* net, const char* name, void* host, size_t bytes)
       CU(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, net->stream));
       break;
     case K_PARITY:
-    case K_SI:
       CU(cudaMemcpyAsync(host, r.par[last], bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    case K_SI:
+      CU(cudaMemcpyAsync(host, si_last(net, r), bytes, cudaMemcpyDeviceToHost, net->stream));
       break;
     case K_CELL: {
       int rc = ensure_scratch(net, r.count);
@@ -1555,8 +1563,10 @@ int bcpnn_write_state(bcpnn_net* net, const char* name, const void* host, size_t
       CU(cudaMemcpyAsync(r.ptr, host, bytes, cudaMemcpyHostToDevice, net->stream));
       break;
     case K_PARITY:
-    case K_SI:
       CU(cudaMemcpyAsync(r.par[last], host, bytes, cudaMemcpyHostToDevice, net->stream));
+      break;
+    case K_SI:
+      CU(cudaMemcpyAsync(si_last(net, r), host, bytes, cudaMemcpyHostToDevice, net->stream));
       break;
     case K_CELL: {
       int rc = ensure_scratch(net, r.count);
@@ -1844,8 +1854,10 @@ extern "C" int bcpnn_read_state_noalloc(bcpnn_net* net, const char* name, void* 
       CU(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, net->stream));
       break;
     case K_PARITY:
-    case K_SI:
       CU(cudaMemcpyAsync(host, r.par[last], bytes, cudaMemcpyDeviceToHost, net->stream));
+      break;
+    case K_SI:
+      CU(cudaMemcpyAsync(host, si_last(net, r), bytes, cudaMemcpyDeviceToHost, net->stream));
       break;
     case K_CELL: {
       /* set-up, once per device with that device current: the device address

@@ -685,12 +685,36 @@ __device__ __forceinline__ void res_draw(const PopDev& pop, bool poisson, int si
   }
 }
 
-/* arrive(): this CTA's arrival at the grid barrier after a tick (all its
-   writes of the tick made); wait(k): the wait for every CTA's k-th arrival,
-   false when it gave up */
-template <typename Arrive, typename Wait>
+/* the grid barrier of the resident launch, split: a CTA arrives (release
+   add) once its tick's source spikes are written and its delay queue has
+   read the previous tick's; only the delay-queue warps wait (acquire poll,
+   bounded) before they read the source spikes of the previous tick */
+__device__ __forceinline__ void mp_arrive(unsigned int* bar) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(bar), "r"(1u) : "memory");
+}
+
+constexpr int kErrBarrierWait = 2; /* the error bit of a grid-barrier wait that ran out of time */
+
+__device__ __forceinline__ bool mp_poll(const unsigned int* bar, unsigned int target, int* err) {
+  unsigned long long t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (;;) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+    if (v >= target) return true;
+    if (*(volatile int*)err) return false;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > 2000000000ull) {
+      atomicOr(err, kErrBarrierWait);
+      return false;
+    }
+    __nanosleep(20);
+  }
+}
+
+/* bar: the arrival counter of the launch, zero at launch */
 __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, const RunParams* __restrict__ rp,
-                                              int it0, int n_ticks, Arrive arrive, Wait wait) {
+                                              int it0, int n_ticks, unsigned int* bar) {
   extern __shared__ __align__(16) float sm[];
   /* descriptors, copied once per launch: every tick reads them in chains */
   __shared__ PopDev s_pop;
@@ -705,6 +729,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
   __shared__ float s_vsum, s_wm;
   __shared__ int s_flag9;
   __shared__ int s_staged; /* rows of projection 0's first chunk staged for this tick, or -1 */
+  __shared__ int s_qok;    /* the delay-queue warps' barrier wait succeeded */
 
   const int tid = threadIdx.x;
   const int P = net->cta_pop[blockIdx.x];
@@ -799,28 +824,26 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       if (tid == 0) s_nlist[q][0] = cnt;
     }
     res_draw(pop, poisson, s0, h, r_u, r_up, tid, blockDim.x);
-    if (tid == 0) s_staged = -1;
+    if (tid == 0) {
+      s_staged = -1;
+      s_qok = 1;
+    }
   }
   __syncthreads();
 #ifdef BCPNN_PHASE_PROBE
   if (tid < kProbeSlots) g_probe_smem[tid] = 0;
   __syncthreads();
   long long probe_clock = clock64();
-#else
-  long long probe_clock = 0;
-#endif
   long long* probe_t = &probe_clock;
-  (void)probe_t;
+#endif
 
   int it = it0;
   for (; it < it0 + n_ticks; ++it) {
-    if (it > it0 && !wait(it - it0)) break;
     MPROBE(0);
 #ifdef BCPNN_PHASE_PROBE
     if (tid == 0) g_probe_smem[kProbeTicks] += 1;
 #endif
     const int simstep = rp->simstep0 + it, kk = rp->k0 + it;
-    const int cur = kk & 1, prev = cur ^ 1;
     const int lp = (it - it0) & 1; /* list parity: this tick's rows */
 
     if (tid < kResPopThreads) {
@@ -917,8 +940,10 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         r_hist[j] = (r_hist[j] << 1) | (sv > 0 ? 1u : 0u);
         pop.spike[idx] = sv;
         if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
+        /* source spikes in three buffers by tick (kk mod 3): a CTA may run
+           one tick ahead of the readers of the previous tick's */
         for (int q = 0; q < pop.n_out; ++q) {
-          int8_t* si = q < kMaxIn ? s_siout[q][cur] : net->projs[pop.out_proj[q]].si[cur];
+          int8_t* si = (q < kMaxIn ? s_siout[q][0] : net->projs[pop.out_proj[q]].si[0]) + (size_t)(kk % 3) * n;
           si[idx] = sv;
         }
       }
@@ -928,11 +953,17 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
          tick's active rows (update_ssi_cpu, :580-588), ascending ---- */
       const int qt = tid - kResPopThreads, qw = qt >> 5, lane = tid & 31;
       const int nq = lp ^ 1;
-      for (int q = 0; q < n_in; ++q) {
+      /* the previous tick's source spikes are complete once every CTA has
+         arrived for it (the launch's first tick reads the last launch's) */
+      if (it > it0) {
+        if (qt == 0 && !mp_poll(bar, (unsigned int)(it - it0) * gridDim.x, net->err)) s_qok = 0;
+        named_sync(kBarQueue, 32 * kResQueueWarps);
+      }
+      for (int q = 0; q < n_in && s_qok; ++q) {
         const ProjDev& J = s_proj[q];
         const int C = J.C, Ns = J.Ns;
         const ResQ V = res_q(sm, L, q, M, C);
-        const int8_t* si = J.si[prev];
+        const int8_t* si = J.si[0] + (size_t)((kk + 2) % 3) * Ns;
         const int ng = (C + 31) >> 5; /* groups of 32 slots; warp qw takes a contiguous range */
         const int per = (ng + kResQueueWarps - 1) / kResQueueWarps;
         const int g0 = qw * per, g1 = min(ng, g0 + per);
@@ -1000,6 +1031,9 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
     }
     __syncthreads();
     MPROBE(10);
+    if (!s_qok) break;
+    /* this tick's source spikes are written and the previous tick's read */
+    if (tid == 0 && it + 1 < it0 + n_ticks) mp_arrive(bar);
 
     /* ---- projections: update_jxx_cpu, update_row_cpu (Proj.cpp:557-706) ---- */
     for (int q = 0; q < n_in; ++q) {
@@ -1127,11 +1161,9 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
       }
     }
-    /* every write of this tick is made: arrive, and draw the next tick's
-       uniforms while the other CTAs arrive */
+    /* the next tick's uniforms and row staging (no other CTA's data) */
     if (it + 1 < it0 + n_ticks) {
       __syncthreads();
-      arrive();
       /* the uniforms by threads 256 up (MCU (tid + 256) mod 512): the staging
          below takes its cells from thread 0 up and its rows from the top */
       {
@@ -1203,6 +1235,9 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         if (tid == 0) s_staged = nr;
       }
       MPROBE(11);
+      /* the next tick's population update reads the uniforms drawn here
+         and shifts the history the staging reads */
+      __syncthreads();
     }
   }
 
