@@ -586,10 +586,15 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
    The delay queue of a tick reads only the previous tick's source spikes and
    qi, so its 4 warps (threads 384-511) compute the next tick's active rows
    while the other 12 warps do the population update; every thread then
-   takes part in the projections.  After its last write of a tick the CTA
-   arrives at the grid barrier and, before it waits, draws the next tick's
-   sampling uniforms and stages the next tick's first row chunk of
-   projection 0 (row traces, cell replays and decays to the next tick). */
+   takes part in the projections.  The previous tick's source spikes are
+   the only data of other CTAs a tick reads, and only the delay queue reads
+   them: a CTA arrives at the grid barrier when the two groups join (its
+   source spikes written, the previous tick's read) and only the delay-queue
+   warps wait, before they read.  CTAs may run one tick apart, so the source
+   spikes live in three buffers by tick (tick mod 3).  After its rows the
+   CTA draws the next tick's sampling uniforms and stages the next tick's
+   first row chunk of projection 0 (row traces, cell replays and decays to
+   the next tick). */
 constexpr int kResQueueWarps = 4;
 constexpr int kResPopThreads = kProjThreads - 32 * kResQueueWarps; /* 384 */
 constexpr int kBarPop = 1, kBarQueue = 2;
