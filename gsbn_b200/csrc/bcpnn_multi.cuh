@@ -45,8 +45,11 @@ __host__ __device__ inline int row_chunk(int M) { return M >= kRowCells ? 1 : kR
    0 barrier wait, 1 support, 2 softmax maximum and exponentials, 3 softmax
    sum, 4 spikes, 5 j-traces and row list, 6 row traces and cell replays,
    7 weights, 8 epsc sums, 9 delay queue, 10 (resident launch) wait for the
-   delay-queue warps, 11 (resident launch) staging of the next tick's first
-   row chunk after the barrier arrival; kProbeTicks counts the ticks */
+   delay-queue warps, 11 (resident launch) the uniforms and the staging of
+   the next tick's first row chunk, 12 (resident launch, the first
+   delay-queue thread) its wait at the grid barrier; kProbeTicks counts the
+   ticks.  In the resident launch slot 0 holds no barrier wait (only the
+   delay-queue warps wait there). */
 #ifdef BCPNN_PHASE_PROBE
 #define MPROBE(slot)                                                   \
   do {                                                                 \
@@ -961,7 +964,13 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       /* the previous tick's source spikes are complete once every CTA has
          arrived for it (the launch's first tick reads the last launch's) */
       if (it > it0) {
+#ifdef BCPNN_PHASE_PROBE
+        const long long qclk = clock64();
+#endif
         if (qt == 0 && !mp_poll(bar, (unsigned int)(it - it0) * gridDim.x, net->err)) s_qok = 0;
+#ifdef BCPNN_PHASE_PROBE
+        if (qt == 0) g_probe_smem[12] += (unsigned long long)(clock64() - qclk);
+#endif
         named_sync(kBarQueue, 32 * kResQueueWarps);
       }
       for (int q = 0; q < n_in && s_qok; ++q) {
