@@ -358,7 +358,7 @@ void enqueue_run(bcpnn_net* net, int n_ticks, bool with_all) {
         multi::all_kernel<<<grid_for((size_t)J.H * J.C * 32, 256), 256, 0, net->stream>>>(net->d_net, net->d_rp, p);
       }
     if (net->multi_persistent) {
-      cudaMemsetAsync(net->bar, 0, sizeof(unsigned int), net->stream);
+      cudaMemsetAsync(net->bar, 0, 4 * sizeof(unsigned int), net->stream);
       int it0 = 0, n = n_ticks;
       void* args[] = {(void*)&net->d_net, (void*)&net->d_rp, (void*)&it0, (void*)&n, (void*)&net->bar};
       cudaLaunchCooperativeKernel(net->multi_resident ? (const void*)multi::res_tick_kernel

@@ -720,7 +720,7 @@ __device__ __forceinline__ bool mp_poll(const unsigned int* bar, unsigned int ta
   }
 }
 
-/* bar: the arrival counter of the launch, zero at launch */
+/* bar: four arrival counters (by tick mod 4), zero at launch */
 __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, const RunParams* __restrict__ rp,
                                               int it0, int n_ticks, unsigned int* bar) {
   extern __shared__ __align__(16) float sm[];
@@ -956,6 +956,138 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         }
       }
       MPROBE(4);
+      /* this tick's source spikes are written: the group's arrival */
+      named_sync(kBarPop, G);
+      if (tid == 0 && it + 1 < it0 + n_ticks) mp_arrive(bar + ((it - it0) & 3));
+
+        /* ---- projections (update_jxx_cpu, update_row_cpu, Proj.cpp:557-706),
+           by the population group while the delay-queue warps run on: the
+           rows of this tick come from the previous tick's queue ---- */
+      for (int q = 0; q < n_in; ++q) {
+        const ProjDev& J = s_proj[q];
+        const TabRef* T = &s_tab[q]; /* coefficients and reciprocals of this kp */
+        const int C = J.C;
+        const ResQ V = res_q(sm, L, q, M, C);
+        const float kp = J.taupdt * rp->prn;
+        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+        const float4* tab = T->tab;
+        const int tlen = T->len;
+        for (int j = tid; j < M; j += G) {
+          float pj = V.pj[j], ej = V.ej[j], zj = V.zj[j];
+          float e = V.epsc[j];
+          e *= (1 - J.kepsc);
+          pj += (ej - pj) * kp;
+          ej += (zj - ej) * k.ke;
+          zj *= (1 - J.kzj);
+          if (r_hist[j] & 1u) zj += J.kftj;
+          if (kp != 0.0f) V.bj[j] = J.bgain * bx_logf(pj + J.eps);
+          V.pj[j] = pj;
+          V.ej[j] = ej;
+          V.zj[j] = zj;
+          V.epsc[j] = e;
+        }
+        const int nrow = s_nlist[q][lp];
+        const int* list = V.list + lp * C;
+        if (tid == 0) s_flag9 = 0;
+        named_sync(kBarPop, G);
+        MPROBE(5);
+        for (int base = 0; base < nrow; base += rch) {
+          const int nr = (nrow - base) < rch ? (nrow - base) : rch;
+          if (q == 0 && base == 0 && s_staged == nr) {
+            /* staged after the previous tick's barrier arrival: the row
+               traces are up to date, the cells replayed and decayed to this
+               tick; what is left is a spike now */
+            for (int t = tid; t < nr; t += G)
+              if (h * C + list[t] == 9) s_flag9 = 1;
+            for (int c = tid; c < nr * M; c += G) {
+              const int rr = c / M, j = c - rr * M;
+              const size_t index = (size_t)(h * C + list[rr]) * M + j;
+              float4 c4 = st_c4[c];
+              if (r_hist[j] & 1u) c4.w += J.kftj;
+              J.cell[index] = c4;
+              s_w[c] = c4.x;
+            }
+            named_sync(kBarPop, G);
+            MPROBE(6);
+          } else {
+          for (int t = tid; t < nr; t += G) {
+            const int sl = list[base + t];
+            s_ti[t] = V.ti[sl];
+            s_zi[t] = V.zi[sl];
+            if (h * C + sl == 9) s_flag9 = 1;
+          }
+          named_sync(kBarPop, G);
+          /* row traces (from the top thread down) beside the cells (from
+             thread 0 up) */
+          for (int t = G - 1 - tid; t < nr; t += G) {
+            const int sl = list[base + t];
+            const int pdt = simstep - s_ti[t];
+            float pi = V.pi[sl];
+            if (pdt > 0) {
+              float4 A, Bv;
+              double2 R0, R1;
+              if (pdt < tlen) {
+                A = tab[(size_t)pdt * 4 + 2];
+                Bv = tab[(size_t)pdt * 4 + 3];
+                R0 = T->rtab[(size_t)pdt * 4 + 2];
+                R1 = T->rtab[(size_t)pdt * 4 + 3];
+              } else {
+                table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
+                recip_part(A, Bv, 2, R0, R1);
+              }
+              /* zi becomes zi*exp(-kzi*pdt) */
+              const float4 rv = row_step_nl(make_float4(pi, V.ei[sl], s_zi[t], 0.0f), T, A, Bv, R0, R1);
+              pi = rv.x;
+              V.pi[sl] = rv.x;
+              V.ei[sl] = rv.y;
+              V.zi[sl] = rv.z + J.kfti;
+            }
+            V.ti[sl] = simstep;
+            s_pi[t] = pi;
+          }
+          for (int c = tid; c < nr * M; c += G) {
+            const int rr = c / M, j = c - rr * M;
+            const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
+            float4 c4 = J.cell[index];
+            const uint32_t hist = r_hist[j];
+            replay_cell_hist(c4, s_ti[rr], s_zi[rr], simstep, hist, B, k, tab, tlen, T, J.kftj);
+            if (hist & 1u) c4.w += J.kftj;
+            J.cell[index] = c4;
+            s_w[c] = c4.x;
+          }
+          named_sync(kBarPop, G);
+          MPROBE(6);
+          }
+          for (int c = tid; c < nr * M; c += G) {
+            const int rr = c / M, j = c - rr * M;
+            const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
+            float w;
+            if (kp != 0.0f) {
+              w = J.wgain * bx_logf((s_w[c] + J.eps2) / ((s_pi[rr] + J.eps) * (V.pj[j] + J.eps)));
+              J.wij[index] = w;
+            } else {
+              w = J.wij[index];
+            }
+            s_w[c] = w;
+          }
+          named_sync(kBarPop, G);
+          MPROBE(7);
+          for (int j = tid; j < M; j += G) {
+            float e = V.epsc[j];
+            for (int rr = 0; rr < nr; ++rr) e += s_w[rr * M + j];
+            V.epsc[j] = e;
+          }
+          named_sync(kBarPop, G);
+          MPROBE(8);
+        }
+        if (tid == 0) {
+          uint32_t f = 0;
+          if (s_flag9) f |= 1;
+          if (h == 9 / M && 9 < n && (r_hist[9 - h * M] & 1u)) f |= 2;
+          if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + s_inp[q]], f);
+          atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
+        }
+      }
     } else {
       /* ---- delay queue (update_que_cpu, Proj.cpp:620-636) and the next
          tick's active rows (update_ssi_cpu, :580-588), ascending ---- */
@@ -967,7 +1099,15 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
 #ifdef BCPNN_PHASE_PROBE
         const long long qclk = clock64();
 #endif
-        if (qt == 0 && !mp_poll(bar, (unsigned int)(it - it0) * gridDim.x, net->err)) s_qok = 0;
+        /* two arrivals per CTA and tick, its population group's (source
+           spikes written) and its delay-queue group's (source spikes read),
+           on the counter of the tick's slot (tick mod 4).  A group arrives
+           for tick u only once tick u - 2 is complete, so while tick t - 1
+           is incomplete no arrival for a tick above t exists, and the
+           slot's count for t - 1 is 2 arrivals x CTAs x its ticks so far */
+        const int tp = it - 1 - it0;
+        if (qt == 0 && !mp_poll(bar + (tp & 3), 2u * gridDim.x * (unsigned int)((tp >> 2) + 1), net->err))
+          s_qok = 0;
 #ifdef BCPNN_PHASE_PROBE
         if (qt == 0) g_probe_smem[12] += (unsigned long long)(clock64() - qclk);
 #endif
@@ -1042,142 +1182,17 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
           if (a < end) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
         }
       }
+      /* the previous tick's source spikes are read: the group's arrival */
+      named_sync(kBarQueue, 32 * kResQueueWarps);
+      if (qt == 0 && it + 1 < it0 + n_ticks) mp_arrive(bar + ((it - it0) & 3));
     }
     __syncthreads();
     MPROBE(10);
     if (!s_qok) break;
-    /* this tick's source spikes are written and the previous tick's read */
-    if (tid == 0 && it + 1 < it0 + n_ticks) mp_arrive(bar);
 
-    /* ---- projections: update_jxx_cpu, update_row_cpu (Proj.cpp:557-706) ---- */
-    for (int q = 0; q < n_in; ++q) {
-      const ProjDev& J = s_proj[q];
-      const TabRef* T = &s_tab[q]; /* coefficients and reciprocals of this kp */
-      const int C = J.C;
-      const ResQ V = res_q(sm, L, q, M, C);
-      const float kp = J.taupdt * rp->prn;
-      const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-      const float4* tab = T->tab;
-      const int tlen = T->len;
-      for (int j = tid; j < M; j += blockDim.x) {
-        float pj = V.pj[j], ej = V.ej[j], zj = V.zj[j];
-        float e = V.epsc[j];
-        e *= (1 - J.kepsc);
-        pj += (ej - pj) * kp;
-        ej += (zj - ej) * k.ke;
-        zj *= (1 - J.kzj);
-        if (r_hist[j] & 1u) zj += J.kftj;
-        if (kp != 0.0f) V.bj[j] = J.bgain * bx_logf(pj + J.eps);
-        V.pj[j] = pj;
-        V.ej[j] = ej;
-        V.zj[j] = zj;
-        V.epsc[j] = e;
-      }
-      const int nrow = s_nlist[q][lp];
-      const int* list = V.list + lp * C;
-      if (tid == 0) s_flag9 = 0;
-      __syncthreads();
-      MPROBE(5);
-      for (int base = 0; base < nrow; base += rch) {
-        const int nr = (nrow - base) < rch ? (nrow - base) : rch;
-        if (q == 0 && base == 0 && s_staged == nr) {
-          /* staged after the previous tick's barrier arrival: the row
-             traces are up to date, the cells replayed and decayed to this
-             tick; what is left is a spike now */
-          for (int t = tid; t < nr; t += blockDim.x)
-            if (h * C + list[t] == 9) s_flag9 = 1;
-          for (int c = tid; c < nr * M; c += blockDim.x) {
-            const int rr = c / M, j = c - rr * M;
-            const size_t index = (size_t)(h * C + list[rr]) * M + j;
-            float4 c4 = st_c4[c];
-            if (r_hist[j] & 1u) c4.w += J.kftj;
-            J.cell[index] = c4;
-            s_w[c] = c4.x;
-          }
-          __syncthreads();
-          MPROBE(6);
-        } else {
-        for (int t = tid; t < nr; t += blockDim.x) {
-          const int sl = list[base + t];
-          s_ti[t] = V.ti[sl];
-          s_zi[t] = V.zi[sl];
-          if (h * C + sl == 9) s_flag9 = 1;
-        }
-        __syncthreads();
-        /* row traces (from the top thread down) beside the cells (from
-           thread 0 up) */
-        for (int t = blockDim.x - 1 - tid; t < nr; t += blockDim.x) {
-          const int sl = list[base + t];
-          const int pdt = simstep - s_ti[t];
-          float pi = V.pi[sl];
-          if (pdt > 0) {
-            float4 A, Bv;
-            double2 R0, R1;
-            if (pdt < tlen) {
-              A = tab[(size_t)pdt * 4 + 2];
-              Bv = tab[(size_t)pdt * 4 + 3];
-              R0 = T->rtab[(size_t)pdt * 4 + 2];
-              R1 = T->rtab[(size_t)pdt * 4 + 3];
-            } else {
-              table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
-              recip_part(A, Bv, 2, R0, R1);
-            }
-            /* zi becomes zi*exp(-kzi*pdt) */
-            const float4 rv = row_step_nl(make_float4(pi, V.ei[sl], s_zi[t], 0.0f), T, A, Bv, R0, R1);
-            pi = rv.x;
-            V.pi[sl] = rv.x;
-            V.ei[sl] = rv.y;
-            V.zi[sl] = rv.z + J.kfti;
-          }
-          V.ti[sl] = simstep;
-          s_pi[t] = pi;
-        }
-        for (int c = tid; c < nr * M; c += blockDim.x) {
-          const int rr = c / M, j = c - rr * M;
-          const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
-          float4 c4 = J.cell[index];
-          const uint32_t hist = r_hist[j];
-          replay_cell_hist(c4, s_ti[rr], s_zi[rr], simstep, hist, B, k, tab, tlen, T, J.kftj);
-          if (hist & 1u) c4.w += J.kftj;
-          J.cell[index] = c4;
-          s_w[c] = c4.x;
-        }
-        __syncthreads();
-        MPROBE(6);
-        }
-        for (int c = tid; c < nr * M; c += blockDim.x) {
-          const int rr = c / M, j = c - rr * M;
-          const size_t index = (size_t)(h * C + list[base + rr]) * M + j;
-          float w;
-          if (kp != 0.0f) {
-            w = J.wgain * bx_logf((s_w[c] + J.eps2) / ((s_pi[rr] + J.eps) * (V.pj[j] + J.eps)));
-            J.wij[index] = w;
-          } else {
-            w = J.wij[index];
-          }
-          s_w[c] = w;
-        }
-        __syncthreads();
-        MPROBE(7);
-        for (int j = tid; j < M; j += blockDim.x) {
-          float e = V.epsc[j];
-          for (int rr = 0; rr < nr; ++rr) e += s_w[rr * M + j];
-          V.epsc[j] = e;
-        }
-        __syncthreads();
-        MPROBE(8);
-      }
-      if (tid == 0) {
-        uint32_t f = 0;
-        if (s_flag9) f |= 1;
-        if (h == 9 / M && 9 < n && (r_hist[9 - h * M] & 1u)) f |= 2;
-        if (f) atomicOr(&net->ss_log[(size_t)it * net->n_projs + s_inp[q]], f);
-        atomicAdd(&net->counters[0], (unsigned long long)nrow * M);
-      }
-    }
-    /* the next tick's uniforms and row staging (no other CTA's data) */
+    /* the next tick's uniforms and row staging (no other CTA's data; the
+       join above ordered this tick's rows and queue before it) */
     if (it + 1 < it0 + n_ticks) {
-      __syncthreads();
       /* the uniforms by threads 256 up (MCU (tid + 256) mod 512): the staging
          below takes its cells from thread 0 up and its rows from the top */
       {
