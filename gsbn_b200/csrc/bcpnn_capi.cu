@@ -326,7 +326,7 @@ int reset_state(bcpnn_net* net) {
     if ((rc = dset(net, D.cell, cells, make_float4(pij0, 0.0f, 0.0f, 0.0f)))) return rc;
     if ((rc = dzero(net, D.tij, cells * sizeof(int)))) return rc;
     if ((rc = dzero(net, D.wij, cells * sizeof(float)))) return rc;
-    if ((rc = dzero(net, D.si[0], 3 * (size_t)J.Ns))) return rc;
+    if ((rc = dzero(net, D.si[0], 4 * (size_t)J.Ns))) return rc;
     if ((rc = dzero(net, D.list_cnt, (size_t)J.H * sizeof(int)))) return rc;
   }
   for (size_t q = 0; q < net->check_cnt.size(); ++q)
@@ -427,11 +427,11 @@ struct Resolved {
 };
 
 /* the source-spike buffer of the last tick: by tick parity, or, for
-   ProcUpdMulti's resident launch, one of three by tick mod 3 (par[0] is the
-   block of three) */
+   ProcUpdMulti's resident launch, one of four by tick mod 4 (par[0] is the
+   block of four) */
 static void* si_last(const bcpnn_net* net, const Resolved& r) {
   if (net->multi && net->multi_persistent && net->multi_resident) {
-    const long long k = ((net->k_total - 1) % 3 + 3) % 3;
+    const long long k = (net->k_total - 1) & 3;
     return (int8_t*)r.par[0] + (size_t)k * r.count;
   }
   return r.par[(int)((net->k_total - 1) & 1)];
@@ -781,9 +781,9 @@ int bcpnn_net_create(const bcpnn_net_desc* desc, bcpnn_net** out) {
     if ((rc = dalloc(net, &D.cell, cells))) return bail(rc);
     if ((rc = dalloc(net, &D.tij, cells))) return bail(rc);
     if ((rc = dalloc(net, &D.wij, cells))) return bail(rc);
-    /* source spikes: one block of three buffers of Ns; the tick parity
-       forms use the first two, ProcUpdMulti's resident launch all three */
-    if ((rc = dalloc(net, &D.si[0], 3 * (size_t)J.Ns))) return bail(rc);
+    /* source spikes: one block of four buffers of Ns; the tick parity
+       forms use the first two, ProcUpdMulti's resident launch all four */
+    if ((rc = dalloc(net, &D.si[0], 4 * (size_t)J.Ns))) return bail(rc);
     D.si[1] = D.si[0] + J.Ns;
     if ((rc = dalloc(net, &D.list, R))) return bail(rc);
     if ((rc = dalloc(net, &D.list_cnt, J.H))) return bail(rc);

@@ -593,8 +593,8 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
    the only data of other CTAs a tick reads, and only the delay queue reads
    them: a CTA arrives at the grid barrier when the two groups join (its
    source spikes written, the previous tick's read) and only the delay-queue
-   warps wait, before they read.  CTAs may run one tick apart, so the source
-   spikes live in three buffers by tick (tick mod 3).  After its rows the
+   warps wait, before they read.  CTAs may run ticks apart, so the source
+   spikes live in four buffers by tick (tick mod 4).  After its rows the
    CTA draws the next tick's sampling uniforms and stages the next tick's
    first row chunk of projection 0 (row traces, cell replays and decays to
    the next tick). */
@@ -948,10 +948,10 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         r_hist[j] = (r_hist[j] << 1) | (sv > 0 ? 1u : 0u);
         pop.spike[idx] = sv;
         if (sv) atomicOr(&log[idx >> 5], 1u << (idx & 31));
-        /* source spikes in three buffers by tick (kk mod 3): a CTA may run
-           one tick ahead of the readers of the previous tick's */
+        /* source spikes in four buffers by tick (kk mod 4): a CTA may write
+           tick u's while others still read ticks u-3 .. u-1 */
         for (int q = 0; q < pop.n_out; ++q) {
-          int8_t* si = (q < kMaxIn ? s_siout[q][0] : net->projs[pop.out_proj[q]].si[0]) + (size_t)(kk % 3) * n;
+          int8_t* si = (q < kMaxIn ? s_siout[q][0] : net->projs[pop.out_proj[q]].si[0]) + (size_t)(kk & 3) * n;
           si[idx] = sv;
         }
       }
@@ -1099,15 +1099,15 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
 #ifdef BCPNN_PHASE_PROBE
         const long long qclk = clock64();
 #endif
-        /* two arrivals per CTA and tick, its population group's (source
-           spikes written) and its delay-queue group's (source spikes read),
-           on the counter of the tick's slot (tick mod 4).  A group arrives
-           for tick u only once tick u - 2 is complete, so while tick t - 1
-           is incomplete no arrival for a tick above t exists, and the
-           slot's count for t - 1 is 2 arrivals x CTAs x its ticks so far */
+        /* one arrival per CTA and tick, its population group's (source
+           spikes written), on the counter of the tick's slot (tick mod 4).
+           A CTA arrives for tick u only once tick u - 2 is complete, so
+           while tick t - 1 is incomplete no arrival for a tick above t
+           exists, and the slot's count for t - 1 is CTAs x its ticks so
+           far.  Tick u - 2 complete also means every CTA's queue has read
+           the spikes of tick u - 4 or earlier: four buffers suffice */
         const int tp = it - 1 - it0;
-        if (qt == 0 && !mp_poll(bar + (tp & 3), 2u * gridDim.x * (unsigned int)((tp >> 2) + 1), net->err))
-          s_qok = 0;
+        if (qt == 0 && !mp_poll(bar + (tp & 3), gridDim.x * (unsigned int)((tp >> 2) + 1), net->err)) s_qok = 0;
 #ifdef BCPNN_PHASE_PROBE
         if (qt == 0) g_probe_smem[12] += (unsigned long long)(clock64() - qclk);
 #endif
@@ -1117,7 +1117,7 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         const ProjDev& J = s_proj[q];
         const int C = J.C, Ns = J.Ns;
         const ResQ V = res_q(sm, L, q, M, C);
-        const int8_t* si = J.si[0] + (size_t)((kk + 2) % 3) * Ns;
+        const int8_t* si = J.si[0] + (size_t)((kk + 3) & 3) * Ns;
         const int ng = (C + 31) >> 5; /* groups of 32 slots; warp qw takes a contiguous range */
         const int per = (ng + kResQueueWarps - 1) / kResQueueWarps;
         const int g0 = qw * per, g1 = min(ng, g0 + per);
@@ -1182,9 +1182,6 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
           if (a < end) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
         }
       }
-      /* the previous tick's source spikes are read: the group's arrival */
-      named_sync(kBarQueue, 32 * kResQueueWarps);
-      if (qt == 0 && it + 1 < it0 + n_ticks) mp_arrive(bar + ((it - it0) & 3));
     }
     __syncthreads();
     MPROBE(10);
