@@ -588,16 +588,17 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
 
    The delay queue of a tick reads only the previous tick's source spikes and
    qi, so its 4 warps (threads 384-511) compute the next tick's active rows
-   while the other 12 warps do the population update; every thread then
-   takes part in the projections.  The previous tick's source spikes are
-   the only data of other CTAs a tick reads, and only the delay queue reads
-   them: a CTA arrives at the grid barrier when the two groups join (its
-   source spikes written, the previous tick's read) and only the delay-queue
-   warps wait, before they read.  CTAs may run ticks apart, so the source
-   spikes live in four buffers by tick (tick mod 4).  After its rows the
-   CTA draws the next tick's sampling uniforms and stages the next tick's
-   first row chunk of projection 0 (row traces, cell replays and decays to
-   the next tick). */
+   while the other 12 warps (the population group) do the population update
+   and then the tick's projections.
+   The previous tick's source spikes are the only data of other CTAs a tick
+   reads, and only the delay queue reads them: the population group arrives
+   at the grid barrier once it has written this tick's source spikes and
+   goes on with the tick's rows (listed by the previous tick's queue), while
+   the delay-queue warps wait for the previous tick's arrivals and run the
+   queue; the groups join before the staging.  CTAs may run ticks apart, so
+   the source spikes live in four buffers by tick (tick mod 4).  Before the
+   next tick the CTA draws its sampling uniforms and stages its first row
+   chunk of projection 0 (row traces, cell replays and decays). */
 constexpr int kResQueueWarps = 4;
 constexpr int kResPopThreads = kProjThreads - 32 * kResQueueWarps; /* 384 */
 constexpr int kBarPop = 1, kBarQueue = 2;
