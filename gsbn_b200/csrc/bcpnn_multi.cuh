@@ -960,6 +960,65 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
       /* this tick's source spikes are written: the group's arrival */
       named_sync(kBarPop, G);
       if (tid == 0 && it + 1 < it0 + n_ticks) mp_arrive(bar + ((it - it0) & 3));
+      /* stage this tick's first row chunk of projection 0 (listed by the
+         previous tick's queue) after the arrival: row traces, and the
+         cells' replays and decays to this tick; the rows phase adds a spike
+         now and writes the cells */
+      if (n_in > 0) {
+        const ProjDev& J = s_proj[0];
+        const TabRef* T = &s_tab[0];
+        const int C = J.C;
+        const ResQ V = res_q(sm, L, 0, M, C);
+        const float kp = J.taupdt * rp->prn;
+        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
+        const float4* tab = T->tab;
+        const int tlen = T->len;
+        const int ts = simstep;
+        const int* nl = V.list + lp * C;
+        const int nrow1 = s_nlist[0][lp];
+        const int nr = nrow1 < rch ? nrow1 : rch;
+        for (int t = tid; t < nr; t += G) {
+          const int sl = nl[t];
+          s_ti[t] = V.ti[sl];
+          s_zi[t] = V.zi[sl];
+        }
+        named_sync(kBarPop, G);
+        for (int t = G - 1 - tid; t < nr; t += G) {
+          const int sl = nl[t];
+          const int pdt = ts - s_ti[t];
+          float pi = V.pi[sl];
+          if (pdt > 0) {
+            float4 A, Bv;
+            double2 R0, R1;
+            if (pdt < tlen) {
+              A = tab[(size_t)pdt * 4 + 2];
+              Bv = tab[(size_t)pdt * 4 + 3];
+              R0 = T->rtab[(size_t)pdt * 4 + 2];
+              R1 = T->rtab[(size_t)pdt * 4 + 3];
+            } else {
+              table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
+              recip_part(A, Bv, 2, R0, R1);
+            }
+            /* zi becomes zi*exp(-kzi*pdt) */
+            const float4 rv = row_step_nl(make_float4(pi, V.ei[sl], s_zi[t], 0.0f), T, A, Bv, R0, R1);
+            pi = rv.x;
+            V.pi[sl] = rv.x;
+            V.ei[sl] = rv.y;
+            V.zi[sl] = rv.z + J.kfti;
+          }
+          V.ti[sl] = ts;
+          s_pi[t] = pi;
+        }
+        for (int c = tid; c < nr * M; c += G) {
+          const int rr = c / M, j = c - rr * M;
+          float4 c4 = J.cell[(size_t)(h * C + nl[rr]) * M + j];
+          /* bit b of the history is tick ts - b; bit 0 (a spike now) is
+             not replayed */
+          replay_cell_hist(c4, s_ti[rr], s_zi[rr], ts, r_hist[j], B, k, tab, tlen, T, J.kftj);
+          st_c4[c] = c4;
+        }
+        if (tid == 0) s_staged = nr;
+      }
 
         /* ---- projections (update_jxx_cpu, update_row_cpu, Proj.cpp:557-706),
            by the population group while the delay-queue warps run on: the
@@ -1188,11 +1247,8 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
     MPROBE(10);
     if (!s_qok) break;
 
-    /* the next tick's uniforms and row staging (no other CTA's data; the
-       join above ordered this tick's rows and queue before it) */
+    /* the next tick's uniforms (they depend on tick and MCU only) */
     if (it + 1 < it0 + n_ticks) {
-      /* the uniforms by threads 256 up (MCU (tid + 256) mod 512): the staging
-         below takes its cells from thread 0 up and its rows from the top */
       {
         const int j = (tid + kProjThreads / 2) & (kProjThreads - 1);
         if (j < M) {
@@ -1201,69 +1257,8 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
           r_up[j] = poisson ? bx_uniform01_poisson(pop.rng_seed, pop.rng_pop, (uint32_t)(simstep + 1), idx) : 1.0f;
         }
       }
-      /* stage the next tick's first row chunk of projection 0: its rows
-         (listed by this tick's delay queue) and their cells change only in
-         their own row update, so their row traces and their cells' replays
-         and decays to the next tick can run now, while the other CTAs
-         arrive; the next tick adds a spike now and writes the cells */
-      if (n_in > 0) {
-        const ProjDev& J = s_proj[0];
-        const TabRef* T = &s_tab[0];
-        const int C = J.C;
-        const ResQ V = res_q(sm, L, 0, M, C);
-        const float kp = J.taupdt * rp->prn;
-        const Coef k = make_coef(kp, J.ke, J.kzi, J.kzj);
-        const float4* tab = T->tab;
-        const int tlen = T->len;
-        const int ts = simstep + 1;
-        const int* nl = V.list + (lp ^ 1) * C;
-        const int nrow1 = s_nlist[0][lp ^ 1];
-        const int nr = nrow1 < rch ? nrow1 : rch;
-        for (int t = tid; t < nr; t += blockDim.x) {
-          const int sl = nl[t];
-          s_ti[t] = V.ti[sl];
-          s_zi[t] = V.zi[sl];
-        }
-        __syncthreads();
-        for (int t = blockDim.x - 1 - tid; t < nr; t += blockDim.x) {
-          const int sl = nl[t];
-          const int pdt = ts - s_ti[t];
-          float pi = V.pi[sl];
-          if (pdt > 0) {
-            float4 A, Bv;
-            double2 R0, R1;
-            if (pdt < tlen) {
-              A = tab[(size_t)pdt * 4 + 2];
-              Bv = tab[(size_t)pdt * 4 + 3];
-              R0 = T->rtab[(size_t)pdt * 4 + 2];
-              R1 = T->rtab[(size_t)pdt * 4 + 3];
-            } else {
-              table_pair(k.kp, k.ke, k.kzi, k.kzj, pdt, 2, A, Bv, k.fp64);
-              recip_part(A, Bv, 2, R0, R1);
-            }
-            /* zi becomes zi*exp(-kzi*pdt) */
-            const float4 rv = row_step_nl(make_float4(pi, V.ei[sl], s_zi[t], 0.0f), T, A, Bv, R0, R1);
-            pi = rv.x;
-            V.pi[sl] = rv.x;
-            V.ei[sl] = rv.y;
-            V.zi[sl] = rv.z + J.kfti;
-          }
-          V.ti[sl] = ts;
-          s_pi[t] = pi;
-        }
-        for (int c = tid; c < nr * M; c += blockDim.x) {
-          const int rr = c / M, j = c - rr * M;
-          float4 c4 = J.cell[(size_t)(h * C + nl[rr]) * M + j];
-          /* bit b + 1 of the shifted history is tick ts - 1 - b; bit 0 (the
-             next tick's own spike) is not replayed */
-          replay_cell_hist(c4, s_ti[rr], s_zi[rr], ts, r_hist[j] << 1, B, k, tab, tlen, T, J.kftj);
-          st_c4[c] = c4;
-        }
-        if (tid == 0) s_staged = nr;
-      }
       MPROBE(11);
-      /* the next tick's population update reads the uniforms drawn here
-         and shifts the history the staging reads */
+      /* the next tick's population update reads the uniforms drawn here */
       __syncthreads();
     }
   }
