@@ -596,9 +596,10 @@ __device__ __forceinline__ void tick_loop(const NetDev* __restrict__ net, const 
    goes on with the tick's rows (listed by the previous tick's queue), while
    the delay-queue warps wait for the previous tick's arrivals and run the
    queue; the groups join before the staging.  CTAs may run ticks apart, so
-   the source spikes live in four buffers by tick (tick mod 4).  Before the
-   next tick the CTA draws its sampling uniforms and stages its first row
-   chunk of projection 0 (row traces, cell replays and decays). */
+   the source spikes live in four buffers by tick (tick mod 4).  Right after
+   its arrival the population group stages the tick's first row chunk of
+   projection 0 (row traces, cell replays and decays); at the end of a tick
+   the CTA draws the next tick's sampling uniforms. */
 constexpr int kResQueueWarps = 4;
 constexpr int kResPopThreads = kProjThreads - 32 * kResQueueWarps; /* 384 */
 constexpr int kBarPop = 1, kBarQueue = 2;
