@@ -1055,9 +1055,9 @@ __device__ __forceinline__ void res_tick_loop(const NetDev* __restrict__ net, co
         for (int base = 0; base < nrow; base += rch) {
           const int nr = (nrow - base) < rch ? (nrow - base) : rch;
           if (q == 0 && base == 0 && s_staged == nr) {
-            /* staged after the previous tick's barrier arrival: the row
-               traces are up to date, the cells replayed and decayed to this
-               tick; what is left is a spike now */
+            /* staged after this tick's barrier arrival: the row traces
+               are up to date, the cells replayed and decayed to this tick;
+               what is left is a spike now */
             for (int t = tid; t < nr; t += G)
               if (h * C + list[t] == 9) s_flag9 = 1;
             for (int c = tid; c < nr * M; c += G) {

@@ -35,9 +35,9 @@ PHASES_B = {16: "barrier wait", 26: "column units of the grid", 19: "  units: ri
             18: "delay queue: sync", 27: "delay queue: list", 28: "spike wait", 29: "unit publication",
             24: "join wait", 25: "staging next chunk"}
 PHASES_MULTI = {0: "barrier wait (global form)", 1: "support", 2: "softmax: max, exp", 3: "softmax: sum", 4: "spikes",
-                5: "j-traces, row list", 6: "row traces, cell replays", 7: "weights", 8: "epsc sums",
+                5: "staging, j-traces, row list", 6: "rows: spike now, replays", 7: "weights", 8: "epsc sums",
                 9: "delay queue", 10: "wait for the delay-queue warps",
-                11: "uniforms, staging next rows", 12: "queue warps: grid-barrier wait"}
+                11: "uniforms", 12: "queue warps: grid-barrier wait"}
 
 
 def main():
@@ -94,8 +94,8 @@ def main():
             for k, ph in PHASES_MULTI.items():
                 med, mx = float(np.median(pt[:, k])), float(pt[:, k].max())
                 tot += med if k != 12 else 0.0  # the queue warps' wait overlaps thread 0's phases
-                print(f"  {ph:<26} {med:7.3f} {mx:7.3f}")
-            print(f"  {'total (median)':<26} {tot:7.3f}")
+                print(f"  {ph:<30} {med:7.3f} {mx:7.3f}")
+            print(f"  {'total (median)':<30} {tot:7.3f}")
         return
     for name, pt in out.items():
         print(f"== {name} segments: us per tick at {a.mhz:.0f} MHz (median CTA / slowest CTA)")
