@@ -43,13 +43,14 @@ __host__ __device__ inline int row_chunk(int M) { return M >= kRowCells ? 1 : kR
 /* phase probe of the persistent launch (BCPNN_PHASE_PROBE): thread 0 adds
    the cycles since its previous mark to slot `slot` of its CTA's counters:
    0 barrier wait, 1 support, 2 softmax maximum and exponentials, 3 softmax
-   sum, 4 spikes, 5 j-traces and row list, 6 row traces and cell replays,
-   7 weights, 8 epsc sums, 9 delay queue, 10 (resident launch) wait for the
-   delay-queue warps, 11 (resident launch) the uniforms and the staging of
-   the next tick's first row chunk, 12 (resident launch, the first
-   delay-queue thread) its wait at the grid barrier; kProbeTicks counts the
-   ticks.  In the resident launch slot 0 holds no barrier wait (only the
-   delay-queue warps wait there). */
+   sum, 4 spikes, 5 j-traces and row list (in the resident launch after the
+   staging of the tick's first row chunk), 6 row traces and cell replays (of
+   a staged chunk: its spike now and the cell writes), 7 weights, 8 epsc
+   sums, 9 delay queue, 10 (resident launch) wait for the delay-queue warps,
+   11 (resident launch) the next tick's uniforms, 12 (resident launch, the
+   first delay-queue thread) its wait at the grid barrier; kProbeTicks
+   counts the ticks.  In the resident launch slot 0 holds no barrier wait
+   (only the delay-queue warps wait there). */
 #ifdef BCPNN_PHASE_PROBE
 #define MPROBE(slot)                                                   \
   do {                                                                 \
